@@ -1,0 +1,150 @@
+"""Seeded synthetic inputs for the benchmark and parity workloads (numpy, host side).
+
+No public dataset is involved: every workload is generated here from a fixed seed.
+  fixture6    the reference test suite's 6x6 fixture (test/linear_solver_test.jl:8-32)
+  plain64     64x64, 10 km: OCEAN column at x = 0, noisy sloping bed, parabolic surface
+  plain1024   the same generator at 1024x1024, 100 km
+  seasonal4096 4096x4096, 200 km: plus seeded LAND / OTHER_BASIN blobs (10 % of cells), a
+              1-year sinusoidal melt (peak 5e-8 m/s) and 64 point moulins of 1-20 m^3/s
+Arrays are Float64, Fortran-ordered, shapes (nx,ny) / (nx+1,ny) / (nx,ny+1).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+GROUNDED, OCEAN, LAND, OTHER_BASIN = 0.0, 1.0, 2.0, 3.0
+SECONDS_PER_YEAR = 365 * 86400.0
+A_VISC = 5e-25  # the reference fixture's rate factor (test/linear_solver_test.jl:20)
+
+
+@dataclass
+class Workload:
+    name: str
+    nx: int
+    ny: int
+    lx: float
+    ly: float
+    inputs: dict
+    sliding_C: float
+    params: dict = field(default_factory=dict)
+    melt: dict | None = None        # None: constant; else SeasonalMeltInput kwargs (+ 'base')
+    seed: int = 0
+
+    @property
+    def dx(self) -> float:
+        return self.lx / (self.nx - 1)
+
+    @property
+    def dy(self) -> float:
+        return self.ly / (self.ny - 1)
+
+
+def _zeros(*shape):
+    return np.zeros(shape, order="F")
+
+
+def fixture6() -> Workload:
+    """test/linear_solver_test.jl:8-32 (and the same block in the other test files)."""
+    nx = ny = 6
+    lx = ly = 1e3
+    dx = lx / (nx - 1)
+    dy = ly / (ny - 1)
+    x = np.arange(nx) * dx
+    mask = np.full((nx, ny), GROUNDED, order="F")
+    mask[-1, :] = OCEAN
+    mask[0, :] = LAND
+    mask[:, 0] = OTHER_BASIN
+    zb = np.asfortranarray(np.repeat((-0.02 * x).reshape(nx, 1), ny, axis=1))
+    ieb = _zeros(nx, ny)
+    ieb[2, 2] = 3 / (dx * dy)
+    inputs = dict(mask=mask, A_visc=np.full((nx, ny), 5e-25, order="F"), zb=zb, zs=zb + 500.0,
+                  b=np.full((nx, ny), 0.01, order="F"), G=np.full((nx, ny), 0.06, order="F"),
+                  ub_x=np.full((nx + 1, ny), 1e-6, order="F"), ub_y=_zeros(nx, ny + 1), ieb=ieb,
+                  taub_x=_zeros(nx + 1, ny), taub_y=_zeros(nx, ny + 1))
+    return Workload("fixture6", nx, ny, lx, ly, inputs, sliding_C=0.25)
+
+
+def plain(nx: int, lx: float, seed: int = 20260, ny: int | None = None, ly: float | None = None,
+          C: float = 1e4) -> Workload:
+    """The plain-method generator: GROUNDED with an OCEAN column at x = 0 (Dirichlet head),
+    zb = 0.01 (lx - x) + N(0, 5 m), zs = zb + 6 sqrt(x + 5000), b = 0.005 + U(-0.001, 0.001),
+    G = 0.05, ub_x = 30 m/a, ub_y = 0, ieb = 1e-8 m/s, A = 5e-25."""
+    ny = nx if ny is None else ny
+    ly = lx if ly is None else ly
+    rng = np.random.default_rng(seed)
+    dx = lx / (nx - 1)
+    x = np.arange(nx) * dx
+    X = np.repeat(x.reshape(nx, 1), ny, axis=1)
+    mask = np.full((nx, ny), GROUNDED, order="F")
+    mask[0, :] = OCEAN
+    zb = np.asfortranarray(0.01 * (lx - X) + rng.normal(0.0, 5.0, size=(ny, nx)).T)
+    zs = np.asfortranarray(zb + 6.0 * np.sqrt(X + 5000.0))
+    b = np.asfortranarray(0.005 + rng.uniform(-0.001, 0.001, size=(ny, nx)).T)
+    inputs = dict(mask=mask, A_visc=np.full((nx, ny), A_VISC, order="F"), zb=zb, zs=zs, b=b,
+                  G=np.full((nx, ny), 0.05, order="F"),
+                  ub_x=np.full((nx + 1, ny), 30.0 / SECONDS_PER_YEAR, order="F"), ub_y=_zeros(nx, ny + 1),
+                  ieb=np.full((nx, ny), 1e-8, order="F"), taub_x=_zeros(nx + 1, ny), taub_y=_zeros(nx, ny + 1))
+    return Workload(f"plain{nx}", nx, ny, lx, ly, inputs, sliding_C=C, seed=seed)
+
+
+def plain64() -> Workload:
+    return plain(64, 10e3, seed=20260)
+
+
+def plain1024() -> Workload:
+    return plain(1024, 100e3, seed=20261)
+
+
+def _paint_blobs(mask: np.ndarray, rng, frac: float, rmin: int, rmax: int) -> None:
+    nx, ny = mask.shape
+    target = int(frac * nx * ny)
+    painted = 0
+    kinds = (LAND, OTHER_BASIN)
+    k = 0
+    while painted < target:
+        r = int(rng.integers(rmin, rmax + 1))
+        cx = int(rng.integers(r + 2, nx - r - 1))
+        cy = int(rng.integers(r, ny - r))
+        x0, x1, y0, y1 = cx - r, cx + r + 1, cy - r, cy + r + 1
+        ii, jj = np.meshgrid(np.arange(x0, x1), np.arange(y0, y1), indexing="ij")
+        disk = (ii - cx) ** 2 + (jj - cy) ** 2 <= r * r
+        sub = mask[x0:x1, y0:y1]
+        fresh = disk & (sub == GROUNDED)
+        sub[fresh] = kinds[k % 2]
+        painted += int(fresh.sum())
+        k += 1
+
+
+def seasonal(nx: int, lx: float, seed: int = 20262, n_moulins: int = 64, blob_frac: float = 0.10) -> Workload:
+    """Mixed-precision workload: the plain generator plus LAND / OTHER_BASIN blobs covering
+    `blob_frac` of the cells, a seasonal sinusoid (period 1 year, peak 5e-8 m/s, expressed as a
+    SeasonalMeltInput window covering the whole year) and `n_moulins` point sources of 1-20 m^3/s
+    each spread as Q/(dx dy) over one GROUNDED cell."""
+    w = plain(nx, lx, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    mask = w.inputs["mask"]
+    rmax = max(2, nx // 100)
+    _paint_blobs(mask, rng, blob_frac, max(1, rmax // 4), rmax)
+    base = _zeros(nx, nx)
+    grounded = np.argwhere(mask == GROUNDED)
+    pick = grounded[rng.choice(len(grounded), size=n_moulins, replace=False)]
+    Q = rng.uniform(1.0, 20.0, size=n_moulins)
+    for (i, j), q in zip(pick, Q):
+        base[i, j] = q / (w.dx * w.dy)
+    peak_ma = 5e-8 * SECONDS_PER_YEAR
+    # i(yf) = offset - amplitude*cos(2 pi yf) with offset = peak/2, amplitude = -peak/2: peak at yf=0
+    w.melt = dict(t_start=0.0, t_end=1.0, amplitude=-peak_ma / 2, offset=peak_ma / 2, i_min=0.0,
+                  seconds_per_year=SECONDS_PER_YEAR, base=base)
+    w.inputs["ieb"] = base.copy(order="F")
+    w.name = f"seasonal{nx}"
+    w.seed = seed
+    return w
+
+
+def seasonal4096() -> Workload:
+    return seasonal(4096, 200e3)
+
+
+WORKLOADS = {"fixture6": fixture6, "plain64": plain64, "plain1024": plain1024, "seasonal4096": seasonal4096}

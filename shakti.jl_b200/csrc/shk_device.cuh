@@ -1,0 +1,147 @@
+// shk_device.cuh -- device helpers: Julia-faithful scalar functions, tile iteration and the
+// deterministic last-block grid reduction.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "shk_internal.cuh"
+
+namespace shk {
+
+// ---- scalar semantics matching the reference (Julia) -----------------------------------------
+
+// Julia x^n for Float64 and Integer n (Base.pow_body): n == 3 is x*x*x; n == 2 gives fl(x*x);
+// other n use a compensated power-by-squaring.
+__device__ __forceinline__ double jl_powi(double x, int n) {
+    if (n == 0) return 1.0;
+    if (n == 1) return x;
+    if (n == 2) return x * x;
+    if (n == 3) return x * x * x;
+    double y = 1.0, xnlo = 0.0, ynlo = 0.0;
+    while (n > 1) {
+        if (n & 1) {
+            double err = fma(y, xnlo, x * ynlo);
+            double hi = x * y;
+            double lo = fma(x, y, -hi);
+            y = hi;
+            ynlo = lo + err;
+        }
+        double err = x * 2.0 * xnlo;
+        double hi = x * x;
+        double lo = fma(x, x, -hi);
+        x = hi;
+        xnlo = lo + err;
+        n >>= 1;
+    }
+    double err = fma(y, xnlo, x * ynlo);
+    if (isfinite(x) && isfinite(err)) return fma(x, y, fma(y, xnlo, x * ynlo));
+    return x * y;
+}
+
+// pow with the reference's canonical_exponent dispatch (src/model_parameters.jl:122-134).
+__device__ __forceinline__ double jl_pow(double x, double e, int e_int) {
+    return e_int >= 0 ? jl_powi(x, e_int) : pow(x, e);
+}
+
+__device__ __forceinline__ double jl_max(double a, double b) {
+    return (isnan(a) || isnan(b)) ? __longlong_as_double(0x7ff8000000000000LL) : (a > b ? a : b);
+}
+__device__ __forceinline__ double jl_min(double a, double b) {
+    return (isnan(a) || isnan(b)) ? __longlong_as_double(0x7ff8000000000000LL) : (a < b ? a : b);
+}
+__device__ __forceinline__ double jl_sign(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : x); }
+__device__ __forceinline__ double jl_clamp(double x, double lo, double hi) {
+    return x > hi ? hi : (x < lo ? lo : x);
+}
+
+__device__ __forceinline__ bool is_dirichlet(uint8_t m) { return m == M_OCEAN || m == M_LAND; }
+
+// ---- tiles -------------------------------------------------------------------------------------
+
+struct Tiles {
+    int nx, ny, tiles_x, ntiles;
+    __device__ __forceinline__ Tiles(int nx_, int ny_) : nx(nx_), ny(ny_) {
+        tiles_x = (nx + kTX - 1) / kTX;
+        ntiles = tiles_x * ((ny + kTY - 1) / kTY);
+    }
+    __device__ __forceinline__ void cell(int t, int &ix, int &iy) const {
+        int tx = t % tiles_x, ty = t / tiles_x;
+        ix = tx * kTX + (int)(threadIdx.x % kTX);
+        iy = ty * kTY + (int)(threadIdx.x / kTX);
+    }
+};
+
+// ---- reductions -----------------------------------------------------------------------------
+
+template <bool MAX>
+__device__ __forceinline__ double red_op(double a, double b) {
+    if (MAX) return jl_max(a, b);
+    return a + b;
+}
+
+template <bool MAX>
+__device__ __forceinline__ double warp_reduce(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = red_op<MAX>(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-reduce NV values; result valid in thread 0.  Deterministic order.
+template <int NV, bool MAX>
+__device__ __forceinline__ void block_reduce(double (&v)[NV]) {
+    __shared__ double sh[NV][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = warp_reduce<MAX>(v[k]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; k++) sh[k][warp] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double t = lane < nwarps ? sh[k][lane] : 0.0;
+            v[k] = warp_reduce<MAX>(t);
+        }
+    }
+    __syncthreads();
+}
+
+// Grid reduction without inter-block waiting.  Returns true in exactly one block (the last to
+// arrive); there, thread 0 holds the totals in out[] (other threads: unspecified).
+template <int NV, bool MAX>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, unsigned int *counter,
+                                            double (&out)[NV]) {
+    __shared__ int am_last;
+    block_reduce<NV, MAX>(v);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) partials[(size_t)k * gridDim.x + blockIdx.x] = v[k];
+        __threadfence();
+        unsigned int prev = atomicAdd(counter, 1u);
+        am_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        acc[k] = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+            acc[k] = red_op<MAX>(acc[k], __ldcg(&partials[(size_t)k * gridDim.x + i]));
+    }
+    block_reduce<NV, MAX>(acc);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) out[k] = acc[k];
+        *counter = 0u;
+        __threadfence();
+    }
+    return true;
+}
+
+} // namespace shk

@@ -1,0 +1,580 @@
+// shk_fields.cu -- point-wise and stencil field kernels of libshakti_b200:
+//   set_initial_conditions!, update_MFLS! assembly, the fused Picard tail, relax_h!, step_b!.
+//
+// Every value is produced with the reference's formula and evaluation order (the library is
+// compiled with --fmad=false, so no a*b+c is contracted), which makes these kernels bit-identical
+// to the reference's unfused kernels except for x^(1/n), where CUDA's pow and Julia's pow may
+// differ in the last bit.  Fusion never changes a value: a face quantity needed by two cells is
+// recomputed by both from the same operands.
+#include <cuda_runtime.h>
+#include <float.h>
+
+#include "shk_device.cuh"
+
+namespace shk {
+
+#define CI(ix, iy) ((size_t)(ix) + (size_t)(iy) * (size_t)nx)
+#define XI(ix, iy) ((size_t)(ix) + (size_t)(iy) * (size_t)(nx + 1))
+#define YI(ix, iy) ((size_t)(ix) + (size_t)(iy) * (size_t)nx)
+
+// ---------------------------------------------------------------------------------------------
+// Mask
+// ---------------------------------------------------------------------------------------------
+
+__global__ void k_mask8(int n, const double *__restrict__ mask, uint8_t *__restrict__ m8) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double m = mask[i];
+        uint8_t c = M_UNKNOWN;
+        if (m == 0.0) c = M_GROUNDED;
+        else if (m == 1.0) c = M_OCEAN;
+        else if (m == 2.0) c = M_LAND;
+        else if (m == 3.0) c = M_OTHER;
+        m8[i] = c;
+    }
+}
+
+// compute_valid_x/y_kernel! (src/mask.jl:62-84) and apply_mask_to_sliding_x/y_kernel!
+// (src/mask.jl:117-136): one thread per face.
+__global__ void k_face_masks_and_sliding(int nx, int ny, const uint8_t *__restrict__ m8,
+                                         double *valid_x, double *valid_y, double *ub_x, double *ub_y) {
+    const long long nxf = (long long)(nx + 1) * ny, nyf = (long long)nx * (ny + 1);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nxf + nyf;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (i < nxf) {
+            int f = (int)(i % (nx + 1)), iy = (int)(i / (nx + 1));
+            bool interior = f > 0 && f < nx;
+            double v = 1.0;
+            bool both_grounded = false;
+            if (interior) {
+                uint8_t a = m8[CI(f - 1, iy)], b = m8[CI(f, iy)];
+                v = (a != M_OTHER && b != M_OTHER) ? 1.0 : 0.0;
+                both_grounded = a == M_GROUNDED && b == M_GROUNDED;
+            }
+            valid_x[i] = v;
+            if (!interior || !both_grounded) ub_x[i] = 0.0;
+        } else {
+            long long j = i - nxf;
+            int ix = (int)(j % nx), f = (int)(j / nx);
+            bool interior = f > 0 && f < ny;
+            double v = 1.0;
+            bool both_grounded = false;
+            if (interior) {
+                uint8_t a = m8[CI(ix, f - 1)], b = m8[CI(ix, f)];
+                v = (a != M_OTHER && b != M_OTHER) ? 1.0 : 0.0;
+                both_grounded = a == M_GROUNDED && b == M_GROUNDED;
+            }
+            valid_y[j] = v;
+            if (!interior || !both_grounded) ub_y[j] = 0.0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// set_initial_conditions! (src/initial_conditions.jl:14-125), centre steps in reference order.
+// ---------------------------------------------------------------------------------------------
+__global__ void k_init_center(int n, Params P, shk_state s, const uint8_t *__restrict__ m8) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint8_t m = m8[i];
+        const double lambda_coeff = 1.5;
+        s.lambda[i] = lambda_coeff * s.A_visc[i];
+        double b = s.b[i];
+        b = (s.mask[i] != 0.0) ? 0.0 : b; // ifelse(mask != GROUNDED, 0, b)
+        s.b[i] = b;
+        double H = s.zs[i] - (s.zb[i] + b); // compute_H!
+        s.H[i] = H;
+        if (P.br != 0.0) s.beta[i] = jl_max(0.0, (P.br - b) / P.lr); // compute_beta!
+        double po = P.rho_i * P.g * H; // compute_po!
+        s.po[i] = po;
+        double pw = po / 2;
+        if (m == M_OCEAN) pw = P.p_atm - P.rho_sw * P.g * jl_min(s.zb[i], 0.0);
+        else if (m == M_LAND || m == M_OTHER) pw = P.p_atm;
+        s.pw[i] = pw;
+        // compute_N! then compute_h!
+        double d = po - pw;
+        s.N[i] = (m == M_GROUNDED) ? d : copysign(0.0, d);
+        s.h[i] = pw / (P.rho_w * P.g) + s.zb[i];
+    }
+}
+
+// compute_abs_ub! (src/static_fields.jl:59-66)
+__global__ void k_abs_ub(int nx, int ny, shk_state s) {
+    const int n = nx * ny;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int ix = i % nx, iy = i / nx;
+        double ubx_c = (s.ub_x[XI(ix, iy)] + s.ub_x[XI(ix + 1, iy)]) / 2;
+        double uby_c = (s.ub_y[YI(ix, iy)] + s.ub_y[YI(ix, iy + 1)]) / 2;
+        s.abs_ub[i] = sqrt(ubx_c * ubx_c + uby_c * uby_c);
+    }
+}
+
+// compute_dpwdx!/dpwdy!, compute_dhdx!/dhdy!, compute_b_x!/b_y! (initial-condition order; the
+// gradient edge faces are never written).
+__global__ void k_init_faces(int nx, int ny, Params P, shk_state s) {
+    const long long nxf = (long long)(nx + 1) * ny, nyf = (long long)nx * (ny + 1);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nxf + nyf;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (i < nxf) {
+            int f = (int)(i % (nx + 1)), iy = (int)(i / (nx + 1));
+            if (f > 0 && f < nx) {
+                size_t a = CI(f - 1, iy), b = CI(f, iy);
+                s.dpwdx[i] = ((s.pw[b] - s.pw[a]) / P.dx) * s.valid_x[i];
+                s.dhdx[i] = ((s.h[b] - s.h[a]) / P.dx) * s.valid_x[i];
+                s.b_x[i] = (s.b[b] + s.b[a]) / 2;
+            } else {
+                s.b_x[i] = s.b[CI(f == 0 ? 0 : nx - 1, iy)];
+            }
+        } else {
+            long long j = i - nxf;
+            int ix = (int)(j % nx), f = (int)(j / nx);
+            if (f > 0 && f < ny) {
+                size_t a = CI(ix, f - 1), b = CI(ix, f);
+                s.dpwdy[j] = ((s.pw[b] - s.pw[a]) / P.dy) * s.valid_y[j];
+                s.dhdy[j] = ((s.h[b] - s.h[a]) / P.dy) * s.valid_y[j];
+                s.b_y[j] = (s.b[b] + s.b[a]) / 2;
+            } else {
+                s.b_y[j] = s.b[CI(ix, f == 0 ? 0 : ny - 1)];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Face physics shared by the tail: q/Re (src/water_flux.jl:192-208) and taub (src/sliding_law.jl)
+// ---------------------------------------------------------------------------------------------
+struct FaceOut {
+    double dh, dpw, q, re, taub, ub;
+};
+
+__device__ __forceinline__ void q_re(const Params &P, double bf, double grad, double &q, double &re) {
+    double G = fabs(grad);
+    double D = (bf * bf * bf * P.g * G) / (12 * (P.nu * P.nu));
+    double R = 2 * D / (1 + sqrt(1 + 4 * P.omega * D));
+    re = R;
+    q = -jl_sign(grad) * P.nu * R;
+}
+
+// One face of any sliding law.  Nf/lf/abs_v already staggered; Cf the face coefficient.
+__device__ __forceinline__ double taub_face(const Params &P, const Sliding &L, double Nf, double lf,
+                                            double abs_v, double ub, double Cf) {
+    if (L.kind == SHK_SLIDING_LINEAR) return Cf * Nf * ub;
+    if (!(abs_v > 0)) return 0.0;
+    double denom = (L.kind == SHK_SLIDING_REG_COULOMB_V0) ? L.v0 : jl_pow(fabs(Nf), P.n, P.n_int) * lf;
+    return Nf * Cf * jl_pow(abs_v / (abs_v + denom), P.inv_n, -1) * (ub / abs_v);
+}
+
+// Cell-centred quantities needed by faces.
+struct CellQ {
+    double h, pw, N, lam, aub;
+};
+
+template <bool FROM_H>
+__device__ __forceinline__ CellQ load_cell(const Params &P, const shk_state &s, const uint8_t *m8, size_t c) {
+    CellQ q;
+    if (FROM_H) {
+        q.h = s.h[c];
+        q.pw = P.rho_w * P.g * (q.h - s.zb[c]);
+        double d = s.po[c] - q.pw;
+        q.N = (m8[c] == M_GROUNDED) ? d : copysign(0.0, d);
+    } else {
+        q.h = s.h[c];
+        q.pw = s.pw[c];
+        q.N = s.N[c];
+    }
+    q.lam = s.lambda[c];
+    q.aub = s.abs_ub[c];
+    return q;
+}
+
+// x- (dir 0) or y-face (dir 1) between cells a (west/south) and b (east/north); a or b may be absent
+// at the domain edge (edge face: gradients read from memory, taub uses the one adjacent cell).
+template <bool FROM_H>
+__device__ __forceinline__ FaceOut face(const Params &P, const Sliding &L, const shk_state &s, int dir,
+                                        size_t fi, bool interior, const CellQ &a, const CellQ &b,
+                                        const CellQ &edge_cell) {
+    FaceOut o;
+    const double *dhf = dir == 0 ? s.dhdx : s.dhdy;
+    const double *dpwf = dir == 0 ? s.dpwdx : s.dpwdy;
+    const double *valid = dir == 0 ? s.valid_x : s.valid_y;
+    const double *bface = dir == 0 ? s.b_x : s.b_y;
+    const double *ubf = dir == 0 ? s.ub_x : s.ub_y;
+    const double dd = dir == 0 ? P.dx : P.dy;
+    if (interior && FROM_H) {
+        double v = valid[fi];
+        o.dh = ((b.h - a.h) / dd) * v;
+        o.dpw = ((b.pw - a.pw) / dd) * v;
+    } else {
+        o.dh = dhf[fi];
+        o.dpw = dpwf[fi];
+    }
+    q_re(P, bface[fi], o.dh, o.q, o.re);
+    o.ub = ubf[fi];
+    if (L.kind == SHK_SLIDING_PRESCRIBED) {
+        o.taub = (dir == 0 ? s.taub_x : s.taub_y)[fi];
+    } else {
+        double Nf, lf, av;
+        if (interior) {
+            Nf = (b.N + a.N) / 2;
+            lf = (b.lam + a.lam) / 2;
+            av = (b.aub + a.aub) / 2;
+        } else {
+            Nf = edge_cell.N;
+            lf = edge_cell.lam;
+            av = edge_cell.aub;
+        }
+        double Cf = (L.kind == SHK_SLIDING_REG_COULOMB) ? L.C : (dir == 0 ? L.Cx : L.Cy)[fi];
+        o.taub = taub_face(P, L, Nf, lf, av, o.ub, Cf);
+    }
+    return o;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused tail: compute_dhdxy!, compute_pw!, compute_dpwdxy!, compute_N!, compute_q_and_Re_xy!,
+// compute_Re!, compute_taub_xy!, compute_mdot!, compute_K! (src/elliptic_solver.jl:193-206),
+// plus the Picard check maxima max|h - h_prev| and max|h| (src/elliptic_solver.jl:162-163).
+// FROM_H = false is the initial-condition variant: pw, N and the gradients are taken as set.
+// ---------------------------------------------------------------------------------------------
+template <bool FROM_H, bool CHECK>
+__global__ void __launch_bounds__(kThreads) k_tail(int nx, int ny, Params P, Sliding L, shk_state s,
+                                                   const uint8_t *__restrict__ m8,
+                                                   const double *__restrict__ h_prev, double *partials,
+                                                   unsigned int *counter, PicDev *pic) {
+    Tiles T(nx, ny);
+    double red[2] = {0.0, 0.0};
+    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+        int ix, iy;
+        T.cell(t, ix, iy);
+        if (ix >= nx || iy >= ny) continue;
+        const size_t c = CI(ix, iy);
+        const CellQ q0 = load_cell<FROM_H>(P, s, m8, c);
+        CellQ qW = q0, qE = q0, qS = q0, qN = q0;
+        if (ix > 0) qW = load_cell<FROM_H>(P, s, m8, c - 1);
+        if (ix < nx - 1) qE = load_cell<FROM_H>(P, s, m8, c + 1);
+        if (iy > 0) qS = load_cell<FROM_H>(P, s, m8, c - nx);
+        if (iy < ny - 1) qN = load_cell<FROM_H>(P, s, m8, c + nx);
+
+        // x-faces: W = face ix (cells ix-1 | ix), E = face ix+1 (cells ix | ix+1)
+        const size_t fW = XI(ix, iy), fE = XI(ix + 1, iy);
+        const size_t fS = YI(ix, iy), fN = YI(ix, iy + 1);
+        FaceOut W = face<FROM_H>(P, L, s, 0, fW, ix > 0, qW, q0, q0);
+        FaceOut E = face<FROM_H>(P, L, s, 0, fE, ix < nx - 1, q0, qE, q0);
+        FaceOut S = face<FROM_H>(P, L, s, 1, fS, iy > 0, qS, q0, q0);
+        FaceOut Nf = face<FROM_H>(P, L, s, 1, fN, iy < ny - 1, q0, qN, q0);
+
+        // centre writes
+        if (FROM_H) {
+            s.pw[c] = q0.pw;
+            s.N[c] = q0.N;
+        }
+        // owned faces: W and S always; E on the last column, N on the last row
+        auto write_x = [&](size_t f, const FaceOut &o, bool interior) {
+            if (interior && FROM_H) {
+                s.dhdx[f] = o.dh;
+                s.dpwdx[f] = o.dpw;
+            }
+            s.q_x[f] = o.q;
+            s.Re_x[f] = o.re;
+            if (L.kind != SHK_SLIDING_PRESCRIBED) s.taub_x[f] = o.taub;
+        };
+        auto write_y = [&](size_t f, const FaceOut &o, bool interior) {
+            if (interior && FROM_H) {
+                s.dhdy[f] = o.dh;
+                s.dpwdy[f] = o.dpw;
+            }
+            s.q_y[f] = o.q;
+            s.Re_y[f] = o.re;
+            if (L.kind != SHK_SLIDING_PRESCRIBED) s.taub_y[f] = o.taub;
+        };
+        write_x(fW, W, ix > 0);
+        if (ix == nx - 1) write_x(fE, E, false);
+        write_y(fS, S, iy > 0);
+        if (iy == ny - 1) write_y(fN, Nf, false);
+
+        // compute_Re! (src/water_flux.jl:107-112)
+        const double Re_c = (W.re + E.re + S.re + Nf.re) / 4;
+        s.Re[c] = Re_c;
+        // compute_mdot! (src/melt_rate.jl:106-137)
+        const double sh = fabs((E.ub * E.taub + W.ub * W.taub) / 2 + (Nf.ub * Nf.taub + S.ub * S.taub) / 2);
+        const double pot = fabs((E.q * E.dh + W.q * W.dh) / 2 + (Nf.q * Nf.dh + S.q * S.dh) / 2);
+        s.shear[c] = sh;
+        s.potential[c] = pot;
+        if (P.with_sensible) {
+            const double sens = (E.q * E.dpw + W.q * W.dpw) / 2 + (Nf.q * Nf.dpw + S.q * S.dpw) / 2;
+            s.sensible[c] = sens;
+            s.mdot[c] = P.Linv * (s.G[c] + sh + P.rho_w * P.g * pot + P.ct * P.cw * P.rho_w * sens);
+        } else {
+            s.mdot[c] = P.Linv * (s.G[c] + sh + P.rho_w * P.g * pot);
+        }
+        // compute_K! (src/water_flux.jl:221-226)
+        const double bb = s.b[c];
+        s.K[c] = (bb * bb * bb * P.g) / (12 * P.nu * (1 + P.omega * Re_c));
+        if (CHECK) {
+            red[0] = jl_max(red[0], fabs(q0.h - h_prev[c]));
+            red[1] = jl_max(red[1], fabs(q0.h));
+        }
+    }
+    if (CHECK) {
+        double out[2];
+        if (grid_reduce<2, true>(red, partials, counter, out) && threadIdx.x == 0) {
+            pic->dmax = out[0];
+            pic->hmax = out[1];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Assembly: update_MFLS_kernel! / update_MFLS_parabolic_kernel! (src/linear_solver.jl:438-588)
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ double dirichlet_head(const Params &P, uint8_t m, double zb) {
+    if (m == M_OCEAN) {
+        double pw_bc = P.p_atm - P.rho_sw * P.g * jl_min(zb, 0.0);
+        return pw_bc / (P.rho_w * P.g) + zb;
+    }
+    return P.p_atm / (P.rho_w * P.g) + zb;
+}
+
+// boundary_K_face (src/k_face_scheme.jl:52-61)
+__device__ __forceinline__ double bK(int kfs, double K1, double K2, uint8_t m2) {
+    if (m2 == M_OTHER) return 0.0;
+    if (m2 == M_OCEAN || m2 == M_LAND) return K1;
+    if (kfs == SHK_KFACE_HARMONIC) return (2 * K1 * K2) / (K1 + K2 + DBL_EPSILON);
+    return (K1 + K2) / 2;
+}
+
+template <bool PARABOLIC>
+__global__ void __launch_bounds__(kThreads) k_assemble(int nx, int ny, Params P, int kfs, double dt,
+                                                       shk_state s, const uint8_t *__restrict__ m8,
+                                                       double *__restrict__ aP, double *__restrict__ aE,
+                                                       double *__restrict__ aN, double *__restrict__ rhs,
+                                                       double *__restrict__ h_prev) {
+    Tiles T(nx, ny);
+    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+        int ix, iy;
+        T.cell(t, ix, iy);
+        if (ix >= nx || iy >= ny) continue;
+        const size_t c = CI(ix, iy);
+        const uint8_t m = m8[c];
+        const double h = s.h[c];
+        if (h_prev) h_prev[c] = h;
+        double oP, oE = 0.0, oN = 0.0, orhs;
+        if (is_dirichlet(m)) {
+            oP = 1;
+            orhs = dirichlet_head(P, m, s.zb[c]);
+        } else if (m == M_OTHER) {
+            oP = 1;
+            orhs = h;
+        } else {
+            const double K = s.K[c];
+            double eE = 0.0, eW = 0.0, eN = 0.0, eS = 0.0;
+            uint8_t mE = 0, mW = 0, mN = 0, mS = 0;
+            if (ix < nx - 1) { mE = m8[c + 1]; eE = bK(kfs, K, s.K[c + 1], mE) / P.dx2; }
+            if (ix > 0) { mW = m8[c - 1]; eW = bK(kfs, K, s.K[c - 1], mW) / P.dx2; }
+            if (iy < ny - 1) { mN = m8[c + nx]; eN = bK(kfs, K, s.K[c + nx], mN) / P.dy2; }
+            if (iy > 0) { mS = m8[c - nx]; eS = bK(kfs, K, s.K[c - nx], mS) / P.dy2; }
+            const double Nc = s.N[c], A = s.A_visc[c], b = s.b[c];
+            const double Nn = jl_pow(fabs(Nc), P.nm1, P.nm1_int);
+            if (PARABOLIC) oP = (eE + eW + eN + eS) + P.e_v / dt;
+            else oP = (eE + eW + eN + eS) + P.n * P.rho_w * P.g * A * Nn * b;
+            double drhs = 0.0;
+            if (ix < nx - 1) {
+                if (is_dirichlet(mE)) drhs += eE * dirichlet_head(P, mE, s.zb[c + 1]);
+                else oE = eE;
+            }
+            if (ix > 0 && is_dirichlet(mW)) drhs += eW * dirichlet_head(P, mW, s.zb[c - 1]);
+            if (iy < ny - 1) {
+                if (is_dirichlet(mN)) drhs += eN * dirichlet_head(P, mN, s.zb[c + nx]);
+                else oN = eN;
+            }
+            if (iy > 0 && is_dirichlet(mS)) drhs += eS * dirichlet_head(P, mS, s.zb[c - nx]);
+            if (PARABOLIC)
+                orhs = s.mdot[c] * (1 / P.rho_w - 1 / P.rho_i) - s.beta[c] * s.abs_ub[c] + A * Nn * Nc * b +
+                       s.ieb[c] + (P.e_v / dt) * h + drhs;
+            else
+                orhs = s.mdot[c] * (1 / P.rho_w - 1 / P.rho_i) - s.beta[c] * s.abs_ub[c] + A * Nn * Nc * b +
+                       A * Nn * (P.n * P.rho_w * P.g * h) * b + s.ieb[c] + drhs;
+        }
+        aP[c] = oP;
+        aE[c] = oE;
+        aN[c] = oN;
+        rhs[c] = orhs;
+    }
+}
+
+__global__ void k_export_mfls(int nx, int ny, const double *aP, const double *aE, const double *aN,
+                              const double *rhs, double *oP, double *oE, double *oW, double *oN, double *oS,
+                              double *orhs) {
+    const int n = nx * ny;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int ix = i % nx, iy = i / nx;
+        if (oP) oP[i] = aP[i];
+        if (oE) oE[i] = aE[i];
+        if (oN) oN[i] = aN[i];
+        if (oW) oW[i] = ix > 0 ? aE[i - 1] : 0.0;
+        if (oS) oS[i] = iy > 0 ? aN[i - nx] : 0.0;
+        if (orhs) orhs[i] = rhs[i];
+    }
+}
+
+// relax_h! (src/elliptic_solver.jl:42-46)
+__global__ void k_relax(int n, double alpha, double *h, const double *h_prev) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        h[i] = alpha * h[i] + (1 - alpha) * h_prev[i];
+}
+
+// compute_b_implicit/explicit_kernel! (src/gap_height.jl:117-135) then compute_beta! (:47-52).
+template <bool IMPLICIT>
+__global__ void k_gap_b(int n, Params P, double dt, shk_state s, const uint8_t *__restrict__ m8) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double b = s.b[i];
+        if (s.mask[i] == 0.0) {
+            const double Nc = s.N[i];
+            const double Nn = jl_pow(fabs(Nc), P.nm1, P.nm1_int);
+            double bnew;
+            if (IMPLICIT)
+                bnew = (b + dt * (s.mdot[i] / P.rho_i + s.beta[i] * s.abs_ub[i])) / (1 + dt * s.A_visc[i] * Nn * Nc);
+            else
+                bnew = b + dt * (s.mdot[i] / P.rho_i + s.beta[i] * s.abs_ub[i] - s.A_visc[i] * Nn * Nc * b);
+            b = jl_clamp(bnew, P.b_min, P.b_max);
+            s.b[i] = b;
+        }
+        if (P.br != 0.0) s.beta[i] = jl_max(0.0, (P.br - b) / P.lr);
+    }
+}
+
+// compute_b_x!/compute_b_y! (src/gap_height.jl:75-108)
+__global__ void k_gap_faces(int nx, int ny, shk_state s) {
+    const long long nxf = (long long)(nx + 1) * ny, nyf = (long long)nx * (ny + 1);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nxf + nyf;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (i < nxf) {
+            int f = (int)(i % (nx + 1)), iy = (int)(i / (nx + 1));
+            double v;
+            if (f == 0) v = s.b[CI(0, iy)];
+            else if (f == nx) v = s.b[CI(nx - 1, iy)];
+            else v = (s.b[CI(f, iy)] + s.b[CI(f - 1, iy)]) / 2;
+            s.b_x[i] = v;
+        } else {
+            long long j = i - nxf;
+            int ix = (int)(j % nx), f = (int)(j / nx);
+            double v;
+            if (f == 0) v = s.b[CI(ix, 0)];
+            else if (f == ny) v = s.b[CI(ix, ny - 1)];
+            else v = (s.b[CI(ix, f)] + s.b[CI(ix, f - 1)]) / 2;
+            s.b_y[j] = v;
+        }
+    }
+}
+
+__global__ void k_fill(size_t n, double *dst, double v, const double *base) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = base ? v + base[i] : v;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------------------------
+static int flat_grid(Ctx *c, long long n) {
+    long long b = (n + kThreads - 1) / kThreads;
+    long long cap = (long long)c->num_sms * 16;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+int build_mask8(Ctx *c) {
+    const int n = c->nx * c->ny;
+    k_mask8<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->st.mask, c->mask8);
+    c->launches++;
+    return check_launch(c, "k_mask8");
+}
+
+int launch_initial_conditions(Ctx *c) {
+    const int nx = c->nx, ny = c->ny, n = nx * ny;
+    const long long nf = (long long)(nx + 1) * ny + (long long)nx * (ny + 1);
+    int rc = build_mask8(c);
+    if (rc) return rc;
+    k_face_masks_and_sliding<<<flat_grid(c, nf), kThreads, 0, c->stream>>>(nx, ny, c->mask8, c->st.valid_x,
+                                                                            c->st.valid_y, c->st.ub_x, c->st.ub_y);
+    c->launches++;
+    if ((rc = check_launch(c, "k_face_masks_and_sliding"))) return rc;
+    k_init_center<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->P, c->st, c->mask8);
+    c->launches++;
+    if ((rc = check_launch(c, "k_init_center"))) return rc;
+    k_abs_ub<<<flat_grid(c, n), kThreads, 0, c->stream>>>(nx, ny, c->st);
+    c->launches++;
+    if ((rc = check_launch(c, "k_abs_ub"))) return rc;
+    k_init_faces<<<flat_grid(c, nf), kThreads, 0, c->stream>>>(nx, ny, c->P, c->st);
+    c->launches++;
+    if ((rc = check_launch(c, "k_init_faces"))) return rc;
+    k_tail<false, false><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, c->P, c->SL, c->st, c->mask8, nullptr,
+                                                                       c->partials, c->counter, nullptr);
+    c->launches++;
+    return check_launch(c, "k_tail<init>");
+}
+
+int launch_assemble(Ctx *c, int parabolic, double dt, bool copy_h_prev) {
+    double *hp = copy_h_prev ? c->h_prev : nullptr;
+    if (parabolic)
+        k_assemble<true><<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->kfs, dt, c->st, c->mask8,
+                                                                      c->aP, c->aE, c->aN, c->rhs, hp);
+    else
+        k_assemble<false><<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->kfs, dt, c->st, c->mask8,
+                                                                       c->aP, c->aE, c->aN, c->rhs, hp);
+    c->launches++;
+    return check_launch(c, "k_assemble");
+}
+
+int launch_export_mfls(Ctx *c, double *aP, double *aE, double *aW, double *aN, double *aS, double *rhs) {
+    const int n = c->nx * c->ny;
+    k_export_mfls<<<flat_grid(c, n), kThreads, 0, c->stream>>>(c->nx, c->ny, c->aP, c->aE, c->aN, c->rhs, aP, aE, aW,
+                                                                aN, aS, rhs);
+    c->launches++;
+    return check_launch(c, "k_export_mfls");
+}
+
+int launch_tail(Ctx *c, bool picard_check) {
+    if (picard_check)
+        k_tail<true, true><<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->SL, c->st, c->mask8,
+                                                                        c->h_prev, c->partials, c->counter,
+                                                                        &c->dev->pic);
+    else
+        k_tail<true, false><<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->SL, c->st, c->mask8,
+                                                                         nullptr, c->partials, c->counter, nullptr);
+    c->launches++;
+    return check_launch(c, "k_tail");
+}
+
+int launch_relax(Ctx *c, double alpha, const double *h_prev) {
+    const int n = c->nx * c->ny;
+    k_relax<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, alpha, c->st.h, h_prev);
+    c->launches++;
+    return check_launch(c, "k_relax");
+}
+
+int launch_step_b(Ctx *c, double dt) {
+    const int nx = c->nx, ny = c->ny, n = nx * ny;
+    const long long nf = (long long)(nx + 1) * ny + (long long)nx * (ny + 1);
+    if (c->gap == SHK_GAP_IMPLICIT)
+        k_gap_b<true><<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->P, dt, c->st, c->mask8);
+    else
+        k_gap_b<false><<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->P, dt, c->st, c->mask8);
+    c->launches++;
+    int rc = check_launch(c, "k_gap_b");
+    if (rc) return rc;
+    k_gap_faces<<<flat_grid(c, nf), kThreads, 0, c->stream>>>(nx, ny, c->st);
+    c->launches++;
+    return check_launch(c, "k_gap_faces");
+}
+
+int launch_fill(Ctx *c, double *dst, double v, size_t n) {
+    k_fill<<<flat_grid(c, (long long)n), kThreads, 0, c->stream>>>(n, dst, v, nullptr);
+    c->launches++;
+    return check_launch(c, "k_fill");
+}
+
+int launch_fill_plus_base(Ctx *c, double *dst, double v, const double *base, size_t n) {
+    k_fill<<<flat_grid(c, (long long)n), kThreads, 0, c->stream>>>(n, dst, v, base);
+    c->launches++;
+    return check_launch(c, "k_fill");
+}
+
+} // namespace shk

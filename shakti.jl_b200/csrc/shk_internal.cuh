@@ -1,0 +1,145 @@
+// shk_internal.cuh -- shared definitions of libshakti_b200 (sm_100a).
+//
+// Data layout in HBM
+//   State arrays: caller-owned Float64, column-major (ix fastest), centre nx*ny, x-face (nx+1)*ny,
+//   y-face nx*(ny+1) -- the reference's State layout (src/state.jl:13-57).
+//   Library-owned:
+//     mask8            uint8 copy of State.mask (codes 0..3, 4 = any other value)
+//     aP, aE, aN, rhs  the assembled matrix-free system.  The operator is exactly symmetric
+//                      (src/linear_solver.jl:468-471), so the reference's aW(i,j) equals aE(i-1,j)
+//                      and aS(i,j) equals aN(i,j-1) bit for bit; only aE/aN are stored and the
+//                      matvec reads the west/south couplings from the neighbour's entry.
+//     x, r, z, p[2], Ap Krylov vectors (p double-buffered: the fused update+matvec reads p_old at
+//                      the neighbours while writing p_new)
+//     Float32 copies of the coefficients and vectors for the mixed-precision inner solve.
+//   Device scalar block (CgDev / ChebDev / PicDev): every Krylov scalar (alpha, beta, gamma, the
+//   stopping test) lives on the device; the host only reads a done flag between launch batches.
+//
+// Reductions: each block reduces its tiles, writes one partial per value, fences and bumps a
+// counter; the last block to arrive sums the partials in a fixed order (deterministic for a fixed
+// grid), finishes the scalar update and resets the counter.  No block ever waits on another.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/shakti_b200.h"
+
+namespace shk {
+
+constexpr int kTX = 32;             // tile width (cells along x, one warp)
+constexpr int kTY = 8;              // tile height
+constexpr int kThreads = kTX * kTY; // 256 threads per block
+constexpr int kMaxRedValues = 4;
+constexpr int kMaxChebSteps = 64;   // chebyshev_nsteps_estimate cap
+constexpr int kMaxChebDegree = 32;
+
+enum : uint8_t { M_GROUNDED = 0, M_OCEAN = 1, M_LAND = 2, M_OTHER = 3, M_UNKNOWN = 4 };
+
+struct CgDev {
+    double gamma, pNorm2, eps_stop, alpha, beta, rnorm, rnorm0, bnorm, rr, pAp;
+    double atol, rtol;
+    long long iter, itmax;
+    int done, status, first, stop_rule;
+};
+
+struct ChebDev {
+    double lam_min, lam_max;   // bounds in use (persist across solves; placeholder 1,1)
+    double est_min, est_max;   // last raw estimate
+    int adopted;               // last estimate adopted?
+    int nsteps;
+    double gamma;              // Lanczos-CG running gamma
+    double alphas[kMaxChebSteps], betas[kMaxChebSteps];
+    double calpha[kMaxChebDegree + 1], cbeta[kMaxChebDegree + 1]; // per-step coefficients, 1-based
+};
+
+struct PicDev {
+    double dmax, hmax;
+};
+
+struct DevScalars {
+    CgDev cg;        // outer (Float64) solve
+    CgDev cg_in;     // inner (Float32) solve of the mixed-precision form
+    ChebDev cheb;
+    PicDev pic;
+    double ref_rr, ref_bb; // mixed precision: outer residual norms
+};
+
+struct Params {
+    double rho_w, rho_sw, rho_i, g, nu, n, omega, L, br, lr, ct, cw, p_atm, b_min, b_max, e_v;
+    double nm1, inv_n;   // n-1, 1/n
+    int n_int, nm1_int;  // integer-valued exponents (-1 if not integral)
+    int with_sensible;   // ct*cw != 0
+    double Linv;         // 1/L
+    double dx, dy, dx2, dy2;
+};
+
+struct Sliding {
+    int kind;
+    double C, v0;
+    const double *Cx, *Cy;
+};
+
+struct Ctx {
+    int nx, ny;
+    double lx, ly, dx, dy;
+    cudaStream_t stream = nullptr;
+    int device = 0, num_sms = 148;
+    shk_params hp{};
+    bool params_set = false, state_bound = false, sliding_set = false, initialized = false;
+    Params P{};
+    Sliding SL{};
+    int kfs = 0, gap = 1;
+    shk_state st{};
+    // library-owned device memory
+    void *arena = nullptr;
+    size_t arena_bytes = 0;
+    uint8_t *mask8 = nullptr;
+    double *aP = nullptr, *aE = nullptr, *aN = nullptr, *rhs = nullptr;
+    double *x = nullptr, *r = nullptr, *z = nullptr, *p[2] = {nullptr, nullptr}, *Ap = nullptr;
+    double *h_prev = nullptr;
+    double *cr[2] = {nullptr, nullptr}, *cp[2] = {nullptr, nullptr}; // Chebyshev r/p buffers
+    double *r64 = nullptr;                                            // mixed: outer residual
+    float *aP32 = nullptr, *aE32 = nullptr, *aN32 = nullptr;
+    float *b32 = nullptr, *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32[2] = {nullptr, nullptr}, *Ap32 = nullptr;
+    float *cr32[2] = {nullptr, nullptr}, *cp32[2] = {nullptr, nullptr};
+    double *partials = nullptr;  // kMaxRedValues * max_blocks
+    unsigned int *counter = nullptr;
+    DevScalars *dev = nullptr;
+    DevScalars *host_dev = nullptr;  // pinned mirror for read-back
+    int max_blocks = 0;
+    int grid_stencil = 0;    // blocks for tile-stride kernels
+    long long launches = 0;
+    std::string err;
+    bool assembled = false;
+    bool assembled_parabolic = false;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Host helpers
+// ---------------------------------------------------------------------------------------------
+int fail(Ctx *c, int status, const std::string &msg);
+int check_cuda(Ctx *c, cudaError_t e, const char *what);
+int check_launch(Ctx *c, const char *what);
+
+// shk_fields.cu
+int build_mask8(Ctx *c);
+int launch_initial_conditions(Ctx *c);
+int launch_assemble(Ctx *c, int parabolic, double dt, bool copy_h_prev);
+int launch_export_mfls(Ctx *c, double *aP, double *aE, double *aW, double *aN, double *aS, double *rhs);
+int launch_tail(Ctx *c, bool picard_check);
+int launch_relax(Ctx *c, double alpha, const double *h_prev);
+int launch_step_b(Ctx *c, double dt);
+int launch_fill(Ctx *c, double *dst, double v, size_t n);
+int launch_fill_plus_base(Ctx *c, double *dst, double v, const double *base, size_t n);
+
+// shk_krylov.cu
+int launch_matvec(Ctx *c, const double *x, double *y);
+int run_chebyshev_bounds(Ctx *c, int nsteps, const double *rhs);
+int cheb_set_bounds(Ctx *c, double lmin, double lmax);
+int launch_chebyshev_apply_standalone(Ctx *c, int degree, const double *x, double *y);
+int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st);
+int read_scalars(Ctx *c);
+
+} // namespace shk

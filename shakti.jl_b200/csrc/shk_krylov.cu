@@ -1,0 +1,738 @@
+// shk_krylov.cu -- matrix-free operator, preconditioned CG, Chebyshev preconditioner, and the
+// mixed-precision iterative-refinement form.
+//
+// CG follows Krylov.jl's cg! (v0.10.8, the reference's dependency; call site
+// src/linear_solver.jl:921): warm start x0 = h, x accumulates the correction from zero, r = b - A x0,
+// z = M^-1 r, p = z, gamma = r'z; per iteration Ap = A p, alpha = gamma/p'Ap, x += alpha p,
+// r -= alpha Ap, z = M^-1 r, stop on sqrt(r'z) <= atol + rtol*sqrt(r0'z0), beta = gamma'/gamma,
+// p = z + beta p; finally h = x + h.  All scalars stay on the device.
+//
+// One CG iteration is two kernels over the grid (Jacobi):
+//   A: p_new = z + beta p_old (z = r/aP recomputed, also at the 4 neighbours), Ap = A p_new,
+//      partial p'Ap  -> last block: alpha (or zero-curvature breakdown)
+//   B: x += alpha p, r -= alpha Ap, z = r/aP, partial r'z and r'r -> last block: stop test, beta
+// Algorithmic traffic per cell and iteration: A reads r, aP, p_old, aE, aN and writes p, Ap;
+// B reads x, p, r, Ap, aP and writes x, r: 14 words (112 B in Float64, 56 B in Float32).
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "shk_device.cuh"
+
+namespace shk {
+
+// ---------------------------------------------------------------------------------------------
+// Stencil: stencil_matvec_kernel! (src/linear_solver.jl:616-633), subtraction order E, W, N, S.
+// West/south couplings are the neighbour's east/north entries (exact symmetry of the assembly).
+// ---------------------------------------------------------------------------------------------
+template <typename T, typename F>
+__device__ __forceinline__ T stencil_apply(const T *__restrict__ aP, const T *__restrict__ aE,
+                                           const T *__restrict__ aN, int nx, int ny, int ix, int iy,
+                                           size_t c, T xc, F val) {
+    T y = aP[c] * xc;
+    if (ix < nx - 1) y -= aE[c] * val(c + 1);
+    if (ix > 0) y -= aE[c - 1] * val(c - 1);
+    if (iy < ny - 1) y -= aN[c] * val(c + nx);
+    if (iy > 0) y -= aN[c - nx] * val(c - nx);
+    return y;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_matvec(int nx, int ny, const T *aP, const T *aE, const T *aN,
+                                                     const T *x, T *y) {
+    Tiles Tl(nx, ny);
+    for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
+        int ix, iy;
+        Tl.cell(t, ix, iy);
+        if (ix >= nx || iy >= ny) continue;
+        size_t c = (size_t)ix + (size_t)iy * nx;
+        y[c] = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, x[c], [&](size_t k) { return x[k]; });
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Scalar updates (run by thread 0 of the last block)
+// ---------------------------------------------------------------------------------------------
+__device__ void cg_init_finish(CgDev *cg, double rz, double rr, double bb) {
+    cg->gamma = rz;
+    const double rn = sqrt(rz);
+    cg->rr = sqrt(rr);
+    cg->bnorm = sqrt(bb);
+    cg->rnorm0 = cg->stop_rule == SHK_STOP_KRYLOV ? rn : cg->rr;
+    cg->rnorm = cg->rnorm0;
+    cg->eps_stop = cg->atol + cg->rtol * rn;
+    cg->pNorm2 = rz;
+    cg->iter = 0;
+    cg->first = 1;
+    cg->beta = 0.0;
+    if (isnan(rz) || isnan(rr)) {
+        cg->done = 1;
+        cg->status = SHK_BREAKDOWN;
+    } else if (rz == 0.0) {
+        cg->done = 1;
+        cg->status = SHK_OK;
+    } else {
+        bool solved = cg->stop_rule == SHK_STOP_KRYLOV ? (rn <= cg->eps_stop) : (cg->rr <= cg->rtol * cg->bnorm);
+        if (solved) {
+            cg->done = 1;
+            cg->status = SHK_OK;
+        } else if (cg->iter >= cg->itmax) {
+            cg->done = 1;
+            cg->status = SHK_NOT_CONVERGED;
+        } else {
+            cg->done = 0;
+        }
+    }
+}
+
+__device__ void cg_iter_finish(CgDev *cg, double rz, double rr) {
+    const double rn = sqrt(rz), rrn = sqrt(rr);
+    cg->rr = rrn;
+    bool solved;
+    if (cg->stop_rule == SHK_STOP_KRYLOV) solved = (rn <= cg->eps_stop) || (rn + 1.0 <= 1.0);
+    else solved = rrn <= cg->rtol * cg->bnorm;
+    cg->rnorm = cg->stop_rule == SHK_STOP_KRYLOV ? rn : rrn;
+    if (!solved) {
+        double beta = rz / cg->gamma;
+        cg->pNorm2 = rz + beta * beta * cg->pNorm2;
+        cg->gamma = rz;
+        cg->beta = beta;
+        cg->first = 0;
+    }
+    cg->iter += 1;
+    if (isnan(rz) || isnan(rr)) {
+        cg->done = 1;
+        cg->status = SHK_BREAKDOWN;
+    } else if (solved) {
+        cg->done = 1;
+        cg->status = SHK_OK;
+    } else if (cg->iter >= cg->itmax) {
+        cg->done = 1;
+        cg->status = SHK_NOT_CONVERGED;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// CG kernels.  T = double (plain form) or float (inner solve of the mixed form).
+// ---------------------------------------------------------------------------------------------
+
+// r = b - A x0 (x0 == nullptr: r = b), x = 0; JAC: partials r'z, r'r, b'b -> init finish;
+// otherwise partials r'r, b'b are parked for the Chebyshev init pass.
+template <typename T, bool JAC>
+__global__ void __launch_bounds__(kThreads) k_cg_init(int nx, int ny, const T *aP, const T *aE, const T *aN,
+                                                      const double *x0, const T *b, T *r, T *x, CgDev *cg,
+                                                      double *partials, unsigned int *counter) {
+    Tiles Tl(nx, ny);
+    double red[3] = {0.0, 0.0, 0.0};
+    for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
+        int ix, iy;
+        Tl.cell(t, ix, iy);
+        if (ix >= nx || iy >= ny) continue;
+        size_t c = (size_t)ix + (size_t)iy * nx;
+        T bc = b[c];
+        T rc;
+        if (x0) {
+            T ax = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, (T)x0[c], [&](size_t k) { return (T)x0[k]; });
+            rc = (T)1 * bc + (T)(-1) * ax;
+        } else {
+            rc = bc;
+        }
+        r[c] = rc;
+        x[c] = (T)0;
+        if (JAC) {
+            T zc = rc / aP[c];
+            red[0] += (double)rc * (double)zc;
+        }
+        red[1] += (double)rc * (double)rc;
+        red[2] += (double)bc * (double)bc;
+    }
+    double out[3];
+    if (grid_reduce<3, false>(red, partials, counter, out) && threadIdx.x == 0) {
+        if (JAC) cg_init_finish(cg, out[0], out[1], out[2]);
+        else {
+            cg->rr = out[1];    // parked: squared norms, consumed by the Chebyshev init pass
+            cg->bnorm = out[2];
+        }
+    }
+}
+
+// A: p_new = z + beta*p_old (p_new = z on the first iteration), Ap = A p_new, partial p'Ap.
+template <typename T, bool JAC>
+__global__ void __launch_bounds__(kThreads) k_cg_A(int nx, int ny, const T *__restrict__ aP,
+                                                   const T *__restrict__ aE, const T *__restrict__ aN,
+                                                   const T *__restrict__ r, const T *__restrict__ zbuf,
+                                                   const T *__restrict__ p_old, T *__restrict__ p_new,
+                                                   T *__restrict__ Ap, CgDev *cg, double *partials,
+                                                   unsigned int *counter, double eps_curv) {
+    if (*(volatile int *)&cg->done) return;
+    const bool first = cg->first != 0;
+    const T beta = (T)cg->beta;
+    auto pval = [&](size_t k) -> T {
+        T z = JAC ? r[k] / aP[k] : zbuf[k];
+        return first ? z : z + beta * p_old[k];
+    };
+    Tiles Tl(nx, ny);
+    double red[1] = {0.0};
+    for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
+        int ix, iy;
+        Tl.cell(t, ix, iy);
+        if (ix >= nx || iy >= ny) continue;
+        size_t c = (size_t)ix + (size_t)iy * nx;
+        T pc = pval(c);
+        T apc = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, pc, pval);
+        p_new[c] = pc;
+        Ap[c] = apc;
+        red[0] += (double)pc * (double)apc;
+    }
+    double out[1];
+    if (grid_reduce<1, false>(red, partials, counter, out) && threadIdx.x == 0) {
+        const double pAp = out[0];
+        cg->pAp = pAp;
+        const double lim = eps_curv * cg->pNorm2;
+        if ((pAp <= lim && fabs(pAp) <= lim) || isnan(pAp)) {
+            cg->done = 1;
+            cg->status = SHK_BREAKDOWN;
+        } else {
+            cg->alpha = cg->gamma / pAp;
+        }
+    }
+}
+
+// B: x += alpha p, r -= alpha Ap; JAC: z = r/aP, partials r'z, r'r -> stop test.
+template <typename T, bool JAC>
+__global__ void __launch_bounds__(kThreads) k_cg_B(int n, const T *__restrict__ aP, const T *__restrict__ p,
+                                                   const T *__restrict__ Ap, T *__restrict__ x, T *__restrict__ r,
+                                                   CgDev *cg, double *partials, unsigned int *counter) {
+    if (*(volatile int *)&cg->done) return;
+    const T alpha = (T)cg->alpha;
+    double red[2] = {0.0, 0.0};
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        T xi = x[i] + alpha * p[i];
+        T ri = r[i] + (-alpha) * Ap[i];
+        x[i] = xi;
+        r[i] = ri;
+        if (JAC) {
+            T zi = ri / aP[i];
+            red[0] += (double)ri * (double)zi;
+            red[1] += (double)ri * (double)ri;
+        }
+    }
+    if (JAC) {
+        double out[2];
+        if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) cg_iter_finish(cg, out[0], out[1]);
+    }
+}
+
+// h = x + h (Krylov adds the warm start back at the end; then s.h .= x).
+__global__ void k_cg_finish(int n, const double *x, double *h) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) h[i] = x[i] + h[i];
+}
+
+// ---------------------------------------------------------------------------------------------
+// Chebyshev preconditioner ldiv! (src/preconditioner.jl:239-267): y ~ A^-1 x by the degree-d
+// Chebyshev semi-iteration on D^-1 A.  The reference's final matvec and residual update do not
+// reach y, so they are skipped (degree-1 matvecs per application, identical y).
+//   FIRST: pc = x/aP (and at neighbours), y = 0 + a1 pc, rc = pc - a1 (A pc)/aP
+//   MID  : pc' = rc + b_k pc, y += a_k pc', rc' = rc - a_k (A pc')/aP
+//   LAST : pc' = rc + b_k pc, y += a_k pc'  (+ CG dot r'z and stop test when inside CG)
+//   ONLY : degree 1: y = 0 + a1 x/aP
+// ---------------------------------------------------------------------------------------------
+enum ChebMode { CH_FIRST = 0, CH_MID = 1, CH_LAST = 2, CH_ONLY = 3 };
+enum ChebCg { CG_NONE = 0, CG_INIT = 1, CG_ITER = 2 };
+
+template <typename T, int MODE, int CGM>
+__global__ void __launch_bounds__(kThreads) k_cheb(int nx, int ny, const T *__restrict__ aP,
+                                                   const T *__restrict__ aE, const T *__restrict__ aN,
+                                                   const T *__restrict__ xin, const T *__restrict__ rc_old,
+                                                   const T *__restrict__ pc_old, T *__restrict__ rc_new,
+                                                   T *__restrict__ pc_new, T *__restrict__ y, int k,
+                                                   const ChebDev *ch, CgDev *cg, double *partials,
+                                                   unsigned int *counter) {
+    if (CGM != CG_NONE && *(volatile int *)&cg->done) return;
+    const T a = (T)ch->calpha[k];
+    const T bt = (T)ch->cbeta[k];
+    Tiles Tl(nx, ny);
+    double red[2] = {0.0, 0.0};
+    for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
+        int ix, iy;
+        Tl.cell(t, ix, iy);
+        if (ix >= nx || iy >= ny) continue;
+        size_t c = (size_t)ix + (size_t)iy * nx;
+        T yc;
+        if (MODE == CH_FIRST) {
+            auto pv = [&](size_t q) -> T { return xin[q] / aP[q]; };
+            T pc = pv(c);
+            yc = (T)0 + a * pc;
+            T apc = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, pc, pv) / aP[c];
+            pc_new[c] = pc;
+            rc_new[c] = pc - a * apc;
+            y[c] = yc;
+        } else if (MODE == CH_MID) {
+            auto pv = [&](size_t q) -> T { return rc_old[q] + bt * pc_old[q]; };
+            T pc = pv(c);
+            yc = y[c] + a * pc;
+            T apc = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, pc, pv) / aP[c];
+            pc_new[c] = pc;
+            rc_new[c] = rc_old[c] - a * apc;
+            y[c] = yc;
+        } else if (MODE == CH_LAST) {
+            T pc = rc_old[c] + bt * pc_old[c];
+            yc = y[c] + a * pc;
+            y[c] = yc;
+        } else {
+            yc = (T)0 + a * (xin[c] / aP[c]);
+            y[c] = yc;
+        }
+        if (CGM != CG_NONE && (MODE == CH_LAST || MODE == CH_ONLY)) {
+            T rcv = xin[c];
+            red[0] += (double)rcv * (double)yc;
+            red[1] += (double)rcv * (double)rcv;
+        }
+    }
+    if (CGM != CG_NONE && (MODE == CH_LAST || MODE == CH_ONLY)) {
+        double out[2];
+        if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
+            if (CGM == CG_INIT) cg_init_finish(cg, out[0], cg->rr, cg->bnorm);
+            else cg_iter_finish(cg, out[0], out[1]);
+        }
+    }
+}
+
+// Chebyshev per-step coefficients from the bounds (src/preconditioner.jl:241-263).
+__device__ void cheb_tables(ChebDev *ch) {
+    const double d_mid = (ch->lam_max + ch->lam_min) / 2;
+    const double c_rad = (ch->lam_max - ch->lam_min) / 2;
+    double alpha = 1.0 / d_mid;
+    ch->calpha[1] = alpha;
+    ch->cbeta[1] = 0.0;
+    double alpha_prev = alpha;
+    for (int k = 2; k <= kMaxChebDegree; k++) {
+        double t = c_rad * alpha_prev / 2;
+        double beta = t * t;
+        alpha = 1.0 / (d_mid - beta / alpha_prev);
+        ch->calpha[k] = alpha;
+        ch->cbeta[k] = beta;
+        alpha_prev = alpha;
+    }
+}
+
+__global__ void k_cheb_set_bounds(ChebDev *ch, double lmin, double lmax) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        ch->lam_min = lmin;
+        ch->lam_max = lmax;
+        cheb_tables(ch);
+    }
+}
+
+// Sturm count of eigenvalues below x for SymTridiagonal(d, e).
+__device__ int sturm(int m, const double *d, const double *e, double x) {
+    int cnt = 0;
+    double q = d[0] - x;
+    if (q < 0) cnt++;
+    for (int i = 1; i < m; i++) {
+        if (q == 0) q = DBL_EPSILON * (fabs(e[i - 1]) + DBL_MIN);
+        q = d[i] - x - e[i - 1] * e[i - 1] / q;
+        if (q < 0) cnt++;
+    }
+    return cnt;
+}
+
+// estimate_eigenvalue_bounds tail + update_chebyshev_bounds! validity/fallback
+// (src/preconditioner.jl:115-133, 219-230).  LAPACK's eigvals(SymTridiagonal) is replaced by
+// bisection on the Sturm count for the two extreme eigenvalues (the only ones used).
+__device__ void cheb_finish_estimate(ChebDev *ch, int m) {
+    double d[kMaxChebSteps], e[kMaxChebSteps];
+    d[0] = 1 / ch->alphas[0];
+    for (int k = 1; k < m; k++) d[k] = 1 / ch->alphas[k] + ch->betas[k - 1] / ch->alphas[k - 1];
+    for (int k = 0; k < m - 1; k++) e[k] = sqrt(ch->betas[k]) / ch->alphas[k];
+    bool finite = true;
+    for (int k = 0; k < m; k++) finite = finite && isfinite(d[k]);
+    for (int k = 0; k < m - 1; k++) finite = finite && isfinite(e[k]);
+    double lmin = __longlong_as_double(0x7ff8000000000000LL), lmax = lmin;
+    if (finite) {
+        double lo = INFINITY, hi = -INFINITY;
+        for (int i = 0; i < m; i++) {
+            double rad = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < m ? fabs(e[i]) : 0.0);
+            lo = fmin(lo, d[i] - rad);
+            hi = fmax(hi, d[i] + rad);
+        }
+        double span = fmax(fabs(lo), fabs(hi));
+        lo -= DBL_EPSILON * span + DBL_MIN;
+        hi += DBL_EPSILON * span + DBL_MIN;
+        double a = lo, b = hi;
+        for (int it = 0; it < 200; it++) {
+            double mid = 0.5 * (a + b);
+            if (mid == a || mid == b) break;
+            if (sturm(m, d, e, mid) >= 1) b = mid; else a = mid;
+        }
+        double rmin = 0.5 * (a + b);
+        a = lo;
+        b = hi;
+        for (int it = 0; it < 200; it++) {
+            double mid = 0.5 * (a + b);
+            if (mid == a || mid == b) break;
+            if (sturm(m, d, e, mid) >= m) b = mid; else a = mid;
+        }
+        double rmax = 0.5 * (a + b);
+        lmin = rmin * 0.9;
+        lmax = rmax * 1.1;
+    }
+    ch->est_min = lmin;
+    ch->est_max = lmax;
+    const bool ok = isfinite(lmin) && isfinite(lmax) && lmin > 0 && lmax > lmin;
+    ch->adopted = ok;
+    if (ok) {
+        ch->lam_min = lmin;
+        ch->lam_max = lmax;
+    }
+    cheb_tables(ch);
+}
+
+// Lanczos-from-CG estimate (src/preconditioner.jl:89-113), step k of nsteps:
+// A: p = rhs (k == 0) or r + beta_{k-1} p_old; Ap = (A p)/aP; alpha_k = gamma/p'Ap.
+template <bool FIRST>
+__global__ void __launch_bounds__(kThreads) k_est_A(int nx, int ny, const double *aP, const double *aE,
+                                                    const double *aN, const double *rhs, const double *r,
+                                                    const double *p_old, double *p_new, double *Ap, int k,
+                                                    int nsteps, ChebDev *ch, double *partials,
+                                                    unsigned int *counter) {
+    const double beta = FIRST ? 0.0 : ch->betas[k - 1];
+    auto pv = [&](size_t q) -> double { return FIRST ? rhs[q] : r[q] + beta * p_old[q]; };
+    Tiles Tl(nx, ny);
+    double red[2] = {0.0, 0.0};
+    for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
+        int ix, iy;
+        Tl.cell(t, ix, iy);
+        if (ix >= nx || iy >= ny) continue;
+        size_t c = (size_t)ix + (size_t)iy * nx;
+        double pc = pv(c);
+        double apc = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, pc, pv) / aP[c];
+        p_new[c] = pc;
+        Ap[c] = apc;
+        red[0] += pc * apc;
+        if (FIRST) red[1] += pc * pc;
+    }
+    double out[2];
+    if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
+        if (FIRST) ch->gamma = out[1];
+        ch->alphas[k] = ch->gamma / out[0];
+        if (k == nsteps - 1) cheb_finish_estimate(ch, nsteps);
+    }
+}
+
+// B: r = (rhs on k == 0) r - alpha_k Ap; beta_k = r'r/gamma.
+template <bool FIRST>
+__global__ void __launch_bounds__(kThreads) k_est_B(int n, const double *rhs, double *r, const double *Ap, int k,
+                                                    ChebDev *ch, double *partials, unsigned int *counter) {
+    const double a = ch->alphas[k];
+    double red[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double ri = (FIRST ? rhs[i] : r[i]) - a * Ap[i];
+        r[i] = ri;
+        red[0] += ri * ri;
+    }
+    double out[1];
+    if (grid_reduce<1, false>(red, partials, counter, out) && threadIdx.x == 0) {
+        ch->betas[k] = out[0] / ch->gamma;
+        ch->gamma = out[0];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Mixed precision helpers
+// ---------------------------------------------------------------------------------------------
+__global__ void k_to_float3(int n, const double *a, const double *b, const double *c, float *fa, float *fb,
+                            float *fc) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        fa[i] = (float)a[i];
+        fb[i] = (float)b[i];
+        fc[i] = (float)c[i];
+    }
+}
+
+// r32 = float(b - A h) with Float64 operator; partials ||r||^2, ||b||^2 (outer residual).
+__global__ void __launch_bounds__(kThreads) k_outer_residual(int nx, int ny, const double *aP, const double *aE,
+                                                             const double *aN, const double *h, const double *b,
+                                                             float *r32, DevScalars *dv, double *partials,
+                                                             unsigned int *counter) {
+    Tiles Tl(nx, ny);
+    double red[2] = {0.0, 0.0};
+    for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
+        int ix, iy;
+        Tl.cell(t, ix, iy);
+        if (ix >= nx || iy >= ny) continue;
+        size_t c = (size_t)ix + (size_t)iy * nx;
+        double ax = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, h[c], [&](size_t k) { return h[k]; });
+        double rc = b[c] - ax;
+        r32[c] = (float)rc;
+        red[0] += rc * rc;
+        red[1] += b[c] * b[c];
+    }
+    double out[2];
+    if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
+        dv->ref_rr = out[0];
+        dv->ref_bb = out[1];
+    }
+}
+
+__global__ void k_refine_update(int n, const float *d, double *h) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) h[i] += (double)d[i];
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host drivers
+// ---------------------------------------------------------------------------------------------
+static int flat_grid(Ctx *c, long long n) {
+    long long b = (n + kThreads - 1) / kThreads;
+    long long cap = (long long)c->grid_stencil;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+int read_scalars(Ctx *c) {
+    cudaError_t e = cudaMemcpyAsync(c->host_dev, c->dev, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return check_cuda(c, e, "read scalars");
+    return check_cuda(c, cudaStreamSynchronize(c->stream), "stream sync");
+}
+
+static int read_cg_flags(Ctx *c, CgDev *dst, const CgDev *src) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(CgDev), cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return check_cuda(c, e, "read cg scalars");
+    return check_cuda(c, cudaStreamSynchronize(c->stream), "stream sync");
+}
+
+int launch_matvec(Ctx *c, const double *x, double *y) {
+    k_matvec<double><<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->aP, c->aE, c->aN, x, y);
+    c->launches++;
+    return check_launch(c, "k_matvec");
+}
+
+int run_chebyshev_bounds(Ctx *c, int nsteps, const double *rhs) {
+    if (nsteps < 2 || nsteps > kMaxChebSteps) return fail(c, SHK_BAD_ARG, "chebyshev nsteps must be in [2, 64]");
+    const int nx = c->nx, ny = c->ny, n = nx * ny;
+    ChebDev *ch = &c->dev->cheb;
+    for (int k = 0; k < nsteps; k++) {
+        double *p_old = c->p[k & 1], *p_new = c->p[(k + 1) & 1];
+        if (k == 0)
+            k_est_A<true><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, c->aP, c->aE, c->aN, rhs, c->r, p_old,
+                                                                       p_new, c->Ap, k, nsteps, ch, c->partials,
+                                                                       c->counter);
+        else
+            k_est_A<false><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, c->aP, c->aE, c->aN, rhs, c->r, p_old,
+                                                                        p_new, c->Ap, k, nsteps, ch, c->partials,
+                                                                        c->counter);
+        c->launches++;
+        if (k < nsteps - 1) {
+            if (k == 0)
+                k_est_B<true><<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, rhs, c->r, c->Ap, k, ch, c->partials,
+                                                                            c->counter);
+            else
+                k_est_B<false><<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, rhs, c->r, c->Ap, k, ch, c->partials,
+                                                                             c->counter);
+            c->launches++;
+        }
+    }
+    return check_launch(c, "chebyshev bounds");
+}
+
+// Enqueue one Chebyshev application y = M^-1 xin (degree deg) in precision T.
+template <typename T, int CGM>
+static void enqueue_cheb(Ctx *c, int deg, const T *aP, const T *aE, const T *aN, const T *xin, T **cr, T **cp, T *y,
+                         CgDev *cg) {
+    const int nx = c->nx, ny = c->ny;
+    const ChebDev *ch = &c->dev->cheb;
+    if (deg == 1) {
+        k_cheb<T, CH_ONLY, CGM><<<c->grid_stencil, kThreads, 0, c->stream>>>(
+            nx, ny, aP, aE, aN, xin, nullptr, nullptr, nullptr, nullptr, y, 1, ch, cg, c->partials, c->counter);
+        c->launches++;
+        return;
+    }
+    k_cheb<T, CH_FIRST, CG_NONE == CGM ? CG_NONE : CGM><<<c->grid_stencil, kThreads, 0, c->stream>>>(
+        nx, ny, aP, aE, aN, xin, nullptr, nullptr, cr[0], cp[0], y, 1, ch, cg, c->partials, c->counter);
+    c->launches++;
+    int cur = 0;
+    for (int k = 2; k < deg; k++) {
+        k_cheb<T, CH_MID, CGM><<<c->grid_stencil, kThreads, 0, c->stream>>>(
+            nx, ny, aP, aE, aN, xin, cr[cur], cp[cur], cr[cur ^ 1], cp[cur ^ 1], y, k, ch, cg, c->partials, c->counter);
+        c->launches++;
+        cur ^= 1;
+    }
+    k_cheb<T, CH_LAST, CGM><<<c->grid_stencil, kThreads, 0, c->stream>>>(
+        nx, ny, aP, aE, aN, xin, cr[cur], cp[cur], nullptr, nullptr, y, deg, ch, cg, c->partials, c->counter);
+    c->launches++;
+}
+
+int cheb_set_bounds(Ctx *c, double lmin, double lmax) {
+    k_cheb_set_bounds<<<1, 32, 0, c->stream>>>(&c->dev->cheb, lmin, lmax);
+    c->launches++;
+    return check_launch(c, "set chebyshev bounds");
+}
+
+int launch_chebyshev_apply_standalone(Ctx *c, int degree, const double *x, double *y) {
+    if (degree < 1 || degree > kMaxChebDegree) return fail(c, SHK_BAD_ARG, "chebyshev degree must be in [1, 32]");
+    enqueue_cheb<double, CG_NONE>(c, degree, c->aP, c->aE, c->aN, x, c->cr, c->cp, y, nullptr);
+    return check_launch(c, "chebyshev apply");
+}
+
+static CgDev make_cg_init(const shk_cg_opts *o, long long n, bool inner, double inner_rtol) {
+    CgDev g;
+    memset(&g, 0, sizeof(g));
+    g.atol = inner ? 0.0 : o->atol;
+    g.rtol = inner ? inner_rtol : o->rtol;
+    g.itmax = o->itmax > 0 ? o->itmax : 2 * n;
+    g.stop_rule = inner ? SHK_STOP_RELRES : o->stop_rule;
+    g.done = 0;
+    g.status = SHK_OK;
+    g.first = 1;
+    return g;
+}
+
+// One preconditioned CG solve in precision T on system (aP, aE, aN), b -> x (correction from x0).
+// x0 (Float64, may be null) is the warm start used only for the initial residual.
+template <typename T>
+static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T *aP, const T *aE, const T *aN,
+                   const double *x0, const T *b, T *x, T *r, T *z, T **p, T *Ap, T **cr, T **cp, long *iters_out) {
+    const int nx = c->nx, ny = c->ny, n = nx * ny;
+    const bool jac = o->precond == SHK_PRECOND_JACOBI;
+    const int deg = o->cheb_degree;
+    const double eps_curv = sizeof(T) == 8 ? DBL_EPSILON : (double)FLT_EPSILON;
+    cudaError_t e = cudaMemcpyAsync(cgd, cgh, sizeof(CgDev), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return check_cuda(c, e, "cg scalars upload");
+    if (jac) {
+        k_cg_init<T, true><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, aP, aE, aN, x0, b, r, x, cgd, c->partials,
+                                                                       c->counter);
+        c->launches++;
+    } else {
+        k_cg_init<T, false><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, aP, aE, aN, x0, b, r, x, cgd,
+                                                                        c->partials, c->counter);
+        c->launches++;
+        enqueue_cheb<T, CG_INIT>(c, deg, aP, aE, aN, r, cr, cp, z, cgd);
+    }
+    int rc = check_launch(c, "cg init");
+    if (rc) return rc;
+    long long enq = 0;
+    int batch = 8;
+    const int batch_max = 256;
+    for (;;) {
+        if ((rc = read_cg_flags(c, cgh, cgd))) return rc;
+        if (cgh->done) break;
+        for (int b2 = 0; b2 < batch; b2++, enq++) {
+            T *p_old = p[enq & 1], *p_new = p[(enq + 1) & 1];
+            if (jac) {
+                k_cg_A<T, true><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, aP, aE, aN, r, nullptr, p_old, p_new,
+                                                                            Ap, cgd, c->partials, c->counter, eps_curv);
+                k_cg_B<T, true><<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd, c->partials,
+                                                                            c->counter);
+                c->launches += 2;
+            } else {
+                k_cg_A<T, false><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, aP, aE, aN, r, z, p_old, p_new, Ap,
+                                                                             cgd, c->partials, c->counter, eps_curv);
+                k_cg_B<T, false><<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd, c->partials,
+                                                                             c->counter);
+                c->launches += 2;
+                enqueue_cheb<T, CG_ITER>(c, deg, aP, aE, aN, r, cr, cp, z, cgd);
+            }
+        }
+        if ((rc = check_launch(c, "cg iterations"))) return rc;
+        if (batch < batch_max) batch *= 2;
+        if (cgh->iter > cgh->itmax + 4) return fail(c, SHK_CUDA_ERROR, "cg iteration accounting overran itmax");
+    }
+    if (iters_out) *iters_out = (long)cgh->iter;
+    return SHK_OK;
+}
+
+int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
+    const int nx = c->nx, ny = c->ny, n = nx * ny;
+    if (o->precond != SHK_PRECOND_JACOBI && o->precond != SHK_PRECOND_CHEBYSHEV)
+        return fail(c, SHK_BAD_ARG, "unknown preconditioner");
+    if (o->precond == SHK_PRECOND_CHEBYSHEV) {
+        if (o->cheb_degree < 1 || o->cheb_degree > kMaxChebDegree)
+            return fail(c, SHK_BAD_ARG, "chebyshev_degree must be in [1, 32]");
+        // _cg_precond! refreshes the bounds from this solve's rhs (src/linear_solver.jl:853-856)
+        int rc = run_chebyshev_bounds(c, o->cheb_nsteps, c->rhs);
+        if (rc) return rc;
+    }
+    shk_cg_stats s;
+    memset(&s, 0, sizeof(s));
+    if (o->precision == SHK_FP64) {
+        CgDev *cgh = &c->host_dev->cg;
+        *cgh = make_cg_init(o, n, false, 0.0);
+        long it = 0;
+        int rc = cg_core<double>(c, o, &c->dev->cg, cgh, c->aP, c->aE, c->aN, c->st.h, c->rhs, c->x, c->r, c->z, c->p,
+                                 c->Ap, c->cr, c->cp, &it);
+        if (rc) return rc;
+        k_cg_finish<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->x, c->st.h);
+        c->launches++;
+        if ((rc = check_launch(c, "cg finish"))) return rc;
+        if ((rc = read_scalars(c))) return rc;
+        const CgDev &g = c->host_dev->cg;
+        s.niter = (long)g.iter;
+        s.status = g.status;
+        s.rnorm0 = g.rnorm0;
+        s.rnorm = g.rnorm;
+    } else if (o->precision == SHK_MIXED) {
+        // Float32 stencil + CG inside Float64 iterative refinement: h <- h + A32^-1 (b - A64 h).
+        k_to_float3<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->aP, c->aE, c->aN, c->aP32, c->aE32, c->aN32);
+        c->launches++;
+        const double inner_rtol = o->inner_rtol > 0 ? o->inner_rtol : 1e-3;
+        const int max_refine = o->max_refine > 0 ? o->max_refine : 50;
+        long total = 0;
+        int refine = 0;
+        int status = SHK_NOT_CONVERGED;
+        for (;;) {
+            k_outer_residual<<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, c->aP, c->aE, c->aN, c->st.h, c->rhs,
+                                                                         c->b32, c->dev, c->partials, c->counter);
+            c->launches++;
+            int rc = read_scalars(c);
+            if (rc) return rc;
+            const double rn = sqrt(c->host_dev->ref_rr), bn = sqrt(c->host_dev->ref_bb);
+            if (refine == 0) s.rnorm0 = rn;
+            s.rnorm = rn;
+            if (isnan(rn)) {
+                status = SHK_BREAKDOWN;
+                break;
+            }
+            if (rn <= o->rtol * bn || rn == 0.0) {
+                status = SHK_OK;
+                break;
+            }
+            if (refine >= max_refine || total >= (o->itmax > 0 ? o->itmax : 2L * n)) break;
+            CgDev *cgh = &c->host_dev->cg_in;
+            *cgh = make_cg_init(o, n, true, inner_rtol);
+            long it = 0;
+            rc = cg_core<float>(c, o, &c->dev->cg_in, cgh, c->aP32, c->aE32, c->aN32, nullptr, c->b32, c->x32, c->r32,
+                                c->z32, c->p32, c->Ap32, c->cr32, c->cp32, &it);
+            if (rc) return rc;
+            if (cgh->status == SHK_BREAKDOWN) {
+                status = SHK_BREAKDOWN;
+                break;
+            }
+            k_refine_update<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->x32, c->st.h);
+            c->launches++;
+            if ((rc = check_launch(c, "refine update"))) return rc;
+            total += it;
+            refine++;
+        }
+        s.niter = total;
+        s.status = status;
+        s.refinements = refine;
+    } else {
+        return fail(c, SHK_BAD_ARG, "unknown precision");
+    }
+    if ((o->precond == SHK_PRECOND_CHEBYSHEV)) {
+        if (o->precision != SHK_FP64) {
+            int rc = read_scalars(c);
+            if (rc) return rc;
+        }
+        s.lambda_min = c->host_dev->cheb.lam_min;
+        s.lambda_max = c->host_dev->cheb.lam_max;
+        s.bounds_valid = c->host_dev->cheb.adopted;
+    }
+    if (st) *st = s;
+    return SHK_OK;
+}
+
+} // namespace shk

@@ -1,0 +1,263 @@
+"""Simulation / run! / step! and set_initial_conditions! mirroring Shakti.jl (src/simulation.jl,
+src/run.jl, src/initial_conditions.jl), driving libshakti_b200."""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import _lib
+from .model import (Arithmetic, Harmonic, ModelParameters, PrescribedSlidingLaw, State, Grid, AbstractMeltInput,
+                    AbstractSlidingLaw)
+from .solvers import (_Context, AbstractLinearSolver, CGIterativeSolver, PicardSolver, solve_parabolic_linear_system)
+
+
+# ---------------------------------------------------------------------------------------------
+# Schemes (src/simulation.jl:9-56, src/melt_rate.jl:19-33, src/gap_height.jl:22-43)
+# ---------------------------------------------------------------------------------------------
+class AbstractHeadScheme:
+    pass
+
+
+class EllipticHeadScheme(AbstractHeadScheme):
+    def __init__(self, ps: PicardSolver):
+        self.ps = ps
+
+
+class ParabolicHeadScheme(AbstractHeadScheme):
+    def __init__(self, ls: AbstractLinearSolver):
+        self.ls = ls
+
+
+class AbstractGapScheme:
+    code = -1
+
+
+class ExplicitGapScheme(AbstractGapScheme):
+    code = 0
+
+
+class ImplicitGapScheme(AbstractGapScheme):
+    code = 1
+
+
+class AbstractSensibleHeatScheme:
+    pass
+
+
+class WithSensibleHeat(AbstractSensibleHeatScheme):
+    pass
+
+
+class NoSensibleHeat(AbstractSensibleHeatScheme):
+    pass
+
+
+class AbstractOpenBySlidingScheme:
+    pass
+
+
+class WithOpenBySliding(AbstractOpenBySlidingScheme):
+    pass
+
+
+class NoOpenBySliding(AbstractOpenBySlidingScheme):
+    pass
+
+
+# ---------------------------------------------------------------------------------------------
+# Observers (src/observer.jl): NoObserver and the in-memory LiveObserver.  File writers (NetCDF,
+# HDF5, JLD2, CSV) are host I/O outside the solve path and are not provided.
+# ---------------------------------------------------------------------------------------------
+class AbstractObserver:
+    def prepare(self, state):
+        pass
+
+    def observe(self, state, t, total_time):
+        pass
+
+    def finalize(self, state):
+        pass
+
+
+class NoObserver(AbstractObserver):
+    pass
+
+
+class LiveObserver(AbstractObserver):
+    def __init__(self, tracked_obs, tracked_times):
+        self.tracked_obs = list(tracked_obs)
+        self.tracked_times = set(int(t) for t in tracked_times)
+        self.data = {name: [] for name in self.tracked_obs}
+        self.times = []
+
+    def observe(self, state, t, total_time):
+        if t in self.tracked_times:
+            self.times.append(total_time)
+            host = state.to_numpy(self.tracked_obs)
+            for name in self.tracked_obs:
+                self.data[name].append(host[name])
+
+
+class Simulation:
+    """Simulation(grid, state, tsteps, dt, p, gap_scheme_choice, tracked_obs, mi, sl; ps, ls,
+    which_observer, which_file_writer, tracked_times, path, k_face_choice, verbose)
+    (src/simulation.jl:105-184)."""
+
+    def __init__(self, grid: Grid, state: State, tsteps: int, dt: float, p: ModelParameters, gap_scheme_choice: str,
+                 tracked_obs, mi: AbstractMeltInput, sl: AbstractSlidingLaw, *, ps: PicardSolver | None = None,
+                 ls: AbstractLinearSolver | None = None, which_observer=None, which_file_writer=None,
+                 tracked_times=None, path=None, k_face_choice: str = "arithmetic", verbose: bool = False):
+        for name in tracked_obs:
+            if not hasattr(state, "lambda_" if name == "lambda" else name):
+                raise ValueError(f'Unknown tracked observable: "{name}" is not a field of State')
+        if p.e_v == 0:
+            if ps is None:
+                raise ValueError("ps (a PicardSolver) must be provided when p.e_v == 0 (elliptic head scheme)")
+            self.hs = EllipticHeadScheme(ps)
+        else:
+            if ls is None:
+                raise ValueError("ls (an AbstractLinearSolver) must be provided when p.e_v != 0 (parabolic head scheme)")
+            self.hs = ParabolicHeadScheme(ls)
+        if gap_scheme_choice == "explicit":
+            self.gs = ExplicitGapScheme()
+        elif gap_scheme_choice == "implicit":
+            self.gs = ImplicitGapScheme()
+        else:
+            raise ValueError(f'Unknown gap_scheme_choice: "{gap_scheme_choice}" (expected "explicit" or "implicit")')
+        self.shs = NoSensibleHeat() if (p.ct == 0 or p.cw == 0) else WithSensibleHeat()
+        self.oss = NoOpenBySliding() if p.br == 0 else WithOpenBySliding()
+        if k_face_choice == "arithmetic":
+            self.kfs = Arithmetic()
+        elif k_face_choice == "harmonic":
+            self.kfs = Harmonic()
+        else:
+            raise ValueError(f'Unknown k_face_choice: "{k_face_choice}" (expected "arithmetic" or "harmonic")')
+        if len(tracked_obs) == 0:
+            self.observer = NoObserver()
+        elif which_observer is None:
+            raise ValueError('which_observer should be specified as "IO" or "Live" when tracked_obs is not empty.')
+        elif which_observer == "IO":
+            raise NotImplementedError("IOObserver (NetCDF/HDF5/JLD2/CSV file writers) is host I/O outside the "
+                                      "solve path and is not provided by this library; use \"Live\".")
+        elif which_observer == "Live":
+            if tracked_times is None:
+                raise ValueError('tracked_times should be specified when which_observer is "Live".')
+            self.observer = LiveObserver(tracked_obs, tracked_times)
+        else:
+            raise ValueError(f'Unknown which_observer: "{which_observer}" (expected "IO" or "Live")')
+        self.grid, self.state, self.tsteps, self.dt, self.p = grid, state, int(tsteps), float(dt), p
+        self.mi, self.sl, self.verbose = mi, sl, bool(verbose)
+        self.total_time = 0.0
+        self.step_stats = []
+
+    @property
+    def ls(self) -> CGIterativeSolver:
+        return self.hs.ps.ls if isinstance(self.hs, EllipticHeadScheme) else self.hs.ls
+
+    def ctx(self) -> _Context:
+        return self.ls.ctx.bind(self.state, self.p, self.sl, self.kfs, self.gs.code)
+
+
+def picard_status(hs: AbstractHeadScheme):
+    """src/run.jl:64-65"""
+    if isinstance(hs, EllipticHeadScheme):
+        return hs.ps.converged, hs.ps.last_iter
+    return None, None
+
+
+def update_ieb(sim: Simulation) -> None:
+    """update_ieb!(sim.mi, sim.state, sim.total_time) (src/melt_input.jl:30, 86-94)."""
+    ctx = sim.ctx()
+    mi = sim.mi.struct()
+    _lib.check(ctx.h, ctx.L.shk_update_ieb(ctx.h, C.byref(mi), float(sim.total_time)))
+
+
+def step_h(sim: Simulation) -> None:
+    """src/run.jl:96-108"""
+    if isinstance(sim.hs, EllipticHeadScheme):
+        ps = sim.hs.ps
+        ctx = sim.ctx()
+        st = _lib.shk_picard_stats()
+        po, o = ps.opts(), ps.ls.opts()
+        rc = ctx.L.shk_picard_solve(ctx.h, C.byref(po), C.byref(o), C.byref(st))
+        _lib.check(ctx.h, rc, allow=(_lib.OK, _lib.NOT_CONVERGED))
+        ps._record(st)
+    else:
+        ls = sim.hs.ls
+        ctx = sim.ctx()
+        st = _lib.shk_cg_stats()
+        o = ls.opts()
+        rc = ctx.L.shk_parabolic_step(ctx.h, float(sim.dt), C.byref(o), C.byref(st))
+        _lib.check(ctx.h, rc, allow=(_lib.OK, _lib.NOT_CONVERGED, _lib.BREAKDOWN))
+        ls._record(st)
+
+
+def step_b(sim: Simulation) -> None:
+    """step_b! (src/run.jl:154-164)"""
+    ctx = sim.ctx()
+    _lib.check(ctx.h, ctx.L.shk_step_b(ctx.h, float(sim.dt)))
+
+
+def step(sim: Simulation) -> None:
+    """step! (src/run.jl:82-88)"""
+    update_ieb(sim)
+    step_h(sim)
+    step_b(sim)
+
+
+def run(sim: Simulation) -> None:
+    """run!(sim) (src/run.jl:21-63) without checkpointing."""
+    sim.total_time = 0.0
+    sim.observer.prepare(sim.state)
+    sim.observer.observe(sim.state, 0, sim.total_time)
+    sim.step_stats = []
+    for t in range(1, sim.tsteps + 1):
+        t0 = time.perf_counter()
+        step(sim)
+        sim.total_time += sim.dt
+        sim.observer.observe(sim.state, t, sim.total_time)
+        conv, last = picard_status(sim.hs)
+        sim.step_stats.append(dict(converged=conv, last_iter=last,
+                                   cg_iters=(sim.hs.ps.cg_iters_total if isinstance(sim.hs, EllipticHeadScheme)
+                                             else sim.hs.ls.stats.niter)))
+        if sim.verbose:
+            import torch
+            torch.cuda.synchronize()
+            print(f"{t} / {sim.tsteps} completed in {time.perf_counter() - t0:.4f}s. "
+                  f"Picard converged: {conv} in {last} iterations", flush=True)
+    sim.observer.finalize(sim.state)
+
+
+# ---------------------------------------------------------------------------------------------
+# set_initial_conditions! (src/initial_conditions.jl:14-125)
+# ---------------------------------------------------------------------------------------------
+def _copy_in(dst, arr):
+    import torch
+    a = np.asarray(arr, dtype=np.float64)
+    if a.shape != tuple(dst.shape):
+        raise ValueError(f"input shape {a.shape} does not match field shape {tuple(dst.shape)}")
+    dst.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+
+
+def set_initial_conditions(s: State, g: Grid, p: ModelParameters, sl: AbstractSlidingLaw, mask, A_visc, zb, zs, b,
+                           G, ub_x, ub_y, ieb, taub_x, taub_y, ctx: _Context | None = None) -> State:
+    """Copy the raw inputs into the device State, then derive every field on the GPU in the
+    reference's order.  The taub inputs are used only by PrescribedSlidingLaw (initialize_taub!)."""
+    for name, arr in (("mask", mask), ("A_visc", A_visc), ("zb", zb), ("zs", zs), ("b", b), ("G", G),
+                      ("ub_x", ub_x), ("ub_y", ub_y), ("ieb", ieb)):
+        _copy_in(s[name], arr)
+    if isinstance(sl, PrescribedSlidingLaw):
+        _copy_in(s.taub_x, taub_x)
+        _copy_in(s.taub_y, taub_y)
+    own = ctx is None
+    ctx = ctx or _Context(g)
+    try:
+        ctx.bind(s, p, sl)
+        _lib.check(ctx.h, ctx.L.shk_set_initial_conditions(ctx.h))
+    finally:
+        if own:
+            ctx.close()
+    return s
