@@ -117,12 +117,13 @@ def _paint_blobs(mask: np.ndarray, rng, frac: float, rmin: int, rmax: int) -> No
         k += 1
 
 
-def seasonal(nx: int, lx: float, seed: int = 20262, n_moulins: int = 64, blob_frac: float = 0.10) -> Workload:
+def seasonal(nx: int, lx: float, seed: int = 20262, n_moulins: int = 64, blob_frac: float = 0.10,
+             C: float = 1e4, moulin_radius_m: float = 0.0, q_range=(1.0, 20.0)) -> Workload:
     """Mixed-precision workload: the plain generator plus LAND / OTHER_BASIN blobs covering
     `blob_frac` of the cells, a seasonal sinusoid (period 1 year, peak 5e-8 m/s, expressed as a
     SeasonalMeltInput window covering the whole year) and `n_moulins` point sources of 1-20 m^3/s
     each spread as Q/(dx dy) over one GROUNDED cell."""
-    w = plain(nx, lx, seed=seed)
+    w = plain(nx, lx, seed=seed, C=C)
     rng = np.random.default_rng(seed + 1)
     mask = w.inputs["mask"]
     rmax = max(2, nx // 100)
@@ -130,9 +131,16 @@ def seasonal(nx: int, lx: float, seed: int = 20262, n_moulins: int = 64, blob_fr
     base = _zeros(nx, nx)
     grounded = np.argwhere(mask == GROUNDED)
     pick = grounded[rng.choice(len(grounded), size=n_moulins, replace=False)]
-    Q = rng.uniform(1.0, 20.0, size=n_moulins)
+    Q = rng.uniform(q_range[0], q_range[1], size=n_moulins)
+    r = int(round(moulin_radius_m / w.dx))
     for (i, j), q in zip(pick, Q):
-        base[i, j] = q / (w.dx * w.dy)
+        if r <= 0:
+            base[i, j] = q / (w.dx * w.dy)
+            continue
+        ii, jj = np.meshgrid(np.arange(max(i - r, 0), min(i + r + 1, nx)),
+                             np.arange(max(j - r, 0), min(j + r + 1, nx)), indexing="ij")
+        disk = ((ii - i) ** 2 + (jj - j) ** 2 <= r * r) & (mask[ii, jj] == GROUNDED)
+        base[ii[disk], jj[disk]] += q / (int(disk.sum()) * w.dx * w.dy)
     peak_ma = 5e-8 * SECONDS_PER_YEAR
     # i(yf) = offset - amplitude*cos(2 pi yf) with offset = peak/2, amplitude = -peak/2: peak at yf=0
     w.melt = dict(t_start=0.0, t_end=1.0, amplitude=-peak_ma / 2, offset=peak_ma / 2, i_min=0.0,
@@ -143,8 +151,38 @@ def seasonal(nx: int, lx: float, seed: int = 20262, n_moulins: int = 64, blob_fr
     return w
 
 
+# The 4096^2 mixed-precision workload uses two settings that keep every timestep well-posed on
+# the reference algorithm itself (demonstrated with the CPU restatement):
+#  - C = 0.25, the reference fixture's regularized-Coulomb coefficient.  With C = 1e4 the
+#    regularized-Coulomb stress reaches ~1e10 Pa, shear heating ~1e4 W/m^2, b grows ~5 cm per
+#    30-minute step, Re ~ 6e5, and Picard stops converging by the third step.
+#  - b_min = 0.002 m, b_max = 1 m: the cap the reference's ModelParameters docstring recommends for
+#    the b -> K -> q -> mdot runaway where N approaches or drops below zero; without it the 1-20
+#    m^3/s single-cell moulins drive N to about -3e7 Pa, the implicit gap denominator turns
+#    negative and b runs away within two steps.
+SEASONAL_PARAMS = dict(b_min=0.002, b_max=1.0)
+SEASONAL_C = 0.25
+
+
+def seasonal_bench(nx: int, lx: float, seed: int = 20262) -> Workload:
+    w = seasonal(nx, lx, seed=seed, C=SEASONAL_C)
+    w.params = dict(SEASONAL_PARAMS)
+    return w
+
+
 def seasonal4096() -> Workload:
-    return seasonal(4096, 200e3)
+    return seasonal_bench(4096, 200e3)
 
 
-WORKLOADS = {"fixture6": fixture6, "plain64": plain64, "plain1024": plain1024, "seasonal4096": seasonal4096}
+def seasonal2048() -> Workload:
+    """Same physics and resolution (dx ~ 49 m) as seasonal4096 on a 100 km domain."""
+    return seasonal_bench(2048, 100e3)
+
+
+def seasonal1024() -> Workload:
+    """Same physics and resolution (dx ~ 49 m) as seasonal4096 on a 50 km domain."""
+    return seasonal_bench(1024, 50e3)
+
+
+WORKLOADS = {"fixture6": fixture6, "plain64": plain64, "plain1024": plain1024, "seasonal1024": seasonal1024, "seasonal2048": seasonal2048,
+             "seasonal4096": seasonal4096}

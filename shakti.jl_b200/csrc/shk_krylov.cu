@@ -638,7 +638,10 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
         }
         if ((rc = check_launch(c, "cg iterations"))) return rc;
         if (batch < batch_max) batch *= 2;
-        if (cgh->iter > cgh->itmax + 4) return fail(c, SHK_CUDA_ERROR, "cg iteration accounting overran itmax");
+        // The device stops at itmax; launches beyond it are no-ops.  If the device-side counters
+        // ever stopped advancing, this bound still ends the loop.
+        if (cgh->iter > cgh->itmax + 4 || enq > cgh->itmax + 2LL * batch_max + 8)
+            return fail(c, SHK_CUDA_ERROR, "cg iteration accounting overran itmax");
     }
     if (iters_out) *iters_out = (long)cgh->iter;
     return SHK_OK;
