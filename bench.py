@@ -157,7 +157,7 @@ def make_sim(shk, w, args, state=None):
     shk.set_initial_conditions(s, g, p, sl, **w.inputs)
     kw = dict(stop_rule="relres", rtol=1e-8, atol=0.0)
     if args.form == "mixed":
-        kw.update(precision="mixed", inner_rtol=1e-3)
+        kw.update(precision="mixed", inner_rtol=1e-2)
     cheb = 4 if args.precond == "chebyshev" else None
     ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, chebyshev_degree=cheb, **kw)
     ps = shk.PicardSolver(500, 1e-6, ls, g)

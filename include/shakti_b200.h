@@ -95,7 +95,9 @@ typedef struct {
  *   stop_rule SHK_STOP_RELRES: ||b - A x||_2 <= rtol*||b||_2 (the recursive residual)
  *   precision SHK_FP64: every vector and coefficient in Float64
  *   precision SHK_MIXED: Float32 stencil and CG inside Float64 iterative refinement; the outer
- *     residual, the refinement update and the stopping test stay Float64 (rel-res rule only). */
+ *     residual, the refinement update and the stopping test stay Float64 (rel-res rule only).
+ *     Each refinement replaces the Float32 residual by the Float64 true residual b - A h and
+ *     continues the CG direction rather than restarting it. */
 enum { SHK_PRECOND_JACOBI = 0, SHK_PRECOND_CHEBYSHEV = 1 };
 enum { SHK_STOP_KRYLOV = 0, SHK_STOP_RELRES = 1 };
 enum { SHK_FP64 = 0, SHK_MIXED = 1 };
@@ -105,10 +107,12 @@ typedef struct {
     int cheb_nsteps;
     int stop_rule;
     int precision;
-    int max_refine;     /* mixed precision: cap on outer refinement steps (<=0: 50)          */
+    int max_refine;     /* mixed precision: cap on outer refinement steps (<=0: 200)         */
     double atol, rtol;  /* Krylov defaults: sqrt(eps(Float64)) both                          */
-    double inner_rtol;  /* mixed precision: inner Float32 CG relative tolerance (<=0: 1e-3)  */
+    double inner_rtol;  /* mixed precision: Float32 residual drop per refinement (<=0: 1e-2) */
     long itmax;         /* <= 0: 2*nx*ny, Krylov's default                                   */
+    long inner_itmax;   /* mixed precision: cap on Float32 iterations between two Float64
+                           residual replacements (<= 0: max(200, (nx+ny)/2))                   */
 } shk_cg_opts;
 
 typedef struct {

@@ -46,7 +46,7 @@ class shk_melt_input(C.Structure):
 class shk_cg_opts(C.Structure):
     _fields_ = [("precond", C.c_int), ("cheb_degree", C.c_int), ("cheb_nsteps", C.c_int), ("stop_rule", C.c_int),
                 ("precision", C.c_int), ("max_refine", C.c_int), ("atol", C.c_double), ("rtol", C.c_double),
-                ("inner_rtol", C.c_double), ("itmax", C.c_long)]
+                ("inner_rtol", C.c_double), ("itmax", C.c_long), ("inner_itmax", C.c_long)]
 
 
 class shk_cg_stats(C.Structure):
@@ -145,7 +145,7 @@ def cuda_stream_handle():
 def default_cg_opts(**kw) -> shk_cg_opts:
     sq = math.sqrt(2.220446049250313e-16)
     o = shk_cg_opts(precond=0, cheb_degree=4, cheb_nsteps=15, stop_rule=0, precision=0, max_refine=0,
-                    atol=sq, rtol=sq, inner_rtol=0.0, itmax=0)
+                    atol=sq, rtol=sq, inner_rtol=0.0, itmax=0, inner_itmax=0)
     for k, v in kw.items():
         setattr(o, k, v)
     return o

@@ -63,8 +63,8 @@ static int ctx_alloc(Ctx *c) {
     size_t o_x = carve(dN), o_r = carve(dN), o_z = carve(dN), o_p0 = carve(dN), o_p1 = carve(dN), o_Ap = carve(dN);
     size_t o_hprev = carve(dN);
     size_t o_cr0 = carve(dN), o_cr1 = carve(dN), o_cp0 = carve(dN), o_cp1 = carve(dN);
-    size_t o_f[14];
-    for (int i = 0; i < 14; i++) o_f[i] = carve(fN);
+    size_t o_f[15];
+    for (int i = 0; i < 15; i++) o_f[i] = carve(fN);
     size_t o_part = carve((size_t)kMaxRedValues * c->max_blocks * sizeof(double));
     size_t o_cnt = carve(64);
     size_t o_dev = carve(sizeof(DevScalars));
@@ -80,9 +80,9 @@ static int ctx_alloc(Ctx *c) {
     c->h_prev = (double *)(b + o_hprev);
     c->cr[0] = (double *)(b + o_cr0); c->cr[1] = (double *)(b + o_cr1);
     c->cp[0] = (double *)(b + o_cp0); c->cp[1] = (double *)(b + o_cp1);
-    float **fl[14] = {&c->aP32, &c->aE32, &c->aN32, &c->b32, &c->x32, &c->r32, &c->z32, &c->p32[0], &c->p32[1],
-                      &c->Ap32, &c->cr32[0], &c->cr32[1], &c->cp32[0], &c->cp32[1]};
-    for (int i = 0; i < 14; i++) *fl[i] = (float *)(b + o_f[i]);
+    float **fl[15] = {&c->aP32, &c->aE32, &c->aN32, &c->b32, &c->x32, &c->r32, &c->z32, &c->p32[0], &c->p32[1],
+                      &c->Ap32, &c->cr32[0], &c->cr32[1], &c->cp32[0], &c->cp32[1], &c->dP32};
+    for (int i = 0; i < 15; i++) *fl[i] = (float *)(b + o_f[i]);
     c->partials = (double *)(b + o_part);
     c->counter = (unsigned int *)(b + o_cnt);
     c->dev = (DevScalars *)(b + o_dev);
@@ -159,7 +159,18 @@ SHK_API int shk_create(int nx, int ny, double lx, double ly, void *stream, void 
     if (g > tiles) g = tiles;
     if (g < 1) g = 1;
     c->grid_stencil = (int)g;
-    c->max_blocks = c->grid_stencil;
+    // Row-marching tiles: kMarchX columns by march_th rows; the height is chosen so that the grid
+    // offers about 12 blocks per SM (one resident wave), between 8 and 64 rows.
+    {
+        const long long tiles_x = (nx + kMarchX - 1) / kMarchX;
+        long long th = (long long)ny * tiles_x / ((long long)c->num_sms * 12);
+        if (th > 64) th = 64;
+        if (th < 8) th = 8;
+        c->march_th = (int)th;
+        c->march_blocks = (int)(tiles_x * ((ny + th - 1) / th));
+    }
+    c->max_blocks = c->grid_stencil > c->march_blocks ? c->grid_stencil : c->march_blocks;
+    if (c->max_blocks < c->num_sms * 8) c->max_blocks = c->num_sms * 8;
     rc = ctx_alloc(c);
     if (rc) {
         if (c->arena) cudaFree(c->arena);

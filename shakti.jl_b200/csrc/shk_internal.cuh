@@ -32,6 +32,9 @@ constexpr int kTX = 32;             // tile width (cells along x, one warp)
 constexpr int kTY = 8;              // tile height
 constexpr int kThreads = kTX * kTY; // 256 threads per block
 constexpr int kMaxRedValues = 4;
+constexpr int kMarchX = 128;        // columns per block of the row-marching stencil kernels
+constexpr int kUnrollB = 2;
+constexpr int kRingRows = 6;        // shared-memory ring depth of the row-marching kernels         // 16-byte vectors in flight per thread in streaming kernels
 constexpr int kMaxChebSteps = 64;   // chebyshev_nsteps_estimate cap
 constexpr int kMaxChebDegree = 32;
 
@@ -40,8 +43,10 @@ enum : uint8_t { M_GROUNDED = 0, M_OCEAN = 1, M_LAND = 2, M_OTHER = 3, M_UNKNOWN
 struct CgDev {
     double gamma, pNorm2, eps_stop, alpha, beta, rnorm, rnorm0, bnorm, rr, pAp;
     double atol, rtol;
+    double rz_last;  // last r'z computed (continuation across a residual replacement)
     long long iter, itmax;
     int done, status, first, stop_rule;
+    int cont;        // init continues the previous search direction instead of restarting
 };
 
 struct ChebDev {
@@ -101,7 +106,7 @@ struct Ctx {
     double *h_prev = nullptr;
     double *cr[2] = {nullptr, nullptr}, *cp[2] = {nullptr, nullptr}; // Chebyshev r/p buffers
     double *r64 = nullptr;                                            // mixed: outer residual
-    float *aP32 = nullptr, *aE32 = nullptr, *aN32 = nullptr;
+    float *aP32 = nullptr, *aE32 = nullptr, *aN32 = nullptr, *dP32 = nullptr;
     float *b32 = nullptr, *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32[2] = {nullptr, nullptr}, *Ap32 = nullptr;
     float *cr32[2] = {nullptr, nullptr}, *cp32[2] = {nullptr, nullptr};
     double *partials = nullptr;  // kMaxRedValues * max_blocks
@@ -110,6 +115,8 @@ struct Ctx {
     DevScalars *host_dev = nullptr;  // pinned mirror for read-back
     int max_blocks = 0;
     int grid_stencil = 0;    // blocks for tile-stride kernels
+    int march_th = 8;        // row-marching tile height
+    int march_blocks = 1;    // row-marching grid (one block per kMarchX x march_th tile)
     long long launches = 0;
     std::string err;
     bool assembled = false;

@@ -13,6 +13,10 @@
 //   B: x += alpha p, r -= alpha Ap, z = r/aP, partial r'z and r'r -> last block: stop test, beta
 // Algorithmic traffic per cell and iteration: A reads r, aP, p_old, aE, aN and writes p, Ap;
 // B reads x, p, r, Ap, aP and writes x, r: 14 words (112 B in Float64, 56 B in Float32).
+#include <algorithm>
+#include <cstdlib>
+
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 #include <float.h>
 #include <stdio.h>
@@ -55,17 +59,33 @@ __global__ void __launch_bounds__(kThreads) k_matvec(int nx, int ny, const T *aP
 // Scalar updates (run by thread 0 of the last block)
 // ---------------------------------------------------------------------------------------------
 __device__ void cg_init_finish(CgDev *cg, double rz, double rr, double bb) {
+    if (cg->cont) {
+        // Residual replacement: keep the previous search direction, p = z + beta p with
+        // beta = r'z (replaced residual) / r'z (last recursive residual).
+        const double beta = rz / cg->rz_last;
+        if (isfinite(beta) && beta >= 0) {
+            cg->beta = beta;
+            cg->pNorm2 = rz + beta * beta * cg->pNorm2;
+            cg->first = 0;
+        } else {
+            cg->first = 1;
+            cg->beta = 0.0;
+            cg->pNorm2 = rz;
+        }
+    } else {
+        cg->first = 1;
+        cg->beta = 0.0;
+        cg->pNorm2 = rz;
+    }
     cg->gamma = rz;
+    cg->rz_last = rz;
     const double rn = sqrt(rz);
     cg->rr = sqrt(rr);
     cg->bnorm = sqrt(bb);
     cg->rnorm0 = cg->stop_rule == SHK_STOP_KRYLOV ? rn : cg->rr;
     cg->rnorm = cg->rnorm0;
     cg->eps_stop = cg->atol + cg->rtol * rn;
-    cg->pNorm2 = rz;
     cg->iter = 0;
-    cg->first = 1;
-    cg->beta = 0.0;
     if (isnan(rz) || isnan(rr)) {
         cg->done = 1;
         cg->status = SHK_BREAKDOWN;
@@ -88,6 +108,7 @@ __device__ void cg_init_finish(CgDev *cg, double rz, double rr, double bb) {
 
 __device__ void cg_iter_finish(CgDev *cg, double rz, double rr) {
     const double rn = sqrt(rz), rrn = sqrt(rr);
+    cg->rz_last = rz;
     cg->rr = rrn;
     bool solved;
     if (cg->stop_rule == SHK_STOP_KRYLOV) solved = (rn <= cg->eps_stop) || (rn + 1.0 <= 1.0);
@@ -158,34 +179,138 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(int nx, int ny, const T *a
 }
 
 // A: p_new = z + beta*p_old (p_new = z on the first iteration), Ap = A p_new, partial p'Ap.
-template <typename T, bool JAC>
-__global__ void __launch_bounds__(kThreads) k_cg_A(int nx, int ny, const T *__restrict__ aP,
-                                                   const T *__restrict__ aE, const T *__restrict__ aN,
-                                                   const T *__restrict__ r, const T *__restrict__ zbuf,
-                                                   const T *__restrict__ p_old, T *__restrict__ p_new,
-                                                   T *__restrict__ Ap, CgDev *cg, double *partials,
-                                                   unsigned int *counter, double eps_curv) {
+//
+// One block owns a tile of kMarchX columns x TH rows and marches up the rows.  Input rows (r or
+// z, aP, p_old, aE, aN, plus one halo column each side) stream into a shared-memory ring with
+// cp.async, kRingRows - 2 rows ahead of use, so DRAM latency overlaps the arithmetic of earlier
+// rows.  For input row k each thread forms p_k once (z = r/aP: one divide per cell) and the block
+// then emits output row k-1, whose five stencil terms are all at hand: p at rows k-2, k-1, k in
+// registers, p at columns x+-1 of row k-1 in a double-buffered shared row, and aE(x-1) in the ring.
+// Subtraction order E, W, N, S as in stencil_matvec_kernel!.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
+    __pipeline_memcpy_async(dst, src, sizeof(T));
+}
+
+// LAPL (Float32 operator of the mixed form): the matvec is applied in Laplacian form
+// y = dP p + aE (p - pE) + aW (p - pW) + aN (p - pN) + aS (p - pS), with dP = aP - (aE+aW+aN+aS)
+// the diagonal excess computed in Float64 and rounded once.  Storing edge conductances and the
+// excess (rather than aP and the couplings) keeps the rounded operator accurate entry by entry
+// for this nearly singular M-matrix, whatever its condition number.
+template <typename T, bool JAC, bool LAPL = false>
+__global__ void __launch_bounds__(kMarchX, 6) k_cg_A(int nx, int ny, int TH, const T *__restrict__ aP,
+                                                  const T *__restrict__ aE, const T *__restrict__ aN,
+                                                  const T *__restrict__ r, const T *__restrict__ zbuf,
+                                                  const T *__restrict__ p_old, T *__restrict__ p_new,
+                                                  T *__restrict__ Ap, CgDev *cg, double *partials,
+                                                  unsigned int *counter, double eps_curv,
+                                                  const T *__restrict__ dP = nullptr) {
     if (*(volatile int *)&cg->done) return;
+    constexpr int R = kRingRows, W = kMarchX + 2;
+    enum { IR = 0, IP = 1, IO = 2, IE = 3, IN = 4, ID = 5, NA = LAPL ? 6 : 5 };
+    __shared__ __align__(16) T ring[R][NA][W];
+    __shared__ T prow[2][W];
     const bool first = cg->first != 0;
     const T beta = (T)cg->beta;
-    auto pval = [&](size_t k) -> T {
-        T z = JAC ? r[k] / aP[k] : zbuf[k];
-        return first ? z : z + beta * p_old[k];
+    const int tiles_x = (nx + kMarchX - 1) / kMarchX;
+    const int x0 = (blockIdx.x % tiles_x) * kMarchX, y0 = (blockIdx.x / tiles_x) * TH;
+    const int tid = threadIdx.x, ix = x0 + tid;
+    const bool inx = ix < nx;
+    const int y1 = min(y0 + TH, ny);
+    const int kfirst = y0 - 1, klast = y1;            // input rows kfirst..klast (clipped below)
+    const T *src_r = JAC ? r : zbuf;
+    // issue the copies of input row q into its ring slot (empty group when out of range)
+    auto issue = [&](int q) {
+        if (q >= 0 && q < ny && q <= klast) {
+            const int slot = (q - kfirst) % R;
+            const size_t rowoff = (size_t)q * nx;
+            if (inx) {
+                const size_t c = rowoff + ix;
+                cp_async_elem(&ring[slot][IR][tid + 1], src_r + c);
+                cp_async_elem(&ring[slot][IP][tid + 1], aP + c);
+                if (!first) cp_async_elem(&ring[slot][IO][tid + 1], p_old + c);
+                cp_async_elem(&ring[slot][IE][tid + 1], aE + c);
+                cp_async_elem(&ring[slot][IN][tid + 1], aN + c);
+                if (LAPL) cp_async_elem(&ring[slot][ID][tid + 1], dP + c);
+            }
+            if (tid == 0 && x0 > 0) {
+                const size_t c = rowoff + x0 - 1;
+                cp_async_elem(&ring[slot][IR][0], src_r + c);
+                if (JAC) cp_async_elem(&ring[slot][IP][0], aP + c);
+                if (!first) cp_async_elem(&ring[slot][IO][0], p_old + c);
+                cp_async_elem(&ring[slot][IE][0], aE + c);
+            }
+            if (tid == kMarchX - 1 && x0 + kMarchX < nx) {
+                const size_t c = rowoff + x0 + kMarchX;
+                cp_async_elem(&ring[slot][IR][W - 1], src_r + c);
+                if (JAC) cp_async_elem(&ring[slot][IP][W - 1], aP + c);
+                if (!first) cp_async_elem(&ring[slot][IO][W - 1], p_old + c);
+            }
+        }
+        __pipeline_commit();
     };
-    Tiles Tl(nx, ny);
-    double red[1] = {0.0};
-    for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
-        int ix, iy;
-        Tl.cell(t, ix, iy);
-        if (ix >= nx || iy >= ny) continue;
-        size_t c = (size_t)ix + (size_t)iy * nx;
-        T pc = pval(c);
-        T apc = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, pc, pval);
-        p_new[c] = pc;
-        Ap[c] = apc;
-        red[0] += (double)pc * (double)apc;
+    auto pform = [&](int slot, int j) -> T {
+        T z = JAC ? ring[slot][IR][j] / ring[slot][IP][j] : ring[slot][IR][j];
+        return first ? z : z + beta * ring[slot][IO][j];
+    };
+    for (int q = kfirst; q < kfirst + R - 2; q++) issue(q);
+    T p_m2 = (T)0, p_m1 = (T)0, aN_m2 = (T)0, aN_m1 = (T)0, aP_m1 = (T)0, aE_m1 = (T)0, dP_m1 = (T)0;
+    double acc = 0.0;
+    for (int k = kfirst; k <= klast; k++) {
+        __pipeline_wait_prior(R - 3);
+        __syncthreads();
+        issue(k + R - 2);  // the slot of row k-2 is free: every thread finished row k-2 before the barrier
+        const bool valid_k = k >= 0 && k < ny;
+        const int slot = (k - kfirst) % R;
+        T p_k = (T)0, aN_k = (T)0, aP_k = (T)0, aE_k = (T)0, dP_k = (T)0;
+        T *pr = prow[k & 1];
+        if (valid_k) {
+            if (inx) {
+                p_k = pform(slot, tid + 1);
+                aP_k = ring[slot][IP][tid + 1];
+                aE_k = ring[slot][IE][tid + 1];
+                aN_k = ring[slot][IN][tid + 1];
+                if (LAPL) dP_k = ring[slot][ID][tid + 1];
+            }
+            pr[tid + 1] = p_k;
+            if (tid == 0) pr[0] = x0 > 0 ? pform(slot, 0) : (T)0;
+            if (tid == kMarchX - 1) pr[W - 1] = (x0 + kMarchX < nx) ? pform(slot, W - 1) : (T)0;
+        }
+        // Output row k-1 reads only data published before this iteration's barrier (its p row and
+        // its ring slot were written in earlier iterations), so no second barrier is needed here.
+        const int iy = k - 1;  // output row
+        if (iy >= y0 && iy < y1 && inx) {
+            const T *pm = prow[iy & 1];
+            const int sm1 = (iy - kfirst) % R;
+            T y;
+            if (LAPL) {
+                y = dP_m1 * p_m1;
+                if (ix < nx - 1) y += aE_m1 * (p_m1 - pm[tid + 2]);
+                if (ix > 0) y += ring[sm1][IE][tid] * (p_m1 - pm[tid]);
+                if (iy + 1 < ny) y += aN_m1 * (p_m1 - p_k);
+                if (iy > 0) y += aN_m2 * (p_m1 - p_m2);
+            } else {
+                y = aP_m1 * p_m1;
+                if (ix < nx - 1) y -= aE_m1 * pm[tid + 2];
+                if (ix > 0) y -= ring[sm1][IE][tid] * pm[tid];
+                if (iy + 1 < ny) y -= aN_m1 * p_k;
+                if (iy > 0) y -= aN_m2 * p_m2;
+            }
+            const size_t c = (size_t)iy * nx + ix;
+            p_new[c] = p_m1;
+            Ap[c] = y;
+            acc += (double)p_m1 * (double)y;
+        }
+        p_m2 = p_m1;
+        p_m1 = p_k;
+        aN_m2 = aN_m1;
+        aN_m1 = aN_k;
+        aP_m1 = aP_k;
+        aE_m1 = aE_k;
+        dP_m1 = dP_k;
     }
-    double out[1];
+    __pipeline_wait_prior(0);
+    double red[1] = {acc}, out[1];
     if (grid_reduce<1, false>(red, partials, counter, out) && threadIdx.x == 0) {
         const double pAp = out[0];
         cg->pAp = pAp;
@@ -199,28 +324,88 @@ __global__ void __launch_bounds__(kThreads) k_cg_A(int nx, int ny, const T *__re
     }
 }
 
+// 16-byte vectors for the streaming kernels.
+template <typename T> struct Vec16;
+template <> struct Vec16<double> {
+    using V = double2;
+    static constexpr int W = 2;
+    __device__ static inline double get(const V &v, int k) { return k == 0 ? v.x : v.y; }
+    __device__ static inline void set(V &v, int k, double a) { if (k == 0) v.x = a; else v.y = a; }
+};
+template <> struct Vec16<float> {
+    using V = float4;
+    static constexpr int W = 4;
+    __device__ static inline float get(const V &v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
+    __device__ static inline void set(V &v, int k, float a) {
+        if (k == 0) v.x = a; else if (k == 1) v.y = a; else if (k == 2) v.z = a; else v.w = a;
+    }
+};
+
 // B: x += alpha p, r -= alpha Ap; JAC: z = r/aP, partials r'z, r'r -> stop test.
+// 16-byte loads, kUnrollB vectors in flight per thread; scalar tail for n not a multiple of the
+// vector width.
 template <typename T, bool JAC>
 __global__ void __launch_bounds__(kThreads) k_cg_B(int n, const T *__restrict__ aP, const T *__restrict__ p,
                                                    const T *__restrict__ Ap, T *__restrict__ x, T *__restrict__ r,
                                                    CgDev *cg, double *partials, unsigned int *counter) {
     if (*(volatile int *)&cg->done) return;
+    using VT = Vec16<T>;
+    using V = typename VT::V;
+    constexpr int W = VT::W;
     const T alpha = (T)cg->alpha;
-    double red[2] = {0.0, 0.0};
+    double rz = 0.0, rr = 0.0;
+    const int nv = n / W;
+    const V *aPv = reinterpret_cast<const V *>(aP), *pv = reinterpret_cast<const V *>(p),
+            *Apv = reinterpret_cast<const V *>(Ap);
+    V *xv = reinterpret_cast<V *>(x), *rv = reinterpret_cast<V *>(r);
     const int stride = gridDim.x * blockDim.x;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    for (int base = blockIdx.x * blockDim.x + threadIdx.x; base < nv; base += stride * kUnrollB) {
+        V X[kUnrollB], P[kUnrollB], R[kUnrollB], AP[kUnrollB], D[kUnrollB];
+#pragma unroll
+        for (int u = 0; u < kUnrollB; u++) {
+            int i = base + u * stride;
+            if (i < nv) {
+                X[u] = xv[i];
+                P[u] = pv[i];
+                R[u] = rv[i];
+                AP[u] = Apv[i];
+                if (JAC) D[u] = aPv[i];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnrollB; u++) {
+            int i = base + u * stride;
+            if (i < nv) {
+#pragma unroll
+                for (int k = 0; k < W; k++) {
+                    T xi = VT::get(X[u], k) + alpha * VT::get(P[u], k);
+                    T ri = VT::get(R[u], k) + (-alpha) * VT::get(AP[u], k);
+                    VT::set(X[u], k, xi);
+                    VT::set(R[u], k, ri);
+                    if (JAC) {
+                        T zi = ri / VT::get(D[u], k);
+                        rz += (double)ri * (double)zi;
+                        rr += (double)ri * (double)ri;
+                    }
+                }
+                xv[i] = X[u];
+                rv[i] = R[u];
+            }
+        }
+    }
+    for (int i = nv * W + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         T xi = x[i] + alpha * p[i];
         T ri = r[i] + (-alpha) * Ap[i];
         x[i] = xi;
         r[i] = ri;
         if (JAC) {
             T zi = ri / aP[i];
-            red[0] += (double)ri * (double)zi;
-            red[1] += (double)ri * (double)ri;
+            rz += (double)ri * (double)zi;
+            rr += (double)ri * (double)ri;
         }
     }
     if (JAC) {
-        double out[2];
+        double red[2] = {rz, rr}, out[2];
         if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) cg_iter_finish(cg, out[0], out[1]);
     }
 }
@@ -443,12 +628,18 @@ __global__ void __launch_bounds__(kThreads) k_est_B(int n, const double *rhs, do
 // ---------------------------------------------------------------------------------------------
 // Mixed precision helpers
 // ---------------------------------------------------------------------------------------------
-__global__ void k_to_float3(int n, const double *a, const double *b, const double *c, float *fa, float *fb,
-                            float *fc) {
+// Float32 operator of the mixed form: aP (Jacobi scaling), aE, aN and the diagonal excess
+// dP = aP - (aE + aW + aN + aS) evaluated in Float64 before rounding.
+__global__ void k_to_float_lapl(int nx, int ny, const double *aP, const double *aE, const double *aN, float *fP,
+                                float *fE, float *fN, float *fD) {
+    const int n = nx * ny;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        fa[i] = (float)a[i];
-        fb[i] = (float)b[i];
-        fc[i] = (float)c[i];
+        const int ix = i % nx, iy = i / nx;
+        const double e = aE[i], w = ix > 0 ? aE[i - 1] : 0.0, no = aN[i], so = iy > 0 ? aN[i - nx] : 0.0;
+        fP[i] = (float)aP[i];
+        fE[i] = (float)e;
+        fN[i] = (float)no;
+        fD[i] = (float)(aP[i] - (e + w + no + so));
     }
 }
 
@@ -487,6 +678,18 @@ __global__ void k_refine_update(int n, const float *d, double *h) {
 static int flat_grid(Ctx *c, long long n) {
     long long b = (n + kThreads - 1) / kThreads;
     long long cap = (long long)c->grid_stencil;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+// Blocks for the 16-byte-vector streaming kernels: enough for kUnrollB vectors per thread, at
+// most the resident capacity (148 SMs x 8 blocks of 256 threads).
+static int stream_grid(Ctx *c, long long n, size_t elem) {
+    long long vec = (long long)(16 / elem);
+    long long per_block = (long long)kThreads * kUnrollB * vec;
+    long long b = (n + per_block - 1) / per_block;
+    long long cap = (long long)c->num_sms * 8;
     if (b > cap) b = cap;
     if (b < 1) b = 1;
     return (int)b;
@@ -594,7 +797,8 @@ static CgDev make_cg_init(const shk_cg_opts *o, long long n, bool inner, double 
 // x0 (Float64, may be null) is the warm start used only for the initial residual.
 template <typename T>
 static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T *aP, const T *aE, const T *aN,
-                   const double *x0, const T *b, T *x, T *r, T *z, T **p, T *Ap, T **cr, T **cp, long *iters_out) {
+                   const double *x0, const T *b, T *x, T *r, T *z, T **p, T *Ap, T **cr, T **cp, long *iters_out,
+                   int p_parity = 0, const T *lapl = nullptr) {
     const int nx = c->nx, ny = c->ny, n = nx * ny;
     const bool jac = o->precond == SHK_PRECOND_JACOBI;
     const int deg = o->cheb_degree;
@@ -620,18 +824,31 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
         if ((rc = read_cg_flags(c, cgh, cgd))) return rc;
         if (cgh->done) break;
         for (int b2 = 0; b2 < batch; b2++, enq++) {
-            T *p_old = p[enq & 1], *p_new = p[(enq + 1) & 1];
-            if (jac) {
-                k_cg_A<T, true><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, aP, aE, aN, r, nullptr, p_old, p_new,
-                                                                            Ap, cgd, c->partials, c->counter, eps_curv);
-                k_cg_B<T, true><<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd, c->partials,
-                                                                            c->counter);
+            T *p_old = p[(enq + p_parity) & 1], *p_new = p[(enq + p_parity + 1) & 1];
+            if (jac && lapl) {
+                k_cg_A<T, true, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(
+                    nx, ny, c->march_th, aP, aE, aN, r, nullptr, p_old, p_new, Ap, cgd, c->partials, c->counter, eps_curv,
+                    lapl);
+                k_cg_B<T, true><<<stream_grid(c, n, sizeof(T)), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd,
+                                                                                          c->partials, c->counter);
+            } else if (jac) {
+                k_cg_A<T, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(nx, ny, c->march_th, aP, aE, aN, r, nullptr,
+                                                                           p_old, p_new, Ap, cgd, c->partials, c->counter,
+                                                                           eps_curv);
+                k_cg_B<T, true><<<stream_grid(c, n, sizeof(T)), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd,
+                                                                                          c->partials, c->counter);
                 c->launches += 2;
             } else {
-                k_cg_A<T, false><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, aP, aE, aN, r, z, p_old, p_new, Ap,
-                                                                             cgd, c->partials, c->counter, eps_curv);
-                k_cg_B<T, false><<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd, c->partials,
-                                                                             c->counter);
+                if (lapl)
+                    k_cg_A<T, false, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(
+                        nx, ny, c->march_th, aP, aE, aN, r, z, p_old, p_new, Ap, cgd, c->partials, c->counter, eps_curv,
+                        lapl);
+                else
+                    k_cg_A<T, false><<<c->march_blocks, kMarchX, 0, c->stream>>>(nx, ny, c->march_th, aP, aE, aN, r, z,
+                                                                                p_old, p_new, Ap, cgd, c->partials,
+                                                                                c->counter, eps_curv);
+                k_cg_B<T, false><<<stream_grid(c, n, sizeof(T)), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd,
+                                                                                           c->partials, c->counter);
                 c->launches += 2;
                 enqueue_cheb<T, CG_ITER>(c, deg, aP, aE, aN, r, cr, cp, z, cgd);
             }
@@ -677,14 +894,27 @@ int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
         s.rnorm0 = g.rnorm0;
         s.rnorm = g.rnorm;
     } else if (o->precision == SHK_MIXED) {
-        // Float32 stencil + CG inside Float64 iterative refinement: h <- h + A32^-1 (b - A64 h).
-        k_to_float3<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->aP, c->aE, c->aN, c->aP32, c->aE32, c->aN32);
+        // Float32 stencil and CG with Float64 residual replacement.  The Float32 CG runs until its
+        // recursive residual has dropped by inner_rtol; then its correction is folded into the
+        // Float64 head (h += x32), the true residual b - A64 h is recomputed in Float64 and the CG
+        // continues from it with the previous search direction.  Convergence is judged only on the
+        // Float64 residual.  A Float32 zero-curvature event restarts the direction instead of
+        // failing; three in a row, or no progress of the Float64 residual, end the solve.
+        k_to_float_lapl<<<flat_grid(c, n), kThreads, 0, c->stream>>>(nx, ny, c->aP, c->aE, c->aN, c->aP32, c->aE32,
+                                                                     c->aN32, c->dP32);
         c->launches++;
-        const double inner_rtol = o->inner_rtol > 0 ? o->inner_rtol : 1e-3;
-        const int max_refine = o->max_refine > 0 ? o->max_refine : 50;
+        const double inner_rtol = o->inner_rtol > 0 ? o->inner_rtol : 1e-2;
+        const int max_refine = o->max_refine > 0 ? o->max_refine : 200;
+        const long long itmax = o->itmax > 0 ? o->itmax : 2LL * n;
+        const long long cycle_cap = o->inner_itmax > 0 ? o->inner_itmax : std::max(200LL, (long long)(nx + ny) / 2);
+        const bool trace = getenv("SHK_VERBOSE") != nullptr;
         long total = 0;
-        int refine = 0;
+        int refine = 0, restarts = 0, stalls = 0;
+        double best = INFINITY;
+        bool cont = false;
+        int parity = 0;
         int status = SHK_NOT_CONVERGED;
+        CgDev *cgh = &c->host_dev->cg_in;
         for (;;) {
             k_outer_residual<<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, c->aP, c->aE, c->aN, c->st.h, c->rhs,
                                                                          c->b32, c->dev, c->partials, c->counter);
@@ -692,6 +922,9 @@ int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
             int rc = read_scalars(c);
             if (rc) return rc;
             const double rn = sqrt(c->host_dev->ref_rr), bn = sqrt(c->host_dev->ref_bb);
+            if (trace)
+                fprintf(stderr, "[shk mixed] cycle %d: ||r64||/||b|| = %.3e, inner iterations so far %ld, inner status %d\n",
+                        refine, rn / bn, total, refine ? cgh->status : -1);
             if (refine == 0) s.rnorm0 = rn;
             s.rnorm = rn;
             if (isnan(rn)) {
@@ -702,22 +935,50 @@ int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
                 status = SHK_OK;
                 break;
             }
-            if (refine >= max_refine || total >= (o->itmax > 0 ? o->itmax : 2L * n)) break;
-            CgDev *cgh = &c->host_dev->cg_in;
-            *cgh = make_cg_init(o, n, true, inner_rtol);
-            long it = 0;
-            rc = cg_core<float>(c, o, &c->dev->cg_in, cgh, c->aP32, c->aE32, c->aN32, nullptr, c->b32, c->x32, c->r32,
-                                c->z32, c->p32, c->Ap32, c->cr32, c->cp32, &it);
-            if (rc) return rc;
-            if (cgh->status == SHK_BREAKDOWN) {
-                status = SHK_BREAKDOWN;
+            if (rn < 0.5 * best) {
+                best = rn;
+                stalls = 0;
+            } else if (++stalls >= 8) {
                 break;
             }
+            if (refine >= max_refine || total >= itmax) break;
+            if (cont) {
+                // keep gamma / pNorm2 / rz_last of the previous inner solve, continue its direction
+                cgh->done = 0;
+                cgh->status = SHK_OK;
+                cgh->iter = 0;
+                cgh->cont = 1;
+                cgh->itmax = std::min(itmax - total, cycle_cap);
+                cgh->rtol = inner_rtol;
+                cgh->atol = 0.0;
+                cgh->stop_rule = SHK_STOP_RELRES;
+            } else {
+                *cgh = make_cg_init(o, n, true, inner_rtol);
+                cgh->itmax = std::min(itmax - total, cycle_cap);
+            }
+            long it = 0;
+            // the inner solve's "x" is the correction: x32 starts at 0 and r32 = b32; a continued
+            // solve starts from the buffer holding the previous solve's last search direction
+            rc = cg_core<float>(c, o, &c->dev->cg_in, cgh, c->aP32, c->aE32, c->aN32, nullptr, c->b32, c->x32, c->r32,
+                                c->z32, c->p32, c->Ap32, c->cr32, c->cp32, &it, parity, c->dP32);
+            if (rc) return rc;
+            if ((rc = read_cg_flags(c, cgh, &c->dev->cg_in))) return rc;
             k_refine_update<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->x32, c->st.h);
             c->launches++;
             if ((rc = check_launch(c, "refine update"))) return rc;
             total += it;
             refine++;
+            parity = (parity + (int)(cgh->iter & 1)) & 1;
+            if (cgh->status == SHK_BREAKDOWN) {  // Float32 zero curvature: restart the direction
+                cont = false;
+                if (++restarts >= 3) {
+                    status = SHK_BREAKDOWN;
+                    break;
+                }
+            } else {
+                restarts = 0;
+                cont = true;
+            }
         }
         s.niter = total;
         s.status = status;

@@ -204,7 +204,7 @@ class CGIterativeSolver(AbstractIterativeSolver):
     def __init__(self, g: Grid, lsy=MatrixFreeLinearSystem, *, chebyshev_degree: int | None = None,
                  chebyshev_nsteps_estimate: int = 15, amg: bool = False, precision: str = "fp64",
                  stop_rule: str = "krylov", atol: float | None = None, rtol: float | None = None, itmax: int = 0,
-                 inner_rtol: float = 1e-3, max_refine: int = 0):
+                 inner_rtol: float = 1e-2, max_refine: int = 0, inner_itmax: int = 0):
         if lsy is SparseAssembledLinearSystem:
             raise RuntimeError("CGIterativeSolver(g, SparseAssembledLinearSystem) is CPU-only; use "
                                "CGIterativeSolver(g, MatrixFreeLinearSystem) under the CUDA backend.")
@@ -232,6 +232,7 @@ class CGIterativeSolver(AbstractIterativeSolver):
         self.itmax = int(itmax)
         self.inner_rtol = float(inner_rtol)
         self.max_refine = int(max_refine)
+        self.inner_itmax = int(inner_itmax)
         self.stats = CgStats()
 
     def opts(self) -> _lib.shk_cg_opts:
@@ -241,7 +242,7 @@ class CGIterativeSolver(AbstractIterativeSolver):
             cheb_nsteps=self.precond.nsteps_estimate if cheb else 15,
             stop_rule=0 if self.stop_rule == "krylov" else 1, precision=0 if self.precision == "fp64" else 1,
             max_refine=self.max_refine, atol=self.atol, rtol=self.rtol, inner_rtol=self.inner_rtol,
-            itmax=self.itmax)
+            itmax=self.itmax, inner_itmax=self.inner_itmax)
 
     def _record(self, s: _lib.shk_cg_stats):
         self.stats = CgStats(niter=s.niter, status=s.status, refinements=s.refinements, rnorm0=s.rnorm0,

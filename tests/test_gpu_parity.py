@@ -285,3 +285,45 @@ def test_cg_status_codes(shk, orc, cuda):
     ls2 = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem)
     stats2 = shk.solve_elliptic_linear_system(ls2, s2, g, pm, shk.Arithmetic(), sl)
     assert stats2.status == shk._lib.BREAKDOWN
+
+
+@pytest.mark.parametrize("precond", [0, 1])
+def test_mixed_precision_single_solve(shk, orc, cuda, precond):
+    """Float32 CG with Float64 residual replacement reaches ||b - A h|| <= 1e-8 ||b|| measured with
+    the Float64 operator.  Its distance to a tight solve is judged against the plain Float64 CG's
+    distance at the same tolerance (rel-res 1e-8 of ||b|| admits errors of ~1e-4 in h here)."""
+    w = shk.configs.plain64()
+    g, pm, sl, osl, s, st = setup_pair(shk, orc, cuda, w, perturb=True)
+    A = orc.assemble(st, None)
+    ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, chebyshev_degree=4 if precond else None,
+                               precision="mixed", stop_rule="relres", rtol=1e-8, atol=0.0)
+    stats = shk.solve_elliptic_linear_system(ls, s, g, pm, shk.Arithmetic(), sl)
+    assert stats.status == 0, stats
+    h = s.h.cpu().numpy()
+    res = np.linalg.norm(A["rhs"] - orc.matvec(A, h)) / np.linalg.norm(A["rhs"])
+    assert res <= 1e-8, res
+    x_tight, _ = orc.cg(A, st["h"], orc.CgSpec(precond=0, atol=0.0, rtol=1e-14))
+    x_plain, _ = orc.cg(A, st["h"], orc.CgSpec(precond=precond, stop_rule=1, atol=0.0, rtol=1e-8))
+    e_mixed, e_plain = relerr(h, x_tight), relerr(x_plain, x_tight)
+    assert e_mixed <= 10 * e_plain + 1e-12, (e_mixed, e_plain)
+
+
+def test_mixed_precision_run_field_errors(shk, orc, cuda):
+    """Five timesteps of the 64x64 workload, mixed form against the Float64 oracle at the same
+    rel-res 1e-8.  Per-field errors (h, N, b, q) are compared with the plain Float64 form's own
+    distance from a tight (1e-13) Float64 run, the size of the tolerance ball."""
+    w = shk.configs.plain64()
+    g, pm, sl, osl, s, st = setup_pair(shk, orc, cuda, w)
+    st_tight = st.copy()
+    ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, precision="mixed", stop_rule="relres", rtol=1e-8,
+                               atol=0.0)
+    ps = shk.PicardSolver(500, 1e-6, ls, g)
+    sim = shk.Simulation(g, s, 5, 3600.0, pm, "implicit", [], shk.ConstantMeltInput(), sl, ps=ps)
+    shk.run(sim)
+    orc.run(st, None, osl, 5, 3600.0, cgspec=orc.CgSpec(precond=0, stop_rule=1, rtol=1e-8, atol=0.0))
+    orc.run(st_tight, None, osl, 5, 3600.0, cgspec=orc.CgSpec(precond=0, stop_rule=1, rtol=1e-13, atol=0.0))
+    host = s.to_numpy(["h", "N", "b", "q_x", "q_y"])
+    for f in ("h", "N", "b", "q_x", "q_y"):
+        e_mixed = relerr(host[f], st_tight[f])
+        e_plain = relerr(st[f], st_tight[f])
+        assert e_mixed <= 10 * e_plain + 1e-9, (f, e_mixed, e_plain)
