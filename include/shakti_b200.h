@@ -227,6 +227,30 @@ SHK_API int shk_run(void *ctx, int head_scheme, double dt, int tsteps, double *t
 /* Launch accounting: number of kernels this context has enqueued since creation. */
 SHK_API long shk_kernel_launches(const void *ctx);
 
+/* ---------------------------------------------------------------------------------------------
+ * Allocation-free solve.  No counterpart in the reference: it exists for callers that cannot
+ * allocate device memory when they solve -- an application whose device memory all belongs to its
+ * own pool allocator, a real-time loop that cannot afford the device-wide synchronisation of
+ * cudaMalloc/cudaFree, or a plugin host that forbids allocation after start-up.
+ *
+ * Float64 Jacobi-preconditioned CG (Krylov.jl cg! semantics, as shk_cg_solve) on a caller-owned
+ * operator in this library's matrix-free form: aP, aE, aN (nx*ny doubles each; the west/south
+ * couplings are the neighbours' east/north entries, exactly what shk_export_mfls writes), rhs,
+ * and x (warm start in, solution out).  Only o->precond = SHK_PRECOND_JACOBI, o->precision =
+ * SHK_FP64 are accepted.  stream may be NULL.
+ *
+ * Scratch (Krylov vectors, reduction partials, scalars) lives in one file-scope device array of
+ * about 2.8 MB that every GPU loading the library holds until the process exits; nothing is
+ * allocated.  Limit: nx*ny <= 65536 cells (e.g. 256 x 256); larger grids return SHK_BAD_ARG with a
+ * message on stderr.  The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current: make that first call before any stream
+ * capture.  All calls share the array and it keeps the last call's contents, so calls that overlap
+ * on the GPU (different streams or host threads) race: serialise them.  Returns the solve's
+ * status (SHK_OK, SHK_NOT_CONVERGED, SHK_BREAKDOWN) or an error code. */
+SHK_API int shk_cg_solve_static(int nx, int ny, const double *aP, const double *aE, const double *aN,
+                                const double *rhs, double *x, const shk_cg_opts *o, shk_cg_stats *st,
+                                void *stream);
+
 #ifdef __cplusplus
 }
 #endif

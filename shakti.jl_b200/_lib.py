@@ -100,6 +100,8 @@ SIGNATURES = {
     "shk_run": (C.c_int, [VP, C.c_int, C.c_double, C.c_int, DP, C.POINTER(shk_melt_input),
                           C.POINTER(shk_picard_opts), C.POINTER(shk_cg_opts), C.POINTER(shk_picard_stats)]),
     "shk_kernel_launches": (C.c_long, [VP]),
+    "shk_cg_solve_static": (C.c_int, [C.c_int, C.c_int, VP, VP, VP, VP, VP, C.POINTER(shk_cg_opts),
+                                      C.POINTER(shk_cg_stats), VP]),
 }
 
 _LIB = None

@@ -1000,3 +1000,141 @@ int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
 }
 
 } // namespace shk
+
+// =============================================================================================
+// Allocation-free Jacobi-PCG solve (shk_cg_solve_static).
+//
+// Some callers cannot allocate device memory at solve time: an application whose device memory
+// is owned entirely by its own pool allocator, code running inside a real-time loop where the
+// device-wide synchronisation of cudaMalloc/cudaFree is not acceptable, or a plugin host that
+// forbids allocation after start-up.  This entry point serves them: its Krylov vectors, grid
+// reduction partials and scalar block live in the file-scope array below, which every GPU that
+// loads the library holds until the process exits.  The caller passes only inputs and outputs.
+//
+// Limits and sharing: at most kStaticMaxCells cells (a 256 x 256 grid); every call uses the same
+// array and leaves its contents behind, so calls that overlap on the GPU (two streams, or two
+// host threads) race and must be serialised by the caller.
+// =============================================================================================
+namespace shk {
+namespace {
+constexpr long long kStaticMaxCells = 65536;
+constexpr int kStaticMaxBlocks = 4096;
+constexpr size_t kStaticVecBytes = (size_t)kStaticMaxCells * sizeof(double);
+constexpr size_t kStaticPartialBytes = (size_t)kMaxRedValues * kStaticMaxBlocks * sizeof(double);
+constexpr size_t kStaticCgOffset = 5 * kStaticVecBytes + kStaticPartialBytes + 256;
+constexpr size_t kStaticBytes = kStaticCgOffset + ((sizeof(CgDev) + 255) / 256) * 256;
+} // namespace
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+// Writes the initial scalar block and clears the reduction counter (it must start at zero; an
+// earlier call that stopped on an error could have left it non-zero).
+__global__ void k_static_init(CgDev *cg, CgDev init, unsigned int *counter) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        *cg = init;
+        *counter = 0u;
+    }
+}
+
+// Device address of g_static_scratch for each device, looked up once per device (with that device
+// current) through cudaGetSymbolAddress: in host code the array's name is only a stand-in.
+static void *g_static_addr[128];
+
+static int static_scratch_address(int device, void **out) {
+    if (device < 0 || device >= 128) return SHK_BAD_ARG;
+    if (!g_static_addr[device]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess || !ptr) {
+            fprintf(stderr, "shk_cg_solve_static: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+            return SHK_CUDA_ERROR;
+        }
+        g_static_addr[device] = ptr;
+    }
+    *out = g_static_addr[device];
+    return SHK_OK;
+}
+
+} // namespace shk
+
+extern "C" SHK_API int shk_cg_solve_static(int nx, int ny, const double *aP, const double *aE, const double *aN,
+                                           const double *rhs, double *x, const shk_cg_opts *o, shk_cg_stats *st,
+                                           void *stream) {
+    using namespace shk;
+    if (!o || !aP || !aE || !aN || !rhs || !x) return SHK_BAD_ARG;
+    if (nx < 2 || ny < 2 || (long long)nx * ny > kStaticMaxCells) {
+        fprintf(stderr, "shk_cg_solve_static: grid %d x %d exceeds the %lld-cell limit of the static scratch "
+                        "(use shk_cg_solve with a context instead)\n", nx, ny, kStaticMaxCells);
+        return SHK_BAD_ARG;
+    }
+    if (o->precond != SHK_PRECOND_JACOBI || o->precision != SHK_FP64 ||
+        (o->stop_rule != SHK_STOP_KRYLOV && o->stop_rule != SHK_STOP_RELRES) || !(o->rtol >= 0) || !(o->atol >= 0)) {
+        fprintf(stderr, "shk_cg_solve_static: only the Float64 Jacobi-preconditioned solve is available here\n");
+        return SHK_BAD_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    int device = 0, sms = 148;
+    if (cudaGetDevice(&device) != cudaSuccess) return SHK_CUDA_ERROR;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return SHK_CUDA_ERROR;
+    void *base = nullptr;
+    int rc = static_scratch_address(device, &base);
+    if (rc) return rc;
+    const int n = nx * ny;
+    // launch geometry, as a context computes it
+    const long long tiles = (long long)((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY);
+    const int grid_stencil = (int)std::max(1LL, std::min((long long)sms * 6, tiles));
+    const long long tiles_x = (nx + kMarchX - 1) / kMarchX;
+    const int march_th = (int)std::min(64LL, std::max(8LL, (long long)ny * tiles_x / ((long long)sms * 12)));
+    const int march_blocks = (int)(tiles_x * ((ny + march_th - 1) / march_th));
+    const int grid_b = (int)std::max(1LL, std::min((long long)sms * 8,
+                                                   ((long long)n / 2 + (long long)kThreads * kUnrollB - 1) /
+                                                       ((long long)kThreads * kUnrollB)));
+    if (march_blocks > kStaticMaxBlocks || grid_stencil > kStaticMaxBlocks) return SHK_BAD_ARG;
+    char *b = (char *)base;
+    double *xc = (double *)(b), *r = (double *)(b + kStaticVecBytes);
+    double *p[2] = {(double *)(b + 2 * kStaticVecBytes), (double *)(b + 3 * kStaticVecBytes)};
+    double *Ap = (double *)(b + 4 * kStaticVecBytes);
+    double *partials = (double *)(b + 5 * kStaticVecBytes);
+    unsigned int *counter = (unsigned int *)(b + 5 * kStaticVecBytes + kStaticPartialBytes);
+    CgDev *cg = (CgDev *)(b + kStaticCgOffset);
+    CgDev init;
+    memset(&init, 0, sizeof(init));
+    init.atol = o->atol;
+    init.rtol = o->rtol;
+    init.itmax = o->itmax > 0 ? o->itmax : 2LL * n;
+    init.stop_rule = o->stop_rule;
+    init.first = 1;
+    k_static_init<<<1, 32, 0, s>>>(cg, init, counter);
+    k_cg_init<double, true><<<grid_stencil, kThreads, 0, s>>>(nx, ny, aP, aE, aN, x, rhs, r, xc, cg, partials, counter);
+    if (cudaGetLastError() != cudaSuccess) return SHK_CUDA_ERROR;
+    CgDev h;
+    long long enq = 0;
+    int batch = 8;
+    for (;;) {
+        if (cudaMemcpyAsync(&h, cg, sizeof(CgDev), cudaMemcpyDeviceToHost, s) != cudaSuccess) return SHK_CUDA_ERROR;
+        if (cudaStreamSynchronize(s) != cudaSuccess) return SHK_CUDA_ERROR;
+        if (h.done) break;
+        if (h.iter > h.itmax + 4 || enq > h.itmax + 2LL * 256 + 8) return SHK_CUDA_ERROR;
+        for (int k = 0; k < batch; k++, enq++) {
+            double *p_old = p[enq & 1], *p_new = p[(enq + 1) & 1];
+            k_cg_A<double, true><<<march_blocks, kMarchX, 0, s>>>(nx, ny, march_th, aP, aE, aN, r, nullptr, p_old,
+                                                                  p_new, Ap, cg, partials, counter, DBL_EPSILON);
+            k_cg_B<double, true><<<grid_b, kThreads, 0, s>>>(n, aP, p_new, Ap, xc, r, cg, partials, counter);
+        }
+        if (cudaGetLastError() != cudaSuccess) return SHK_CUDA_ERROR;
+        if (batch < 256) batch *= 2;
+    }
+    k_cg_finish<<<std::max(1, std::min(sms * 8, (n + kThreads - 1) / kThreads)), kThreads, 0, s>>>(n, xc, x);
+    if (cudaGetLastError() != cudaSuccess) return SHK_CUDA_ERROR;
+    if (cudaMemcpyAsync(&h, cg, sizeof(CgDev), cudaMemcpyDeviceToHost, s) != cudaSuccess) return SHK_CUDA_ERROR;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return SHK_CUDA_ERROR;
+    if (st) {
+        memset(st, 0, sizeof(*st));
+        st->niter = (long)h.iter;
+        st->status = h.status;
+        st->rnorm0 = h.rnorm0;
+        st->rnorm = h.rnorm;
+        st->lambda_min = st->lambda_max = 1.0;
+    }
+    return h.status;
+}
