@@ -98,7 +98,11 @@ typedef struct {
  *     residual, the refinement update and the stopping test stay Float64 (rel-res rule only).
  *     Each refinement replaces the Float32 residual by the Float64 true residual b - A h and
  *     continues the CG direction rather than restarting it. */
-enum { SHK_PRECOND_JACOBI = 0, SHK_PRECOND_CHEBYSHEV = 1 };
+/* SHK_PRECOND_MULTIGRID: this library's extension, the GPU counterpart of the reference's
+ * CPU-only AMGPreconditioner (src/preconditioner.jl:298-327): a Float32 aggregation-multigrid
+ * V-cycle (2x2 aggregation, Galerkin coarse operators in Laplacian form) inside the Float64 CG.
+ * Requires precision SHK_FP64 (the outer CG). */
+enum { SHK_PRECOND_JACOBI = 0, SHK_PRECOND_CHEBYSHEV = 1, SHK_PRECOND_MULTIGRID = 2 };
 enum { SHK_STOP_KRYLOV = 0, SHK_STOP_RELRES = 1 };
 enum { SHK_FP64 = 0, SHK_MIXED = 1 };
 typedef struct {

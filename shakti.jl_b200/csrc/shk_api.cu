@@ -6,6 +6,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
+#include <cstdlib>
 #include <new>
 #include <string>
 
@@ -65,6 +67,18 @@ static int ctx_alloc(Ctx *c) {
     size_t o_cr0 = carve(dN), o_cr1 = carve(dN), o_cp0 = carve(dN), o_cp1 = carve(dN);
     size_t o_f[15];
     for (int i = 0; i < 15; i++) o_f[i] = carve(fN);
+    // multigrid hierarchy: level 0 aliases the Float32 operator; levels >= 1 own their arrays
+    int dims[2 * kMgMaxLevels];
+    c->mg_levels = mg_levels_for(c->nx, c->ny, dims, kMgMaxLevels);
+    if (c->mg_levels < 1) return fail(c, SHK_BAD_ARG, "grid too large for the multigrid hierarchy");
+    size_t o_act0 = carve(n);
+    size_t o_mg[kMgMaxLevels][10];
+    for (int l = 1; l < c->mg_levels; l++) {
+        const size_t m = (size_t)dims[2 * l] * dims[2 * l + 1];
+        for (int k = 0; k < 3; k++) o_mg[l][k] = carve(m * sizeof(double));
+        for (int k = 3; k < 9; k++) o_mg[l][k] = carve(m * sizeof(float)); // aE, aN, dP, aP, x0, x1
+        o_mg[l][9] = carve(m * sizeof(float) + m);                       // b, then act bytes
+    }
     size_t o_part = carve((size_t)kMaxRedValues * c->max_blocks * sizeof(double));
     size_t o_cnt = carve(64);
     size_t o_dev = carve(sizeof(DevScalars));
@@ -83,6 +97,24 @@ static int ctx_alloc(Ctx *c) {
     float **fl[15] = {&c->aP32, &c->aE32, &c->aN32, &c->b32, &c->x32, &c->r32, &c->z32, &c->p32[0], &c->p32[1],
                       &c->Ap32, &c->cr32[0], &c->cr32[1], &c->cp32[0], &c->cp32[1], &c->dP32};
     for (int i = 0; i < 15; i++) *fl[i] = (float *)(b + o_f[i]);
+    for (int l = 0; l < c->mg_levels; l++) {
+        MgLevel &m = c->mg[l];
+        m.nx = dims[2 * l];
+        m.ny = dims[2 * l + 1];
+        if (l == 0) {
+            m.aE = c->aE32; m.aN = c->aN32; m.dP = c->dP32; m.aP = c->aP32;
+            m.act = (uint8_t *)(b + o_act0);
+            m.x[0] = c->cr32[0]; m.x[1] = c->cr32[1];
+            m.b = nullptr;
+            continue;
+        }
+        const size_t cnt = (size_t)m.nx * m.ny;
+        m.aE64 = (double *)(b + o_mg[l][0]); m.aN64 = (double *)(b + o_mg[l][1]); m.dP64 = (double *)(b + o_mg[l][2]);
+        m.aE = (float *)(b + o_mg[l][3]); m.aN = (float *)(b + o_mg[l][4]); m.dP = (float *)(b + o_mg[l][5]);
+        m.aP = (float *)(b + o_mg[l][6]); m.x[0] = (float *)(b + o_mg[l][7]); m.x[1] = (float *)(b + o_mg[l][8]);
+        m.b = (float *)(b + o_mg[l][9]);
+        m.act = (uint8_t *)(b + o_mg[l][9] + cnt * sizeof(float));
+    }
     c->partials = (double *)(b + o_part);
     c->counter = (unsigned int *)(b + o_cnt);
     c->dev = (DevScalars *)(b + o_dev);
@@ -169,6 +201,9 @@ SHK_API int shk_create(int nx, int ny, double lx, double ly, void *stream, void 
         c->march_th = (int)th;
         c->march_blocks = (int)(tiles_x * ((ny + th - 1) / th));
     }
+    if (const char *v = getenv("SHK_MG_NU")) c->mg_nu = std::max(1, atoi(v));
+    if (const char *v = getenv("SHK_MG_OMEGA")) c->mg_omega = (float)atof(v);
+    if (const char *v = getenv("SHK_MG_OMEGA_C")) c->mg_omega_c = (float)atof(v);
     c->max_blocks = c->grid_stencil > c->march_blocks ? c->grid_stencil : c->march_blocks;
     if (c->max_blocks < c->num_sms * 8) c->max_blocks = c->num_sms * 8;
     rc = ctx_alloc(c);
@@ -350,6 +385,9 @@ static int validate_cg(Ctx *c, const shk_cg_opts *o) {
     if (o->precond == SHK_PRECOND_CHEBYSHEV) {
         if (o->cheb_degree < 1) return fail(c, SHK_BAD_ARG, "ChebyshevPreconditioner: degree must be >= 1");
         if (o->cheb_nsteps < 2) return fail(c, SHK_BAD_ARG, "ChebyshevPreconditioner: nsteps_estimate must be >= 2");
+    } else if (o->precond == SHK_PRECOND_MULTIGRID) {
+        if (o->precision != SHK_FP64)
+            return fail(c, SHK_BAD_ARG, "the multigrid preconditioner runs inside the Float64 CG (precision SHK_FP64)");
     } else if (o->precond != SHK_PRECOND_JACOBI) {
         return fail(c, SHK_BAD_ARG, "unknown preconditioner");
     }

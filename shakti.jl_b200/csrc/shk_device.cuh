@@ -144,4 +144,83 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, u
     return true;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Scalar updates (run by thread 0 of the last block)
+// ---------------------------------------------------------------------------------------------
+static __device__ void cg_init_finish(CgDev *cg, double rz, double rr, double bb) {
+    if (cg->cont) {
+        // Residual replacement: keep the previous search direction, p = z + beta p with
+        // beta = r'z (replaced residual) / r'z (last recursive residual).
+        const double beta = rz / cg->rz_last;
+        if (isfinite(beta) && beta >= 0) {
+            cg->beta = beta;
+            cg->pNorm2 = rz + beta * beta * cg->pNorm2;
+            cg->first = 0;
+        } else {
+            cg->first = 1;
+            cg->beta = 0.0;
+            cg->pNorm2 = rz;
+        }
+    } else {
+        cg->first = 1;
+        cg->beta = 0.0;
+        cg->pNorm2 = rz;
+    }
+    cg->gamma = rz;
+    cg->rz_last = rz;
+    const double rn = sqrt(rz);
+    cg->rr = sqrt(rr);
+    cg->bnorm = sqrt(bb);
+    cg->rnorm0 = cg->stop_rule == SHK_STOP_KRYLOV ? rn : cg->rr;
+    cg->rnorm = cg->rnorm0;
+    cg->eps_stop = cg->atol + cg->rtol * rn;
+    cg->iter = 0;
+    if (isnan(rz) || isnan(rr)) {
+        cg->done = 1;
+        cg->status = SHK_BREAKDOWN;
+    } else if (rz == 0.0) {
+        cg->done = 1;
+        cg->status = SHK_OK;
+    } else {
+        bool solved = cg->stop_rule == SHK_STOP_KRYLOV ? (rn <= cg->eps_stop) : (cg->rr <= cg->rtol * cg->bnorm);
+        if (solved) {
+            cg->done = 1;
+            cg->status = SHK_OK;
+        } else if (cg->iter >= cg->itmax) {
+            cg->done = 1;
+            cg->status = SHK_NOT_CONVERGED;
+        } else {
+            cg->done = 0;
+        }
+    }
+}
+
+static __device__ void cg_iter_finish(CgDev *cg, double rz, double rr) {
+    const double rn = sqrt(rz), rrn = sqrt(rr);
+    cg->rz_last = rz;
+    cg->rr = rrn;
+    bool solved;
+    if (cg->stop_rule == SHK_STOP_KRYLOV) solved = (rn <= cg->eps_stop) || (rn + 1.0 <= 1.0);
+    else solved = rrn <= cg->rtol * cg->bnorm;
+    cg->rnorm = cg->stop_rule == SHK_STOP_KRYLOV ? rn : rrn;
+    if (!solved) {
+        double beta = rz / cg->gamma;
+        cg->pNorm2 = rz + beta * beta * cg->pNorm2;
+        cg->gamma = rz;
+        cg->beta = beta;
+        cg->first = 0;
+    }
+    cg->iter += 1;
+    if (isnan(rz) || isnan(rr)) {
+        cg->done = 1;
+        cg->status = SHK_BREAKDOWN;
+    } else if (solved) {
+        cg->done = 1;
+        cg->status = SHK_OK;
+    } else if (cg->iter >= cg->itmax) {
+        cg->done = 1;
+        cg->status = SHK_NOT_CONVERGED;
+    }
+}
+
 } // namespace shk

@@ -71,6 +71,17 @@ struct DevScalars {
     double ref_rr, ref_bb; // mixed precision: outer residual norms
 };
 
+// One level of the multigrid hierarchy (level 0 aliases the Float32 operator of the mixed form).
+struct MgLevel {
+    int nx = 0, ny = 0;
+    float *aE = nullptr, *aN = nullptr, *dP = nullptr, *aP = nullptr;
+    uint8_t *act = nullptr;
+    float *x[2] = {nullptr, nullptr};
+    float *b = nullptr;
+    double *aE64 = nullptr, *aN64 = nullptr, *dP64 = nullptr;
+};
+constexpr int kMgMaxLevels = 24;
+
 struct Params {
     double rho_w, rho_sw, rho_i, g, nu, n, omega, L, br, lr, ct, cw, p_atm, b_min, b_max, e_v;
     double nm1, inv_n;   // n-1, 1/n
@@ -113,6 +124,11 @@ struct Ctx {
     unsigned int *counter = nullptr;
     DevScalars *dev = nullptr;
     DevScalars *host_dev = nullptr;  // pinned mirror for read-back
+    MgLevel mg[kMgMaxLevels];
+    int mg_levels = 0;
+    int mg_nu = 2;           // damped-Jacobi sweeps before and after each coarse correction
+    float mg_omega = 0.8f;   // Jacobi damping
+    float mg_omega_c = 1.0f; // coarse-correction scaling
     int max_blocks = 0;
     int grid_stencil = 0;    // blocks for tile-stride kernels
     int march_th = 8;        // row-marching tile height
@@ -148,5 +164,10 @@ int cheb_set_bounds(Ctx *c, double lmin, double lmax);
 int launch_chebyshev_apply_standalone(Ctx *c, int degree, const double *x, double *y);
 int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st);
 int read_scalars(Ctx *c);
+
+// shk_mg.cu
+int mg_levels_for(int nx, int ny, int *dims, int maxl);
+int mg_setup(Ctx *c);
+int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init);
 
 } // namespace shk

@@ -15,6 +15,7 @@
 // B reads x, p, r, Ap, aP and writes x, r: 14 words (112 B in Float64, 56 B in Float32).
 #include <algorithm>
 #include <cstdlib>
+#include <type_traits>
 
 #include <cuda_pipeline.h>
 #include <cuda_runtime.h>
@@ -52,85 +53,6 @@ __global__ void __launch_bounds__(kThreads) k_matvec(int nx, int ny, const T *aP
         if (ix >= nx || iy >= ny) continue;
         size_t c = (size_t)ix + (size_t)iy * nx;
         y[c] = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, x[c], [&](size_t k) { return x[k]; });
-    }
-}
-
-// ---------------------------------------------------------------------------------------------
-// Scalar updates (run by thread 0 of the last block)
-// ---------------------------------------------------------------------------------------------
-__device__ void cg_init_finish(CgDev *cg, double rz, double rr, double bb) {
-    if (cg->cont) {
-        // Residual replacement: keep the previous search direction, p = z + beta p with
-        // beta = r'z (replaced residual) / r'z (last recursive residual).
-        const double beta = rz / cg->rz_last;
-        if (isfinite(beta) && beta >= 0) {
-            cg->beta = beta;
-            cg->pNorm2 = rz + beta * beta * cg->pNorm2;
-            cg->first = 0;
-        } else {
-            cg->first = 1;
-            cg->beta = 0.0;
-            cg->pNorm2 = rz;
-        }
-    } else {
-        cg->first = 1;
-        cg->beta = 0.0;
-        cg->pNorm2 = rz;
-    }
-    cg->gamma = rz;
-    cg->rz_last = rz;
-    const double rn = sqrt(rz);
-    cg->rr = sqrt(rr);
-    cg->bnorm = sqrt(bb);
-    cg->rnorm0 = cg->stop_rule == SHK_STOP_KRYLOV ? rn : cg->rr;
-    cg->rnorm = cg->rnorm0;
-    cg->eps_stop = cg->atol + cg->rtol * rn;
-    cg->iter = 0;
-    if (isnan(rz) || isnan(rr)) {
-        cg->done = 1;
-        cg->status = SHK_BREAKDOWN;
-    } else if (rz == 0.0) {
-        cg->done = 1;
-        cg->status = SHK_OK;
-    } else {
-        bool solved = cg->stop_rule == SHK_STOP_KRYLOV ? (rn <= cg->eps_stop) : (cg->rr <= cg->rtol * cg->bnorm);
-        if (solved) {
-            cg->done = 1;
-            cg->status = SHK_OK;
-        } else if (cg->iter >= cg->itmax) {
-            cg->done = 1;
-            cg->status = SHK_NOT_CONVERGED;
-        } else {
-            cg->done = 0;
-        }
-    }
-}
-
-__device__ void cg_iter_finish(CgDev *cg, double rz, double rr) {
-    const double rn = sqrt(rz), rrn = sqrt(rr);
-    cg->rz_last = rz;
-    cg->rr = rrn;
-    bool solved;
-    if (cg->stop_rule == SHK_STOP_KRYLOV) solved = (rn <= cg->eps_stop) || (rn + 1.0 <= 1.0);
-    else solved = rrn <= cg->rtol * cg->bnorm;
-    cg->rnorm = cg->stop_rule == SHK_STOP_KRYLOV ? rn : rrn;
-    if (!solved) {
-        double beta = rz / cg->gamma;
-        cg->pNorm2 = rz + beta * beta * cg->pNorm2;
-        cg->gamma = rz;
-        cg->beta = beta;
-        cg->first = 0;
-    }
-    cg->iter += 1;
-    if (isnan(rz) || isnan(rr)) {
-        cg->done = 1;
-        cg->status = SHK_BREAKDOWN;
-    } else if (solved) {
-        cg->done = 1;
-        cg->status = SHK_OK;
-    } else if (cg->iter >= cg->itmax) {
-        cg->done = 1;
-        cg->status = SHK_NOT_CONVERGED;
     }
 }
 
@@ -801,7 +723,17 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
                    int p_parity = 0, const T *lapl = nullptr) {
     const int nx = c->nx, ny = c->ny, n = nx * ny;
     const bool jac = o->precond == SHK_PRECOND_JACOBI;
+    const bool mg = o->precond == SHK_PRECOND_MULTIGRID;
     const int deg = o->cheb_degree;
+    // z = M^-1 r for the non-Jacobi preconditioners (with the CG dot r'z fused into the last pass)
+    auto apply_precond = [&](bool init) -> int {
+        if constexpr (std::is_same<T, double>::value) {
+            if (mg) return mg_apply(c, r, z, cgd, init);
+        }
+        if (init) enqueue_cheb<T, CG_INIT>(c, deg, aP, aE, aN, r, cr, cp, z, cgd);
+        else enqueue_cheb<T, CG_ITER>(c, deg, aP, aE, aN, r, cr, cp, z, cgd);
+        return SHK_OK;
+    };
     const double eps_curv = sizeof(T) == 8 ? DBL_EPSILON : (double)FLT_EPSILON;
     cudaError_t e = cudaMemcpyAsync(cgd, cgh, sizeof(CgDev), cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return check_cuda(c, e, "cg scalars upload");
@@ -813,7 +745,8 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
         k_cg_init<T, false><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, aP, aE, aN, x0, b, r, x, cgd,
                                                                         c->partials, c->counter);
         c->launches++;
-        enqueue_cheb<T, CG_INIT>(c, deg, aP, aE, aN, r, cr, cp, z, cgd);
+        int prc = apply_precond(true);
+        if (prc) return prc;
     }
     int rc = check_launch(c, "cg init");
     if (rc) return rc;
@@ -850,7 +783,8 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
                 k_cg_B<T, false><<<stream_grid(c, n, sizeof(T)), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd,
                                                                                            c->partials, c->counter);
                 c->launches += 2;
-                enqueue_cheb<T, CG_ITER>(c, deg, aP, aE, aN, r, cr, cp, z, cgd);
+                int prc = apply_precond(false);
+                if (prc) return prc;
             }
         }
         if ((rc = check_launch(c, "cg iterations"))) return rc;
@@ -866,8 +800,16 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
 
 int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
     const int nx = c->nx, ny = c->ny, n = nx * ny;
-    if (o->precond != SHK_PRECOND_JACOBI && o->precond != SHK_PRECOND_CHEBYSHEV)
+    if (o->precond != SHK_PRECOND_JACOBI && o->precond != SHK_PRECOND_CHEBYSHEV && o->precond != SHK_PRECOND_MULTIGRID)
         return fail(c, SHK_BAD_ARG, "unknown preconditioner");
+    if (o->precond == SHK_PRECOND_MULTIGRID) {
+        // Float32 Laplacian-form operator of level 0, then the coarse levels
+        k_to_float_lapl<<<flat_grid(c, n), kThreads, 0, c->stream>>>(nx, ny, c->aP, c->aE, c->aN, c->aP32, c->aE32,
+                                                                     c->aN32, c->dP32);
+        c->launches++;
+        int rc = mg_setup(c);
+        if (rc) return rc;
+    }
     if (o->precond == SHK_PRECOND_CHEBYSHEV) {
         if (o->cheb_degree < 1 || o->cheb_degree > kMaxChebDegree)
             return fail(c, SHK_BAD_ARG, "chebyshev_degree must be in [1, 32]");

@@ -204,7 +204,7 @@ class CGIterativeSolver(AbstractIterativeSolver):
     def __init__(self, g: Grid, lsy=MatrixFreeLinearSystem, *, chebyshev_degree: int | None = None,
                  chebyshev_nsteps_estimate: int = 15, amg: bool = False, precision: str = "fp64",
                  stop_rule: str = "krylov", atol: float | None = None, rtol: float | None = None, itmax: int = 0,
-                 inner_rtol: float = 1e-2, max_refine: int = 0, inner_itmax: int = 0):
+                 inner_rtol: float = 1e-2, max_refine: int = 0, inner_itmax: int = 0, multigrid: bool = False):
         if lsy is SparseAssembledLinearSystem:
             raise RuntimeError("CGIterativeSolver(g, SparseAssembledLinearSystem) is CPU-only; use "
                                "CGIterativeSolver(g, MatrixFreeLinearSystem) under the CUDA backend.")
@@ -214,6 +214,10 @@ class CGIterativeSolver(AbstractIterativeSolver):
             raise RuntimeError("AMGPreconditioner is CPU/SparseMatrixCSC-only (AlgebraicMultigrid.jl has no GPU array "
                                "support); use CGIterativeSolver(g, SparseAssembledLinearSystem; amg = true) instead, or "
                                "chebyshev_degree here for a GPU-capable accelerated preconditioner.")
+        if multigrid and chebyshev_degree is not None:
+            raise ValueError("chebyshev_degree and multigrid are mutually exclusive preconditioner choices; pick one.")
+        if multigrid and precision != "fp64":
+            raise ValueError("the multigrid preconditioner runs inside the Float64 CG (precision='fp64')")
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         if stop_rule not in ("krylov", "relres"):
@@ -233,12 +237,13 @@ class CGIterativeSolver(AbstractIterativeSolver):
         self.inner_rtol = float(inner_rtol)
         self.max_refine = int(max_refine)
         self.inner_itmax = int(inner_itmax)
+        self.multigrid = bool(multigrid)
         self.stats = CgStats()
 
     def opts(self) -> _lib.shk_cg_opts:
         cheb = self.precond is not None
         return _lib.default_cg_opts(
-            precond=1 if cheb else 0, cheb_degree=self.precond.degree if cheb else 4,
+            precond=2 if self.multigrid else (1 if cheb else 0), cheb_degree=self.precond.degree if cheb else 4,
             cheb_nsteps=self.precond.nsteps_estimate if cheb else 15,
             stop_rule=0 if self.stop_rule == "krylov" else 1, precision=0 if self.precision == "fp64" else 1,
             max_refine=self.max_refine, atol=self.atol, rtol=self.rtol, inner_rtol=self.inner_rtol,

@@ -327,3 +327,39 @@ def test_mixed_precision_run_field_errors(shk, orc, cuda):
         e_mixed = relerr(host[f], st_tight[f])
         e_plain = relerr(st[f], st_tight[f])
         assert e_mixed <= 10 * e_plain + 1e-9, (f, e_mixed, e_plain)
+
+
+@pytest.mark.parametrize("wname", ["fixture6", "plain64"])
+def test_multigrid_preconditioned_solve(shk, orc, cuda, wname):
+    """Float64 CG preconditioned by the Float32 aggregation-multigrid V-cycle reaches the Float64
+    true residual 1e-8 ||b|| in far fewer iterations than Jacobi, and lands as close to a tight solve
+    as the plain Float64 CG at the same tolerance."""
+    w = shk.configs.WORKLOADS[wname]()
+    g, pm, sl, osl, s, st = setup_pair(shk, orc, cuda, w, perturb=True)
+    A = orc.assemble(st, None)
+    ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, multigrid=True, stop_rule="relres", rtol=1e-8, atol=0.0)
+    stats = shk.solve_elliptic_linear_system(ls, s, g, pm, shk.Arithmetic(), sl)
+    assert stats.status == 0, stats
+    h = s.h.cpu().numpy()
+    res = np.linalg.norm(A["rhs"] - orc.matvec(A, h)) / np.linalg.norm(A["rhs"])
+    assert res <= 1e-8, res
+    x_tight, _ = orc.cg(A, st["h"], orc.CgSpec(precond=0, atol=0.0, rtol=1e-14))
+    x_plain, sp = orc.cg(A, st["h"], orc.CgSpec(precond=0, stop_rule=1, atol=0.0, rtol=1e-8))
+    assert relerr(h, x_tight) <= 10 * relerr(x_plain, x_tight) + 1e-12
+    assert stats.niter <= max(sp["niter"], 10)
+
+
+def test_multigrid_run_matches_oracle_tight(shk, orc, cuda):
+    """Five timesteps of the 64x64 workload with the multigrid form at a tight tolerance (rel-res
+    1e-13) agree with the Float64 oracle run (Jacobi CG, same tolerance) to 1e-8.  The two use
+    different Krylov iterates, so they agree to the solution accuracy that rel-res 1e-13 of ||b||
+    gives here (~1e-9), not to the 1e-10 that same-algorithm runs reach."""
+    w = shk.configs.plain64()
+    g, pm, sl, osl, s, st = setup_pair(shk, orc, cuda, w)
+    ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, multigrid=True, stop_rule="relres", rtol=1e-13,
+                               atol=0.0)
+    ps = shk.PicardSolver(500, 1e-6, ls, g)
+    sim = shk.Simulation(g, s, 5, 3600.0, pm, "implicit", [], shk.ConstantMeltInput(), sl, ps=ps)
+    shk.run(sim)
+    orc.run(st, None, osl, 5, 3600.0, cgspec=orc.CgSpec(precond=0, stop_rule=1, rtol=1e-13, atol=0.0))
+    assert_fields_close(s, st, tol=1e-8)
