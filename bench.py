@@ -1,14 +1,17 @@
 """Benchmark: converged timesteps/s of the SHAKTI head solve + field updates on the 4096^2 seasonal
 workload, rel-res 1e-8 linear solves, on 1..N GPUs (one independent replica instance per rank).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|mixed] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form multigrid|plain|fp32cg]
+                    [--impl ours|reference]
 
 One step is one timestep (update_ieb!, Picard to convergence with every CG solve at
-||b - A h||_2 <= 1e-8 ||b||_2, step_b!).  `value` times K device-resident steps with CUDA events
-after W warm-up steps; `e2e` re-runs the same K steps from the same state through the public API
-with each step's forcing (the ieb field) copied in from pinned host memory and the step's result
-(h and b) copied back.  The reference arm (--impl reference) times the CPU restatement of the
-reference algorithm on the host cores.
+||b - A h||_2 <= 1e-8 ||b||_2, step_b!).  `value` times K device-resident steps of the chosen form
+(default: Float64 CG preconditioned by the Float32 aggregation-multigrid V-cycle) with CUDA events
+after W warm-up steps; `plain_fp64_gpu` times the same window with plain Float64 Jacobi CG (the
+reference's algorithm on the GPU); `e2e` re-runs the chosen form's K steps from the same state
+through the public API with each step's forcing (the ieb field) copied in from pinned host memory
+and the step's result (h and b) copied back.  The reference arm (--impl reference) times the CPU
+restatement of the reference algorithm on the host cores.
 """
 from __future__ import annotations
 
@@ -30,16 +33,25 @@ import __graft_entry__ as entry  # noqa: E402
 
 METRIC = "converged timesteps/s at 4096² (rel-res 1e-8), chosen form vs plain FP64 GPU CG"
 UNIT = "timesteps/s"
-CG_WORDS = {"plain": 14, "mixed": 14}  # words per cell per CG iteration (A: 7, B: 7)
+# Algorithmic bytes per cell of one CG iteration.  Jacobi (Float64): k_cg_A reads aP, aE, aN, r,
+# p_old and writes p_new, Ap; k_cg_B reads aP, p_new, Ap, x, r and writes x, r (14 words).  With a
+# separate preconditioner, k_cg_A reads z instead of r (7 words) and k_cg_B does not read aP (6).
+CG_BYTES = {"plain": 14 * 8, "fp32cg": 14 * 4, "multigrid": 13 * 8}
+FORMS = {"multigrid": "Float64 CG + Float32 aggregation-multigrid V-cycle preconditioner",
+         "plain": "Float64 CG, Jacobi (the reference algorithm)",
+         "fp32cg": "Float32 Jacobi CG with Float64 residual replacement"}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=16)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--form", default="multigrid", choices=list(FORMS))
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain Float64 comparison pass")
+    ap.add_argument("--write-counts", default=None,
+                    help="write the plain pass's Picard/CG iteration counts of the timed window here")
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "chebyshev"])
     ap.add_argument("--workload", default="seasonal4096")
     ap.add_argument("--dt", type=float, default=1800.0)
@@ -49,7 +61,7 @@ def parse():
     ap.add_argument("--out", default=None, help="also write the JSON line here")
     ap.add_argument("--profile-cg", type=int, default=0,
                     help="profiling case: initialise the workload, assemble once and run exactly this many CG "
-                         "iterations (plain, then mixed inner), then exit")
+                         "iterations of each form, then exit")
     return ap.parse_args()
 
 
@@ -149,17 +161,19 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------------------------
-def make_sim(shk, w, args, state=None):
+def make_sim(shk, w, args, state=None, form=None):
     g = shk.Grid(w.nx, w.ny, w.lx, w.ly)
     p = shk.ModelParameters(**w.params)
     sl = shk.RegularizedCoulombSlidingLaw(w.sliding_C)
     s = state or shk.State(g)
     shk.set_initial_conditions(s, g, p, sl, **w.inputs)
+    form = form or args.form
     kw = dict(stop_rule="relres", rtol=1e-8, atol=0.0)
-    if args.form == "mixed":
+    if form == "fp32cg":
         kw.update(precision="mixed", inner_rtol=1e-2)
-    cheb = 4 if args.precond == "chebyshev" else None
-    ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, chebyshev_degree=cheb, **kw)
+    cheb = 4 if (args.precond == "chebyshev" and form != "multigrid") else None
+    ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, chebyshev_degree=cheb,
+                               multigrid=(form == "multigrid"), **kw)
     ps = shk.PicardSolver(500, 1e-6, ls, g)
     mi = shk.SeasonalBaseMeltInput(**w.melt) if w.melt else shk.ConstantMeltInput()
     sim = shk.Simulation(g, s, 1, args.dt, p, "implicit", [], mi, sl, ps=ps)
@@ -175,31 +189,127 @@ def run_steps(shk, sim, n, record=None):
             record.append(dict(picard=ps.last_iter, converged=ps.converged, cg=ps.cg_iters_total))
 
 
-def measure_cg_iteration(shk, sim, iters=200):
-    """Average duration of one CG iteration (kernels A + B) on the current assembled system, by
-    CUDA events around exactly `iters` iterations (rtol = 0, itmax = iters)."""
+def mg_vcycle_bytes(nx, ny, nu=2):
+    """Algorithmic bytes of one V-cycle per launch (all levels), for nu = 2 sweeps per side.
+    Level 0 (Float64 residual in, Float64 z out), per fine cell: first sweep 17 B, sweep 33 B,
+    restriction 26 B, prolongation + sweep 34 B, last sweep with z and the dots 37 B.  Coarse
+    levels (Float32), per cell: 13 + 29 + 22 + 30 + 29 B.  The levels that fit in one block's
+    shared memory (29 B per cell, 200 KiB) are read once (operator 17 B + b 4 B per cell) and level
+    lb's result written once (4 B per cell)."""
+    dims = [(nx, ny)]
+    while dims[-1] != (1, 1):
+        a, b = dims[-1]
+        dims.append(((a + 1) // 2, (b + 1) // 2))
+    cells = [a * b for a, b in dims]
+    lb = len(dims) - 1
+    rest = 0
+    for l in range(len(dims) - 1, 0, -1):
+        rest += cells[l]
+        if rest * 29 > 200 * 1024:
+            break
+        lb = l
+    total = 147 * cells[0] if len(dims) > 1 else 37 * cells[0]
+    for l in range(1, lb):
+        total += 123 * cells[l]
+    if len(dims) > 1:
+        total += 25 * cells[lb] + sum(17 * cells[l] for l in range(lb + 1, len(dims)))
+    return total
+
+
+def iteration_bytes(form, nx, ny):
+    cells = nx * ny
+    b = CG_BYTES[form] * cells
+    if form == "multigrid":
+        b += mg_vcycle_bytes(nx, ny)
+    return b
+
+
+def measure_cg_iteration(shk, sim, form, short=20, long=220):
+    """Average duration of one CG iteration of `form` (k_cg_A + k_cg_B, plus the V-cycle for the
+    multigrid form) on the current assembled system: CUDA events around a solve of exactly `long`
+    iterations minus one of `short` iterations (rtol = 0), so set-up and initial residual cancel."""
+    import ctypes as C
     import torch
     ls = sim.ls
-    saved = (ls.rtol, ls.atol, ls.itmax, ls.stop_rule, ls.precision)
+    saved = (ls.rtol, ls.atol, ls.itmax, ls.stop_rule, ls.precision, ls.max_refine, ls.inner_rtol)
     h0 = sim.state.h.clone()
-    ls.rtol, ls.atol, ls.itmax, ls.stop_rule, ls.precision = 0.0, 0.0, iters, "relres", "fp64"
     ctx = sim.ctx()
-    import ctypes as C
     assert ctx.L.shk_assemble(ctx.h, 0, 0.0) == 0
-    o = ls.opts()
-    st = shk._lib.shk_cg_stats()
-    ctx.L.shk_cg_solve(ctx.h, C.byref(o), C.byref(st))  # warm
+
+    def timed(iters):
+        ls.rtol, ls.atol, ls.itmax, ls.stop_rule = 0.0, 0.0, iters, "relres"
+        if form == "fp32cg":
+            ls.precision, ls.max_refine, ls.inner_rtol = "mixed", 1, 1e-30
+        o = ls.opts()
+        st = shk._lib.shk_cg_stats()
+        sim.state.h.copy_(h0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.L.shk_cg_solve(ctx.h, C.byref(o), C.byref(st))
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), int(st.niter)
+
+    timed(short)  # warm (graph capture, caches)
+    ms_s, n_s = timed(short)
+    ms_l, n_l = timed(long)
     sim.state.h.copy_(h0)
+    ls.rtol, ls.atol, ls.itmax, ls.stop_rule, ls.precision, ls.max_refine, ls.inner_rtol = saved
+    return (ms_l - ms_s) / max(n_l - n_s, 1), n_l - n_s
+
+
+def roofline_for(shk, sim, form, w, peaks):
+    it_ms, it_n = measure_cg_iteration(shk, sim, form)
+    nbytes = iteration_bytes(form, w.nx, w.ny)
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = nbytes / (it_ms / 1e3) / 1e9
+    kernel = {"plain": "k_cg_A + k_cg_B (one Jacobi-PCG iteration, Float64)",
+              "fp32cg": "k_cg_A + k_cg_B (one Jacobi-PCG iteration, Float32 Laplacian form)",
+              "multigrid": "one multigrid-preconditioned CG iteration: k_cg_A + k_cg_B (Float64) + the Float32 "
+                           "V-cycle (level kernels + k_mg_bottom + k_mg_last)"}[form]
+    r = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+         "frac": round(achieved / peak, 4), "traffic": None, "kernel": kernel,
+         "algorithmic_bytes_per_launch": nbytes, "us_per_iteration": round(it_ms * 1e3, 2),
+         "iterations_timed": it_n,
+         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s (of fallback)"}
+    tf = ROOT / "profiles" / f"traffic_{form}_{w.name}.json"
+    if tf.exists():
+        tr = json.loads(tf.read_text())
+        r["traffic"] = int(tr["dram_bytes_per_iteration"])
+        r["traffic_source"] = tr.get("source")
+    return r
+
+
+def timed_pass(shk, w, args, form, pg, clocks=None):
+    """W warm-up steps, then K timed steps of `form` (device-resident); returns the record."""
+    import torch
+    sim = make_sim(shk, w, args, form=form)
+    warm = []
+    run_steps(shk, sim, args.warmup, warm)
     torch.cuda.synchronize()
+    ctx = sim.ctx()
+    launches0 = ctx.launches()
+    barrier(pg)
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rec = []
     e0.record()
-    ctx.L.shk_cg_solve(ctx.h, C.byref(o), C.byref(st))
+    run_steps(shk, sim, args.steps, rec)
     e1.record()
     torch.cuda.synchronize()
+    barrier(pg)
+    clk = clocks.stop() if clocks else None
     ms = e0.elapsed_time(e1)
-    sim.state.h.copy_(h0)
-    ls.rtol, ls.atol, ls.itmax, ls.stop_rule, ls.precision = saved
-    return ms / max(st.niter, 1), int(st.niter)
+    return dict(sim=sim, rec=rec, warm=warm, ms=ms, ms_max=max_over_ranks(pg, ms),
+                launches=ctx.launches() - launches0, clocks=clk, h_after=sim.state.h.clone())
+
+
+def counts_of(rec):
+    return {"steps": len(rec), "picard_iters": sum(r["picard"] for r in rec), "cg_iters": sum(r["cg"] for r in rec),
+            "all_converged": all(r["converged"] for r in rec)}
 
 
 def ours(args, world, rank, local, pg):
@@ -210,50 +320,34 @@ def ours(args, world, rank, local, pg):
     if rank > 0:  # independent replica per rank: same shape, different seed
         w = shk.configs.seasonal_bench(w.nx, w.lx, seed=w.seed + 1000 * rank)
     cells = w.nx * w.ny
-
-    # ---- device-resident pass -------------------------------------------------------------
-    sim = make_sim(shk, w, args)
-    warm = []
-    run_steps(shk, sim, args.warmup, warm)
-    torch.cuda.synchronize()
-    ctx = sim.ctx()
-    launches0 = ctx.launches()
-    clocks = ClockSampler(torch.cuda.current_device())
-    barrier(pg)
-    torch.cuda.synchronize()
-    clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    rec = []
-    e0.record()
-    run_steps(shk, sim, args.steps, rec)
-    e1.record()
-    torch.cuda.synchronize()
-    barrier(pg)
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    launches = ctx.launches() - launches0
-    ms_max = max_over_ranks(pg, ms)
-    value = world * args.steps / (ms_max / 1e3)
-    state_after = sim.state.h.clone()
-
-    # dominant kernel: one CG iteration (k_cg_A + k_cg_B), measured live on the current system
-    it_ms, it_n = measure_cg_iteration(shk, sim)
-    bytes_per_iter = CG_WORDS["plain"] * 8 * cells
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = bytes_per_iter / (it_ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
-                "kernel": "k_cg_A + k_cg_B (one Jacobi-PCG iteration, Float64)",
-                "algorithmic_bytes_per_launch": bytes_per_iter, "us_per_iteration": round(it_ms * 1e3, 2),
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
-    traffic_file = ROOT / "profiles" / "cg_traffic_per_cell.json"
-    if traffic_file.exists():
-        tr = json.loads(traffic_file.read_text())
-        roofline["traffic"] = round(tr["bytes_per_cell_per_iteration"] * cells)
-        roofline["traffic_source"] = tr.get("source")
-    del sim
+
+    # ---- device-resident pass of the chosen form ---------------------------------------------
+    main = timed_pass(shk, w, args, args.form, pg, ClockSampler(torch.cuda.current_device()))
+    value = world * args.steps / (main["ms_max"] / 1e3)
+    roofline = roofline_for(shk, main["sim"], args.form, w, peaks)
+    state_after = main.pop("h_after")
+    del main["sim"]
     torch.cuda.empty_cache()
+
+    # ---- plain Float64 Jacobi CG on the GPU, same window -------------------------------------
+    plain = None
+    plain_rec = None
+    if not args.no_plain and args.form != "plain":
+        pp = timed_pass(shk, w, args, "plain", pg)
+        plain_rec = pp["rec"]
+        pv = world * args.steps / (pp["ms_max"] / 1e3)
+        plain = {"value": round(pv, 4), "unit": UNIT, "ms_per_step": round(pp["ms_max"] / args.steps, 3),
+                 "chosen_over_plain": round(value / pv, 3), "gpu_launches": int(sum_over_ranks(pg, pp["launches"])),
+                 "roofline": roofline_for(shk, pp["sim"], "plain", w, peaks), "timed_steps": counts_of(plain_rec)}
+        del pp
+        torch.cuda.empty_cache()
+    elif args.form == "plain":
+        plain_rec = main["rec"]
+    if args.write_counts and rank == 0 and plain_rec is not None:
+        Path(args.write_counts).write_text(json.dumps(
+            dict(counts_of(plain_rec), workload=w.name, warmup=args.warmup, form="plain Float64 Jacobi CG, relres 1e-8",
+                 per_step=plain_rec), indent=1) + "\n")
 
     # ---- end-to-end pass through the public API with host buffers ---------------------------
     e2e = None
@@ -261,7 +355,6 @@ def ours(args, world, rank, local, pg):
         sim = make_sim(shk, w, args)
         run_steps(shk, sim, args.warmup)
         mi = sim.mi
-        host_ieb = torch.empty((w.ny, w.nx), dtype=torch.float64).pin_memory()
         host_h = torch.empty((w.ny, w.nx), dtype=torch.float64).pin_memory()
         host_b = torch.empty((w.ny, w.nx), dtype=torch.float64).pin_memory()
         base_t = torch.from_numpy(np.ascontiguousarray(w.melt["base"].T)) if w.melt else None
@@ -298,37 +391,44 @@ def ours(args, world, rank, local, pg):
         del sim
         torch.cuda.empty_cache()
 
-    # ---- CPU baseline (rank 0, N = 1 only) --------------------------------------------------
+    # ---- CPU baseline (rank 0, N = 1 only): the reference algorithm's iteration counts --------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(shk, w, args, warm, rec)
+        counts_src = "this run's plain Float64 pass"
+        rec = plain_rec
+        if rec is None:
+            cf = ROOT / "profiles" / f"step_counts_{w.name}.json"
+            if cf.exists():
+                rec, counts_src = json.loads(cf.read_text())["per_step"], cf.name
+            else:
+                rec, counts_src = main["rec"], "the chosen form's own counts (plain counts unavailable)"
+        cpu = cpu_baseline(shk, w, args, rec, counts_src)
 
-    total_cg = sum(r["cg"] for r in rec)
-    total_pic = sum(r["picard"] for r in rec)
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "plain" else "f32+f64",
+        "warmup": args.warmup, "ms_per_step": round(main["ms_max"] / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": {"plain": "f64", "fp32cg": "f32+f64", "multigrid": "f64+f32"}[args.form],
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": f"{w.name}: {w.nx}x{w.ny} cells, {w.lx / 1e3:g} km, seasonal melt + 64 moulins, "
                                f"10% LAND/OTHER_BASIN blobs",
-                   "form": f"{args.form}-{args.precond}", "stop": "relres 1e-8 (||b-Ah||/||b||)",
+                   "form": FORMS[args.form], "stop": "relres 1e-8 (||b-Ah||/||b||, Float64)",
                    "picard": "500 iters, tol 1e-6", "dt_s": args.dt, "sliding": f"RegularizedCoulomb C={w.sliding_C}",
                    "params": w.params, "gap": "implicit", "kface": "arithmetic",
                    "l2": "inputs larger than L2 (about 8 GB resident per GPU)",
                    "parallelism": f"replicas x{world} (independent instances, no data-path collective)"},
         "roofline": roofline,
+        "plain_fp64_gpu": plain,
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": int(sum_over_ranks(pg, launches)),
-        "clocks": clk,
-        "timed_steps": {"picard_iters": total_pic, "cg_iters": total_cg,
-                        "per_step": rec, "all_converged": all(r["converged"] for r in rec)},
+        "gpu_launches": int(sum_over_ranks(pg, main["launches"])),
+        "clocks": main["clocks"],
+        "timed_steps": dict(counts_of(main["rec"]), per_step=main["rec"]),
     }
     return line
 
 
-def cpu_baseline(shk, w, args, warm, rec):
+def cpu_baseline(shk, w, args, rec, counts_src):
     """The CPU restatement of the reference algorithm on the host cores, on a bounded sample of
     the same workload: the 4096^2 initial state, timing one assembly, one field-update tail, one
     gap step and a run of Jacobi CG iterations; the timestep rate is these costs combined with the
@@ -348,7 +448,7 @@ def cpu_baseline(shk, w, args, warm, rec):
                        f"1 assembly ({costs['assemble_s']:.3f} s), 1 tail ({costs['tail_s']:.3f} s), 1 gap step "
                        f"({costs['gap_s']:.3f} s), {costs['cg_iters']} Jacobi CG iterations "
                        f"({costs['cg_iter_s'] * 1e3:.1f} ms each); rate = these costs x the timed window's "
-                       f"{pic} Picard and {cg} CG iterations over {steps} steps"),
+                       f"{pic} Picard and {cg} CG iterations over {steps} steps ({counts_src})"),
             "costs": costs}
 
 
@@ -398,7 +498,7 @@ def reference(args, world, rank, local, pg):
     orc = entry.load_oracle()
     orc.build()
     w = shk.configs.WORKLOADS[args.workload]()
-    counts_file = ROOT / "profiles" / "step_counts_seasonal4096.json"
+    counts_file = ROOT / "profiles" / f"step_counts_{w.name}.json"
     counts = json.loads(counts_file.read_text()) if counts_file.exists() else None
     threads = os.cpu_count() or 1
     orc.set_num_threads(threads)
@@ -432,8 +532,8 @@ def reference(args, world, rank, local, pg):
 
 
 def profile_cg(args):
-    """Small, self-ending case for ncu: one assembly and exactly args.profile_cg CG iterations in
-    Float64 and in Float32 (mixed inner) on the workload's initial state."""
+    """Small, self-ending case for ncu: one assembly and exactly args.profile_cg CG iterations of
+    the selected form on the workload's initial state."""
     import ctypes as C
     import torch
     shk = entry.load_package()
@@ -441,20 +541,19 @@ def profile_cg(args):
     sim = make_sim(shk, w, args)
     ctx = sim.ctx()
     assert ctx.L.shk_assemble(ctx.h, 0, 0.0) == 0
-    out = {}
-    for prec in ("fp64", "mixed"):
-        ls = sim.ls
-        ls.precision, ls.stop_rule, ls.rtol, ls.atol, ls.itmax = prec, "relres", 0.0, 0.0, args.profile_cg
+    ls = sim.ls
+    ls.stop_rule, ls.rtol, ls.atol, ls.itmax = "relres", 0.0, 0.0, args.profile_cg
+    if args.form == "fp32cg":
         ls.max_refine = 1
-        o = ls.opts()
-        if prec == "mixed":
-            o.inner_rtol = 1e-30  # inner solve runs exactly itmax iterations
-        st = shk._lib.shk_cg_stats()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ctx.L.shk_cg_solve(ctx.h, C.byref(o), C.byref(st))
-        torch.cuda.synchronize()
-        out[prec] = dict(niter=st.niter, ms=round((time.perf_counter() - t0) * 1e3, 3))
+    o = ls.opts()
+    if args.form == "fp32cg":
+        o.inner_rtol = 1e-30  # the inner solve runs exactly itmax iterations
+    st = shk._lib.shk_cg_stats()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.L.shk_cg_solve(ctx.h, C.byref(o), C.byref(st))
+    torch.cuda.synchronize()
+    out = dict(form=args.form, niter=st.niter, ms=round((time.perf_counter() - t0) * 1e3, 3))
     print(json.dumps({"profile_cg": out, "workload": w.name, "cells": w.nx * w.ny}))
 
 

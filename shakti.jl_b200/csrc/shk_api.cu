@@ -204,6 +204,13 @@ SHK_API int shk_create(int nx, int ny, double lx, double ly, void *stream, void 
     if (const char *v = getenv("SHK_MG_NU")) c->mg_nu = std::max(1, atoi(v));
     if (const char *v = getenv("SHK_MG_OMEGA")) c->mg_omega = (float)atof(v);
     if (const char *v = getenv("SHK_MG_OMEGA_C")) c->mg_omega_c = (float)atof(v);
+    // SHK_CG_GRAPHS: 0 issues each CG iteration's kernels directly, 1 replays one CUDA graph per
+    // iteration in host-sized batches, 2 (default) runs the whole iteration loop as one graph with a
+    // device-side WHILE node
+    if (const char *v = getenv("SHK_CG_GRAPHS")) {
+        c->graph_mode = std::min(2, std::max(0, atoi(v)));
+        c->graphs_disabled = c->graph_mode == 0;
+    }
     c->max_blocks = c->grid_stencil > c->march_blocks ? c->grid_stencil : c->march_blocks;
     if (c->max_blocks < c->num_sms * 8) c->max_blocks = c->num_sms * 8;
     rc = ctx_alloc(c);
@@ -222,6 +229,9 @@ SHK_API int shk_destroy(void *ctx) {
     if (!c) return SHK_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     else cudaDeviceSynchronize();
+    for (auto &g : c->graphs) cudaGraphExecDestroy(g.exec);
+    c->graphs.clear();
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     if (c->arena) cudaFree(c->arena);
     if (c->host_dev) cudaFreeHost(c->host_dev);
     delete c;

@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <vector>
 
 #include "../../include/shakti_b200.h"
 
@@ -47,6 +48,7 @@ struct CgDev {
     long long iter, itmax;
     int done, status, first, stop_rule;
     int cont;        // init continues the previous search direction instead of restarting
+    unsigned int trips;  // trips of the device-side iteration loop (bounded)
 };
 
 struct ChebDev {
@@ -134,6 +136,17 @@ struct Ctx {
     int march_th = 8;        // row-marching tile height
     int march_blocks = 1;    // row-marching grid (one block per kMarchX x march_th tile)
     long long launches = 0;
+    // CUDA graphs of the CG iteration loop, keyed by precision, preconditioner, degree, p parity
+    struct GraphSlot {
+        long long key;
+        cudaGraphExec_t exec;
+        long long launches;  // kernels per replay (per trip for the device loop)
+    };
+    std::vector<GraphSlot> graphs;
+    cudaStream_t cap_stream = nullptr;  // capture only; nothing executes on it
+    int graph_mode = 2;                 // 0 direct launches, 1 one graph per iteration, 2 device-side loop
+    bool graphs_disabled = false;       // set when capture fails: direct launches from then on
+    bool loop_disabled = false;         // set when the device-loop graph cannot be built
     std::string err;
     bool assembled = false;
     bool assembled_parabolic = false;

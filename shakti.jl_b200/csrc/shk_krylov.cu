@@ -14,6 +14,7 @@
 // Algorithmic traffic per cell and iteration: A reads r, aP, p_old, aE, aN and writes p, Ap;
 // B reads x, p, r, Ap, aP and writes x, r: 14 words (112 B in Float64, 56 B in Float32).
 #include <algorithm>
+#include <functional>
 #include <cstdlib>
 #include <type_traits>
 
@@ -702,6 +703,14 @@ int launch_chebyshev_apply_standalone(Ctx *c, int degree, const double *x, doubl
     return check_launch(c, "chebyshev apply");
 }
 
+// Condition of the device-side CG loop: another trip (two iterations) while the solve has not
+// stopped, and never more than itmax/2 + 8 trips, so the loop ends whatever the flags say.
+__global__ void k_cg_loop_cond(CgDev *cg, cudaGraphConditionalHandle h) {
+    const unsigned int t = ++cg->trips;
+    const bool more = !*(volatile int *)&cg->done && 2LL * (long long)t < cg->itmax + 16;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
 static CgDev make_cg_init(const shk_cg_opts *o, long long n, bool inner, double inner_rtol) {
     CgDev g;
     memset(&g, 0, sizeof(g));
@@ -735,6 +744,7 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
         return SHK_OK;
     };
     const double eps_curv = sizeof(T) == 8 ? DBL_EPSILON : (double)FLT_EPSILON;
+    cgh->trips = 0;
     cudaError_t e = cudaMemcpyAsync(cgd, cgh, sizeof(CgDev), cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return check_cuda(c, e, "cg scalars upload");
     if (jac) {
@@ -750,6 +760,133 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
     }
     int rc = check_launch(c, "cg init");
     if (rc) return rc;
+
+    // One CG iteration: stencil + p update + p'Ap (k_cg_A), x/r update (k_cg_B), preconditioner.
+    // Every kernel returns at once when the device-side stop flag is set.
+    auto enqueue_iteration = [&](int par) -> int {
+        T *p_old = p[par], *p_new = p[par ^ 1];
+        if (jac && lapl) {
+            k_cg_A<T, true, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(
+                nx, ny, c->march_th, aP, aE, aN, r, nullptr, p_old, p_new, Ap, cgd, c->partials, c->counter, eps_curv,
+                lapl);
+        } else if (jac) {
+            k_cg_A<T, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(nx, ny, c->march_th, aP, aE, aN, r, nullptr,
+                                                                       p_old, p_new, Ap, cgd, c->partials, c->counter,
+                                                                       eps_curv);
+        } else if (lapl) {
+            k_cg_A<T, false, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(
+                nx, ny, c->march_th, aP, aE, aN, r, z, p_old, p_new, Ap, cgd, c->partials, c->counter, eps_curv, lapl);
+        } else {
+            k_cg_A<T, false><<<c->march_blocks, kMarchX, 0, c->stream>>>(nx, ny, c->march_th, aP, aE, aN, r, z, p_old,
+                                                                        p_new, Ap, cgd, c->partials, c->counter,
+                                                                        eps_curv);
+        }
+        if (jac)
+            k_cg_B<T, true><<<stream_grid(c, n, sizeof(T)), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd,
+                                                                                      c->partials, c->counter);
+        else
+            k_cg_B<T, false><<<stream_grid(c, n, sizeof(T)), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd,
+                                                                                       c->partials, c->counter);
+        c->launches += 2;
+        if (!jac) return apply_precond(false);
+        return SHK_OK;
+    };
+
+    // Graphs are keyed by everything that their kernel arguments depend on within one context.
+    const long long key_base = ((long long)(lapl != nullptr) << 41) | ((long long)(sizeof(T) == 4) << 40) |
+                               ((long long)o->precond << 32) | ((long long)deg << 8);
+    // Records enqueue() on the context's private capture stream (the caller's stream may be the
+    // legacy default stream, which cannot be captured), into *graph when `into`, else into a new
+    // graph returned in *graph.  Nothing executes.  Returns the launches recorded, or -1.
+    auto capture = [&](cudaGraph_t *graph, bool into, const std::function<int()> &enqueue) -> long long {
+        cudaError_t ce = cudaSuccess;
+        if (!c->cap_stream) ce = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking);
+        if (ce != cudaSuccess) return -1;
+        ce = into ? cudaStreamBeginCaptureToGraph(c->cap_stream, *graph, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal)
+                  : cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+        if (ce != cudaSuccess) return -1;
+        const long long before = c->launches;
+        cudaStream_t user = c->stream;
+        c->stream = c->cap_stream;
+        const int irc = enqueue();
+        c->stream = user;
+        cudaGraph_t g = nullptr;
+        ce = cudaStreamEndCapture(c->cap_stream, &g);
+        const long long recorded = c->launches - before;
+        c->launches = before;
+        if (ce != cudaSuccess || irc != SHK_OK) {
+            if (g && !into) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return -1;
+        }
+        if (!into) *graph = g;
+        return recorded;
+    };
+
+    // Mode 2: the whole iteration loop as one graph.  A WHILE node runs a body of two iterations (the
+    // search-direction buffers alternate within the body) and k_cg_loop_cond, which clears the
+    // loop condition once the solve stops (or at the trip bound).  The host waits once per solve,
+    // and no iteration is issued past the stop.
+    if (c->graph_mode == 2 && !c->loop_disabled) {
+        const long long key = key_base | (1LL << 42) | p_parity;
+        Ctx::GraphSlot *slot = nullptr;
+        for (auto &g : c->graphs)
+            if (g.key == key) slot = &g;
+        if (!slot) {
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            long long per_trip = -1;
+            cudaGraphConditionalHandle handle;
+            bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess &&
+                      cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+            if (ok) {
+                cudaGraphNodeParams np = {};
+                np.type = cudaGraphNodeTypeConditional;
+                np.conditional.handle = handle;
+                np.conditional.type = cudaGraphCondTypeWhile;
+                np.conditional.size = 1;
+                cudaGraphNode_t node;
+                ok = cudaGraphAddNode(&node, graph, nullptr, 0, &np) == cudaSuccess;
+                if (ok) {
+                    cudaGraph_t body = np.conditional.phGraph_out[0];
+                    per_trip = capture(&body, true, [&]() -> int {
+                        int rc2 = enqueue_iteration(p_parity);
+                        if (!rc2) rc2 = enqueue_iteration(p_parity ^ 1);
+                        if (rc2) return rc2;
+                        k_cg_loop_cond<<<1, 1, 0, c->stream>>>(cgd, handle);
+                        c->launches++;
+                        return check_launch(c, "cg loop condition");
+                    });
+                    ok = per_trip > 0 && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+                }
+            }
+            if (graph) cudaGraphDestroy(graph);
+            if (!ok) {
+                cudaGetLastError();
+                if (exec) cudaGraphExecDestroy(exec);
+                c->loop_disabled = true;  // per-iteration graphs from now on
+            } else {
+                c->graphs.push_back({key, exec, per_trip});
+                slot = &c->graphs.back();
+            }
+        }
+        if (slot) {
+            if ((rc = read_cg_flags(c, cgh, cgd))) return rc;
+            if (!cgh->done) {
+                e = cudaGraphLaunch(slot->exec, c->stream);
+                if (e != cudaSuccess) return check_cuda(c, e, "cg loop graph launch");
+                if ((rc = read_cg_flags(c, cgh, cgd))) return rc;
+                c->launches += slot->launches * (long long)cgh->trips;
+                if (!cgh->done) return fail(c, SHK_CUDA_ERROR, "cg device loop reached its trip bound before stopping");
+            }
+            if (iters_out) *iters_out = (long)cgh->iter;
+            return SHK_OK;
+        }
+    }
+
+    // Modes 0 and 1: batches of iterations issued by the host (8, 16, ... 256), the stop flag read
+    // between batches; in mode 1 each iteration is one replay of a captured graph.
     long long enq = 0;
     int batch = 8;
     const int batch_max = 256;
@@ -757,35 +894,35 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
         if ((rc = read_cg_flags(c, cgh, cgd))) return rc;
         if (cgh->done) break;
         for (int b2 = 0; b2 < batch; b2++, enq++) {
-            T *p_old = p[(enq + p_parity) & 1], *p_new = p[(enq + p_parity + 1) & 1];
-            if (jac && lapl) {
-                k_cg_A<T, true, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(
-                    nx, ny, c->march_th, aP, aE, aN, r, nullptr, p_old, p_new, Ap, cgd, c->partials, c->counter, eps_curv,
-                    lapl);
-                k_cg_B<T, true><<<stream_grid(c, n, sizeof(T)), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd,
-                                                                                          c->partials, c->counter);
-            } else if (jac) {
-                k_cg_A<T, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(nx, ny, c->march_th, aP, aE, aN, r, nullptr,
-                                                                           p_old, p_new, Ap, cgd, c->partials, c->counter,
-                                                                           eps_curv);
-                k_cg_B<T, true><<<stream_grid(c, n, sizeof(T)), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd,
-                                                                                          c->partials, c->counter);
-                c->launches += 2;
-            } else {
-                if (lapl)
-                    k_cg_A<T, false, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(
-                        nx, ny, c->march_th, aP, aE, aN, r, z, p_old, p_new, Ap, cgd, c->partials, c->counter, eps_curv,
-                        lapl);
-                else
-                    k_cg_A<T, false><<<c->march_blocks, kMarchX, 0, c->stream>>>(nx, ny, c->march_th, aP, aE, aN, r, z,
-                                                                                p_old, p_new, Ap, cgd, c->partials,
-                                                                                c->counter, eps_curv);
-                k_cg_B<T, false><<<stream_grid(c, n, sizeof(T)), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd,
-                                                                                           c->partials, c->counter);
-                c->launches += 2;
-                int prc = apply_precond(false);
-                if (prc) return prc;
+            const int par = (int)((enq + p_parity) & 1);
+            if (c->graph_mode >= 1 && !c->graphs_disabled) {
+                const long long key = key_base | par;
+                cudaGraphExec_t exec = nullptr;
+                for (auto &g : c->graphs)
+                    if (g.key == key) {
+                        exec = g.exec;
+                        c->launches += g.launches;
+                    }
+                if (!exec) {
+                    cudaGraph_t graph = nullptr;
+                    const long long rec = capture(&graph, false, [&]() { return enqueue_iteration(par); });
+                    if (rec < 0 || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+                        cudaGetLastError();
+                        c->graphs_disabled = true;  // direct launches from now on
+                        exec = nullptr;
+                    } else {
+                        c->graphs.push_back({key, exec, rec});
+                        c->launches += rec;
+                    }
+                    if (graph) cudaGraphDestroy(graph);
+                }
+                if (exec) {
+                    e = cudaGraphLaunch(exec, c->stream);
+                    if (e != cudaSuccess) return check_cuda(c, e, "cg iteration graph launch");
+                    continue;
+                }
             }
+            if ((rc = enqueue_iteration(par))) return rc;
         }
         if ((rc = check_launch(c, "cg iterations"))) return rc;
         if (batch < batch_max) batch *= 2;

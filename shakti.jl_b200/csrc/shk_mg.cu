@@ -12,8 +12,8 @@
 // Identity rows (OCEAN/LAND/OTHER_BASIN cells: aP = 1, no couplings) are not aggregated (their row
 // of P is zero); the smoother solves them exactly.  The V-cycle is symmetric (the same damped-Jacobi
 // sweeps before and after the coarse correction; exact solve on the 1x1 coarsest level), so it is
-// a valid CG preconditioner.  Per level: nu damped-Jacobi sweeps (omega = 2/3) before and after,
-// coarse correction scaled by omega_c.
+// a valid CG preconditioner.  Per level: nu damped-Jacobi sweeps (omega) before and after, coarse
+// correction scaled by omega_c; the levels that fit in one block's shared memory run as one kernel.
 #include <cuda_runtime.h>
 #include <float.h>
 #include <string.h>
@@ -103,7 +103,10 @@ struct Lv {
     int nx, ny;
     const float *aE, *aN, *dP, *aP;
     const uint8_t *act;
+    const int *done;  // the outer CG's stop flag: V-cycles issued after the stop do no work
 };
+
+__device__ __forceinline__ bool cg_finished(const int *done) { return done && *(const volatile int *)done; }
 
 // (A x)_c in Laplacian form, with x given by a functor (so fused kernels can form x on the fly)
 template <typename F>
@@ -118,46 +121,59 @@ __device__ __forceinline__ float lapl_apply(const Lv &L, int ix, int iy, size_t 
 
 __device__ __forceinline__ float omega_of(const Lv &L, size_t c, float w) { return L.act[c] ? w : 1.0f; }
 
+// The level kernels use a 2D grid of 32 x 8 blocks, one thread per cell (no div/mod per cell).
+#define CELL2D()                                                                                      \
+    if (cg_finished(L.done)) return;                                                                  \
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y; \
+    const bool inside = ix < L.nx && iy < L.ny;                                                       \
+    const size_t k = (size_t)ix + (size_t)iy * L.nx;
+
 // First pre-smoothing sweep from x = 0: x = omega b / aP.  Level 0 reads b in Float64 (the outer
 // residual).
 template <typename TB>
 __global__ void k_mg_pre0(Lv L, const TB *b, float *x, float w) {
-    GSTRIDE(k, L.nx * L.ny) x[k] = omega_of(L, k, w) * (float)b[k] / L.aP[k];
+    CELL2D();
+    if (inside) x[k] = omega_of(L, k, w) * (float)b[k] / L.aP[k];
 }
 
 // One damped-Jacobi sweep: xo = xi + omega (b - A xi) / aP.
 template <typename TB>
 __global__ void k_mg_sweep(Lv L, const TB *b, const float *xi, float *xo, float w) {
-    GSTRIDE(k, L.nx * L.ny) {
-        const int ix = k % L.nx, iy = k / L.nx;
-        const float xc = xi[k];
-        const float ax = lapl_apply(L, ix, iy, k, xc, [&](size_t q) { return xi[q]; });
-        xo[k] = xc + omega_of(L, k, w) * ((float)b[k] - ax) / L.aP[k];
-    }
+    CELL2D();
+    if (!inside) return;
+    const float xc = xi[k];
+    const float ax = lapl_apply(L, ix, iy, k, xc, [&](size_t q) { return xi[q]; });
+    xo[k] = xc + omega_of(L, k, w) * ((float)b[k] - ax) / L.aP[k];
 }
 
 // Restriction of the residual: bc(C) = sum over the active fine cells of aggregate C of (b - A x).
+// One thread per coarse cell (2D grid over the coarse level).
 template <typename TB>
 __global__ void k_mg_restrict(Lv L, const TB *b, const float *x, int nxc, int nyc, float *bc) {
-    GSTRIDE(k, nxc * nyc) {
-        const int I = k % nxc, J = k / nxc;
-        float s = 0.0f;
-        for (int dj = 0; dj < 2; dj++)
-            for (int di = 0; di < 2; di++) {
-                const int i = 2 * I + di, j = 2 * J + dj;
-                if (i >= L.nx || j >= L.ny) continue;
-                const size_t c = (size_t)i + (size_t)j * L.nx;
-                if (!L.act[c]) continue;
-                const float ax = lapl_apply(L, i, j, c, x[c], [&](size_t q) { return x[q]; });
-                s += (float)b[c] - ax;
-            }
-        bc[k] = s;
-    }
+    if (cg_finished(L.done)) return;
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= nxc || J >= nyc) return;
+    float s = 0.0f;
+#pragma unroll
+    for (int dj = 0; dj < 2; dj++)
+#pragma unroll
+        for (int di = 0; di < 2; di++) {
+            const int i = 2 * I + di, j = 2 * J + dj;
+            if (i >= L.nx || j >= L.ny) continue;
+            const size_t c = (size_t)i + (size_t)j * L.nx;
+            if (!L.act[c]) continue;
+            const float ax = lapl_apply(L, i, j, c, x[c], [&](size_t q) { return x[q]; });
+            s += (float)b[c] - ax;
+        }
+    bc[(size_t)I + (size_t)J * nxc] = s;
 }
 
-// Coarsest level (1 x 1): exact solve.
-__global__ void k_mg_coarsest(Lv L, const float *b, float *x) {
-    GSTRIDE(k, L.nx * L.ny) x[k] = L.act[k] ? b[k] / L.dP[k] : b[k];
+// x + omega_c (P xc) at fine cell (i, j) = q
+__device__ __forceinline__ float prolonged(const Lv &L, const float *xi, const float *xc, int nxc, float wc, int i,
+                                           int j, size_t q) {
+    float v = xi[q];
+    if (L.act[q]) v += wc * xc[(size_t)(i >> 1) + (size_t)(j >> 1) * nxc];
+    return v;
 }
 
 // Prolongation fused with the first post-smoothing sweep:
@@ -165,42 +181,40 @@ __global__ void k_mg_coarsest(Lv L, const float *b, float *x) {
 template <typename TB>
 __global__ void k_mg_prolong_sweep(Lv L, const TB *b, const float *xi, const float *xc, int nxc, float wc, float w,
                                    float *xo) {
-    GSTRIDE(k, L.nx * L.ny) {
-        const int ix = k % L.nx, iy = k / L.nx;
-        auto xt = [&](size_t q) -> float {
-            const int qi = (int)(q % L.nx), qj = (int)(q / L.nx);
-            float v = xi[q];
-            if (L.act[q]) v += wc * xc[(size_t)(qi >> 1) + (size_t)(qj >> 1) * nxc];
-            return v;
-        };
-        const float xk = xt(k);
-        const float ax = lapl_apply(L, ix, iy, k, xk, xt);
-        xo[k] = xk + omega_of(L, k, w) * ((float)b[k] - ax) / L.aP[k];
-    }
+    CELL2D();
+    if (!inside) return;
+    const float xk = prolonged(L, xi, xc, nxc, wc, ix, iy, k);
+    float y = L.dP[k] * xk;
+    if (ix < L.nx - 1) y += L.aE[k] * (xk - prolonged(L, xi, xc, nxc, wc, ix + 1, iy, k + 1));
+    if (ix > 0) y += L.aE[k - 1] * (xk - prolonged(L, xi, xc, nxc, wc, ix - 1, iy, k - 1));
+    if (iy < L.ny - 1) y += L.aN[k] * (xk - prolonged(L, xi, xc, nxc, wc, ix, iy + 1, k + L.nx));
+    if (iy > 0) y += L.aN[k - L.nx] * (xk - prolonged(L, xi, xc, nxc, wc, ix, iy - 1, k - L.nx));
+    xo[k] = xk + omega_of(L, k, w) * ((float)b[k] - y) / L.aP[k];
 }
 
 // Last post-smoothing sweep on level 0, writing z in Float64 and finishing the outer CG's r'z:
-// z = xi + omega (r - A xi)/aP; partials r'z, r'r -> init or iteration finish.
+// z = xt + omega (r - A xt)/aP (xt = xi, plus the prolonged coarse correction when PROLONG);
+// partials r'z, r'r -> init or iteration finish.  1D grid (the grid reduction is 1D).
 template <bool PROLONG>
 __global__ void __launch_bounds__(kThreads) k_mg_last(Lv L, const double *r, const float *xi, const float *xc, int nxc,
                                                       float wc, float w, double *z, CgDev *cg, int init,
                                                       double *partials, unsigned int *counter) {
     if (*(volatile int *)&cg->done) return;
     double red[2] = {0.0, 0.0};
-    GSTRIDE(k, L.nx * L.ny) {
-        const int ix = k % L.nx, iy = k / L.nx;
-        auto xt = [&](size_t q) -> float {
-            float v = xi[q];
-            if (PROLONG && L.act[q]) {
-                const int qi = (int)(q % L.nx), qj = (int)(q / L.nx);
-                v += wc * xc[(size_t)(qi >> 1) + (size_t)(qj >> 1) * nxc];
-            }
-            return v;
+    GSTRIDE(kk, L.nx * L.ny) {
+        const size_t k = (size_t)kk;
+        const int ix = kk % L.nx, iy = kk / L.nx;
+        auto xt = [&](int i, int j, size_t q) -> float {
+            return PROLONG ? prolonged(L, xi, xc, nxc, wc, i, j, q) : xi[q];
         };
-        const float xk = xt(k);
-        const float ax = lapl_apply(L, ix, iy, k, xk, xt);
+        const float xk = xt(ix, iy, k);
+        float y = L.dP[k] * xk;
+        if (ix < L.nx - 1) y += L.aE[k] * (xk - xt(ix + 1, iy, k + 1));
+        if (ix > 0) y += L.aE[k - 1] * (xk - xt(ix - 1, iy, k - 1));
+        if (iy < L.ny - 1) y += L.aN[k] * (xk - xt(ix, iy + 1, k + L.nx));
+        if (iy > 0) y += L.aN[k - L.nx] * (xk - xt(ix, iy - 1, k - L.nx));
         const double rk = r[k];
-        const double zk = (double)(xk + omega_of(L, k, w) * ((float)rk - ax) / L.aP[k]);
+        const double zk = (double)(xk + omega_of(L, k, w) * ((float)rk - y) / L.aP[k]);
         z[k] = zk;
         red[0] += rk * zk;
         red[1] += rk * rk;
@@ -213,6 +227,106 @@ __global__ void __launch_bounds__(kThreads) k_mg_last(Lv L, const double *r, con
 }
 
 // ---------------------------------------------------------------------------------------------
+// Bottom of the V-cycle in one block: every level from `lb` down to the 1 x 1 coarsest level lives
+// in shared memory (29 bytes per cell: aE, aN, dP, aP, x, scratch, b and the activity flag); the
+// block runs the same pre-smoothing / restriction / exact solve / prolongation / post-smoothing
+// sequence as the per-level kernels, separated by __syncthreads, and writes level lb's result to
+// global memory.  This replaces five launches per small level with one launch per V-cycle.
+// ---------------------------------------------------------------------------------------------
+constexpr size_t kBottomBytesPerCell = 7 * sizeof(float) + 1;
+constexpr size_t kBottomBytes = 200 * 1024;
+
+struct BottomLevel {
+    int nx, ny, off;  // offset of this level's cells in the shared arrays
+};
+struct BottomPlan {
+    int nlev, total;
+    BottomLevel lv[kMgMaxLevels];
+    const float *aE[kMgMaxLevels], *aN[kMgMaxLevels], *dP[kMgMaxLevels], *aP[kMgMaxLevels];
+    const uint8_t *act[kMgMaxLevels];
+    const int *done;
+};
+
+__global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b_top, float *x_top, int nu, float w,
+                                                    float wc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (cg_finished(P.done)) return;
+    const int T = P.total;
+    float *sE = (float *)smem_raw, *sN = sE + T, *sD = sN + T, *sP = sD + T, *sX = sP + T, *sY = sX + T, *sB = sY + T;
+    uint8_t *sA = (uint8_t *)(sB + T);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int l = 0; l < P.nlev; l++) {
+        const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
+        for (int i = tid; i < n; i += nt) {
+            sE[o + i] = P.aE[l][i];
+            sN[o + i] = P.aN[l][i];
+            sD[o + i] = P.dP[l][i];
+            sP[o + i] = P.aP[l][i];
+            sA[o + i] = P.act[l][i];
+            if (l == 0) sB[o + i] = b_top[i];
+        }
+    }
+    __syncthreads();
+    // (A X)_i on level l (level-local index i)
+    auto Ax = [&](int l, const float *X, int i) -> float {
+        const int nx = P.lv[l].nx, ny = P.lv[l].ny, o = P.lv[l].off, ix = i % nx, iy = i / nx;
+        const float xc = X[o + i];
+        float y = sD[o + i] * xc;
+        if (ix < nx - 1) y += sE[o + i] * (xc - X[o + i + 1]);
+        if (ix > 0) y += sE[o + i - 1] * (xc - X[o + i - 1]);
+        if (iy < ny - 1) y += sN[o + i] * (xc - X[o + i + nx]);
+        if (iy > 0) y += sN[o + i - nx] * (xc - X[o + i - nx]);
+        return y;
+    };
+    auto om = [&](int l, int i) -> float { return sA[P.lv[l].off + i] ? w : 1.0f; };
+    // one damped-Jacobi sweep on level l: Y = X + omega (B - A X)/aP, then X = Y
+    auto sweep = [&](int l) {
+        const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
+        for (int i = tid; i < n; i += nt) sY[o + i] = sX[o + i] + om(l, i) * (sB[o + i] - Ax(l, sX, i)) / sP[o + i];
+        __syncthreads();
+        for (int i = tid; i < n; i += nt) sX[o + i] = sY[o + i];
+        __syncthreads();
+    };
+    const int L = P.nlev;
+    for (int l = 0; l < L - 1; l++) {  // descend
+        const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
+        for (int i = tid; i < n; i += nt) sX[o + i] = om(l, i) * sB[o + i] / sP[o + i];
+        __syncthreads();
+        for (int s = 1; s < nu; s++) sweep(l);
+        const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, nxc = P.lv[l + 1].nx, nyc = P.lv[l + 1].ny, oc = P.lv[l + 1].off;
+        for (int c = tid; c < nxc * nyc; c += nt) {
+            const int I = c % nxc, J = c / nxc;
+            float sres = 0.0f;
+            for (int dj = 0; dj < 2; dj++)
+                for (int di = 0; di < 2; di++) {
+                    const int i = 2 * I + di, j = 2 * J + dj;
+                    if (i >= nxf || j >= nyf) continue;
+                    const int f = i + j * nxf;
+                    if (!sA[o + f]) continue;
+                    sres += sB[o + f] - Ax(l, sX, f);
+                }
+            sB[oc + c] = sres;
+        }
+        __syncthreads();
+    }
+    {  // coarsest level: exact solve
+        const int l = L - 1, n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
+        for (int i = tid; i < n; i += nt) sX[o + i] = sA[o + i] ? sB[o + i] / sD[o + i] : sB[o + i];
+        __syncthreads();
+    }
+    for (int l = L - 2; l >= 0; l--) {  // ascend
+        const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, o = P.lv[l].off, nxc = P.lv[l + 1].nx, oc = P.lv[l + 1].off;
+        for (int f = tid; f < nxf * nyf; f += nt) {
+            const int i = f % nxf, j = f / nxf;
+            if (sA[o + f]) sX[o + f] += wc * sX[oc + (i >> 1) + (j >> 1) * nxc];
+        }
+        __syncthreads();
+        for (int s = 0; s < nu; s++) sweep(l);
+    }
+    for (int i = tid; i < P.lv[0].nx * P.lv[0].ny; i += nt) x_top[i] = sX[i];
+}
+
+// ---------------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------------
 static int mg_grid(Ctx *c, long long n) {
@@ -221,11 +335,42 @@ static int mg_grid(Ctx *c, long long n) {
     return (int)std::max(1LL, std::min(b, cap));
 }
 
-static Lv level_view(const MgLevel &m) { return Lv{m.nx, m.ny, m.aE, m.aN, m.dP, m.aP, m.act}; }
+static const dim3 kBlock2d(32, 8);
+static dim3 grid2d(int nx, int ny) { return dim3((unsigned)((nx + 31) / 32), (unsigned)((ny + 7) / 8)); }
+
+static Lv level_view(const MgLevel &m, const int *done) {
+    return Lv{m.nx, m.ny, m.aE, m.aN, m.dP, m.aP, m.act, done};
+}
+
+// First level >= 1 from which the rest of the hierarchy fits the bottom kernel's shared memory.
+static int bottom_level(const Ctx *c) {
+    long long rest = 0;
+    int lb = c->mg_levels - 1;
+    for (int l = c->mg_levels - 1; l >= 1; l--) {
+        rest += (long long)c->mg[l].nx * c->mg[l].ny;
+        if ((size_t)rest * kBottomBytesPerCell > kBottomBytes) break;
+        lb = l;
+    }
+    return lb;
+}
+
+static size_t bottom_plan(const Ctx *c, int lb, BottomPlan *P) {
+    P->nlev = c->mg_levels - lb;
+    int off = 0;
+    for (int k = 0; k < P->nlev; k++) {
+        const MgLevel &m = c->mg[lb + k];
+        P->lv[k] = BottomLevel{m.nx, m.ny, off};
+        P->aE[k] = m.aE; P->aN[k] = m.aN; P->dP[k] = m.dP; P->aP[k] = m.aP; P->act[k] = m.act;
+        off += m.nx * m.ny;
+    }
+    P->total = off;
+    return (size_t)off * kBottomBytesPerCell;
+}
 
 // Rebuilds every level's operator from the assembled Float64 system (after k_to_float_lapl).
 int mg_setup(Ctx *c) {
     if (c->mg_levels < 1) return fail(c, SHK_CUDA_ERROR, "multigrid hierarchy not allocated");
+    if (grid2d(c->nx, c->ny).y > 65535u) return fail(c, SHK_BAD_ARG, "multigrid needs ny <= 524280");
     MgLevel *lv = c->mg;
     const int n0 = c->nx * c->ny;
     k_mg_act0<<<mg_grid(c, n0), kThreads, 0, c->stream>>>(n0, c->mask8, lv[0].act);
@@ -241,73 +386,91 @@ int mg_setup(Ctx *c) {
             g.nx, g.ny, g.aE64, g.aN64, g.dP64, g.act, (float *)g.aE, (float *)g.aN, (float *)g.dP, (float *)g.aP);
         c->launches += 2;
     }
+    if (c->mg_levels > 1) {
+        // the bottom kernel's dynamic shared memory limit, once per device
+        static bool attr_set[128] = {};
+        if (c->device < 0 || c->device >= 128) return fail(c, SHK_BAD_ARG, "device ordinal out of range");
+        if (!attr_set[c->device]) {
+            cudaError_t e = cudaFuncSetAttribute(k_mg_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)kBottomBytes);
+            if (e != cudaSuccess) return check_cuda(c, e, "multigrid bottom shared memory");
+            attr_set[c->device] = true;
+        }
+    }
     return check_launch(c, "multigrid setup");
 }
 
-// Recursive V-cycle on level l >= 1 with rhs lv[l].b, solution into lv[l].x[0].
-static void vcycle(Ctx *c, int l) {
+// Recursive V-cycle on level l >= 1 with rhs lv[l].b; the solution ends in lv[l].x[*res].
+static int vcycle(Ctx *c, int l, const int *done, int *res) {
     MgLevel &m = c->mg[l];
-    Lv L = level_view(m);
-    const int n = m.nx * m.ny;
+    const Lv L = level_view(m, done);
     const float w = c->mg_omega, wc = c->mg_omega_c;
-    if (l == c->mg_levels - 1) {
-        k_mg_coarsest<<<mg_grid(c, n), kThreads, 0, c->stream>>>(L, m.b, m.x[0]);
+    if (l == bottom_level(c)) {
+        BottomPlan P;
+        const size_t smem = bottom_plan(c, l, &P);
+        P.done = done;
+        k_mg_bottom<<<1, 1024, smem, c->stream>>>(P, m.b, m.x[0], c->mg_nu, w, wc);
         c->launches++;
-        return;
+        *res = 0;
+        return SHK_OK;
     }
     MgLevel &g = c->mg[l + 1];
-    k_mg_pre0<float><<<mg_grid(c, n), kThreads, 0, c->stream>>>(L, m.b, m.x[0], w);
+    const dim3 gf = grid2d(m.nx, m.ny), gc = grid2d(g.nx, g.ny);
+    k_mg_pre0<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[0], w);
     int cur = 0;
     for (int s = 1; s < c->mg_nu; s++, cur ^= 1)
-        k_mg_sweep<float><<<mg_grid(c, n), kThreads, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1], w);
-    k_mg_restrict<float><<<mg_grid(c, (long long)g.nx * g.ny), kThreads, 0, c->stream>>>(L, m.b, m.x[cur], g.nx, g.ny,
-                                                                                        g.b);
+        k_mg_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1], w);
+    k_mg_restrict<float><<<gc, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], g.nx, g.ny, g.b);
     c->launches += 1 + c->mg_nu;
-    vcycle(c, l + 1);
-    k_mg_prolong_sweep<float><<<mg_grid(c, n), kThreads, 0, c->stream>>>(L, m.b, m.x[cur], g.x[0], g.nx, wc, w,
-                                                                         m.x[cur ^ 1]);
+    int gres = 0;
+    int rc = vcycle(c, l + 1, done, &gres);
+    if (rc) return rc;
+    k_mg_prolong_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], g.x[gres], g.nx, wc, w,
+                                                              m.x[cur ^ 1]);
     cur ^= 1;
     for (int s = 1; s < c->mg_nu; s++, cur ^= 1)
-        k_mg_sweep<float><<<mg_grid(c, n), kThreads, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1], w);
+        k_mg_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1], w);
     c->launches += c->mg_nu;
-    if (cur != 0) {  // leave the result in x[0]
-        cudaMemcpyAsync(m.x[0], m.x[1], (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
-    }
+    *res = cur;
+    return SHK_OK;
 }
 
 // z = M^-1 r on level 0 (r Float64), then the outer CG's r'z (init or iteration finish).
 int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
     MgLevel &m = c->mg[0];
-    Lv L = level_view(m);
+    const Lv L = level_view(m, &cg->done);
     const int n = m.nx * m.ny;
     const float w = c->mg_omega, wc = c->mg_omega_c;
+    const int gl = std::min(c->max_blocks, std::max(1, std::min(c->num_sms * 8, (n + kThreads - 1) / kThreads)));
     if (c->mg_levels == 1) {
-        k_mg_last<false><<<c->grid_stencil, kThreads, 0, c->stream>>>(L, r, m.x[0], nullptr, 1, wc, w, z, cg, init,
-                                                                      c->partials, c->counter);
+        k_mg_last<false><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[0], nullptr, 1, wc, w, z, cg, init, c->partials,
+                                                         c->counter);
         c->launches++;
         return check_launch(c, "multigrid apply");
     }
     MgLevel &g = c->mg[1];
-    k_mg_pre0<double><<<mg_grid(c, n), kThreads, 0, c->stream>>>(L, r, m.x[0], w);
+    const dim3 gf = grid2d(m.nx, m.ny), gc = grid2d(g.nx, g.ny);
+    k_mg_pre0<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[0], w);
     int cur = 0;
     for (int s = 1; s < c->mg_nu; s++, cur ^= 1)
-        k_mg_sweep<double><<<mg_grid(c, n), kThreads, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1], w);
-    k_mg_restrict<double><<<mg_grid(c, (long long)g.nx * g.ny), kThreads, 0, c->stream>>>(L, r, m.x[cur], g.nx, g.ny,
-                                                                                         g.b);
+        k_mg_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1], w);
+    k_mg_restrict<double><<<gc, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], g.nx, g.ny, g.b);
     c->launches += 1 + c->mg_nu;
-    vcycle(c, 1);
+    int gres = 0;
+    int rc = vcycle(c, 1, &cg->done, &gres);
+    if (rc) return rc;
     if (c->mg_nu == 1) {
-        k_mg_last<true><<<c->grid_stencil, kThreads, 0, c->stream>>>(L, r, m.x[cur], g.x[0], g.nx, wc, w, z, cg, init,
-                                                                     c->partials, c->counter);
+        k_mg_last<true><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[cur], g.x[gres], g.nx, wc, w, z, cg, init,
+                                                        c->partials, c->counter);
         c->launches++;
     } else {
-        k_mg_prolong_sweep<double><<<mg_grid(c, n), kThreads, 0, c->stream>>>(L, r, m.x[cur], g.x[0], g.nx, wc, w,
-                                                                              m.x[cur ^ 1]);
+        k_mg_prolong_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], g.x[gres], g.nx, wc, w,
+                                                                   m.x[cur ^ 1]);
         cur ^= 1;
         for (int s = 2; s < c->mg_nu; s++, cur ^= 1)
-            k_mg_sweep<double><<<mg_grid(c, n), kThreads, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1], w);
-        k_mg_last<false><<<c->grid_stencil, kThreads, 0, c->stream>>>(L, r, m.x[cur], nullptr, 1, wc, w, z, cg, init,
-                                                                      c->partials, c->counter);
+            k_mg_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1], w);
+        k_mg_last<false><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[cur], nullptr, 1, wc, w, z, cg, init, c->partials,
+                                                         c->counter);
         c->launches += c->mg_nu;
     }
     return check_launch(c, "multigrid apply");
