@@ -145,6 +145,36 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, u
 }
 
 // ---------------------------------------------------------------------------------------------
+// Per-block reads of the device-side CG scalars.  Thread (0,0) reads them and shares them through
+// shared memory, so a launch sends one request per block to the scalars' L2 line instead of one
+// per warp (a hot spot that cost more than the data traffic of the small level kernels).  Every
+// thread of the block must call these, before any early return.
+// ---------------------------------------------------------------------------------------------
+struct CgView {
+    int done, first;
+    double alpha, beta;
+};
+
+__device__ __forceinline__ CgView block_cg_view(const CgDev *cg) {
+    __shared__ CgView v;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        v.done = *(const volatile int *)&cg->done;
+        v.first = cg->first;
+        v.alpha = cg->alpha;
+        v.beta = cg->beta;
+    }
+    __syncthreads();
+    return v;
+}
+
+__device__ __forceinline__ bool block_cg_done(const int *done) {
+    __shared__ int d;
+    if (threadIdx.x == 0 && threadIdx.y == 0) d = done ? *(const volatile int *)done : 0;
+    __syncthreads();
+    return d != 0;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Scalar updates (run by thread 0 of the last block)
 // ---------------------------------------------------------------------------------------------
 static __device__ void cg_init_finish(CgDev *cg, double rz, double rr, double bb) {

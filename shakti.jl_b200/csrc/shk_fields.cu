@@ -5,7 +5,7 @@
 // compiled with --fmad=false, so no a*b+c is contracted), which makes these kernels bit-identical
 // to the reference's unfused kernels except for x^(1/n), where CUDA's pow and Julia's pow may
 // differ in the last bit.  Fusion never changes a value: a face quantity needed by two cells is
-// recomputed by both from the same operands.
+// computed once from the same operands and shared.
 #include <cuda_runtime.h>
 #include <float.h>
 
@@ -232,85 +232,118 @@ __device__ __forceinline__ FaceOut face(const Params &P, const Sliding &L, const
 // compute_Re!, compute_taub_xy!, compute_mdot!, compute_K! (src/elliptic_solver.jl:193-206),
 // plus the Picard check maxima max|h - h_prev| and max|h| (src/elliptic_solver.jl:162-163).
 // FROM_H = false is the initial-condition variant: pw, N and the gradients are taken as set.
+//
+// One 32 x 8 tile per block iteration, one thread per cell: (1) the tile's cells and a one-cell
+// halo (no corners) are loaded to shared memory with pw and N formed from h; (2) each of the
+// tile's 33 x 8 x-faces and 32 x 9 y-faces is computed once (q, Re, taub from the reference's
+// face formulas), the faces the tile owns are written, and the products the cells need
+// (Re, ub*taub, q*dh, q*dpw) stay in shared memory; (3) each cell sums its four faces.
 // ---------------------------------------------------------------------------------------------
+constexpr int kTailW = kTX, kTailH = kTY;           // cells per tile
+constexpr int kTailHW = kTailW + 2, kTailHH = kTailH + 2; // with the halo
+constexpr int kTailXF = (kTailW + 1) * kTailH;      // x-faces of a tile
+constexpr int kTailYF = kTailW * (kTailH + 1);      // y-faces of a tile
+
+struct FaceSm {
+    double re, ut, qd, qp;  // Re, ub*taub, q*dh, q*dpw
+};
+
 template <bool FROM_H, bool CHECK>
 __global__ void __launch_bounds__(kThreads) k_tail(int nx, int ny, Params P, Sliding L, shk_state s,
                                                    const uint8_t *__restrict__ m8,
                                                    const double *__restrict__ h_prev, double *partials,
                                                    unsigned int *counter, PicDev *pic) {
-    Tiles T(nx, ny);
+    __shared__ CellQ cq[kTailHH][kTailHW];
+    __shared__ FaceSm fx[kTailXF], fy[kTailYF];
+    const int tiles_x = (nx + kTailW - 1) / kTailW, ntiles = tiles_x * ((ny + kTailH - 1) / kTailH);
+    const int tid = threadIdx.x, tx = tid % kTailW, ty = tid / kTailW;
     double red[2] = {0.0, 0.0};
-    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
-        int ix, iy;
-        T.cell(t, ix, iy);
-        if (ix >= nx || iy >= ny) continue;
-        const size_t c = CI(ix, iy);
-        const CellQ q0 = load_cell<FROM_H>(P, s, m8, c);
-        CellQ qW = q0, qE = q0, qS = q0, qN = q0;
-        if (ix > 0) qW = load_cell<FROM_H>(P, s, m8, c - 1);
-        if (ix < nx - 1) qE = load_cell<FROM_H>(P, s, m8, c + 1);
-        if (iy > 0) qS = load_cell<FROM_H>(P, s, m8, c - nx);
-        if (iy < ny - 1) qN = load_cell<FROM_H>(P, s, m8, c + nx);
-
-        // x-faces: W = face ix (cells ix-1 | ix), E = face ix+1 (cells ix | ix+1)
-        const size_t fW = XI(ix, iy), fE = XI(ix + 1, iy);
-        const size_t fS = YI(ix, iy), fN = YI(ix, iy + 1);
-        FaceOut W = face<FROM_H>(P, L, s, 0, fW, ix > 0, qW, q0, q0);
-        FaceOut E = face<FROM_H>(P, L, s, 0, fE, ix < nx - 1, q0, qE, q0);
-        FaceOut S = face<FROM_H>(P, L, s, 1, fS, iy > 0, qS, q0, q0);
-        FaceOut Nf = face<FROM_H>(P, L, s, 1, fN, iy < ny - 1, q0, qN, q0);
-
-        // centre writes
-        if (FROM_H) {
-            s.pw[c] = q0.pw;
-            s.N[c] = q0.N;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int x0 = (t % tiles_x) * kTailW, y0 = (t / tiles_x) * kTailH;
+        // (1) cells of the tile and its halo
+        for (int k = tid; k < kTailHH * kTailHW; k += kThreads) {
+            const int hx = k % kTailHW, hy = k / kTailHW, ix = x0 - 1 + hx, iy = y0 - 1 + hy;
+            const bool corner = (hx == 0 || hx == kTailHW - 1) && (hy == 0 || hy == kTailHH - 1);
+            if (corner || ix < 0 || ix >= nx || iy < 0 || iy >= ny) continue;
+            cq[hy][hx] = load_cell<FROM_H>(P, s, m8, CI(ix, iy));
         }
-        // owned faces: W and S always; E on the last column, N on the last row
-        auto write_x = [&](size_t f, const FaceOut &o, bool interior) {
-            if (interior && FROM_H) {
-                s.dhdx[f] = o.dh;
-                s.dpwdx[f] = o.dpw;
+        __syncthreads();
+        // (2) faces
+        for (int k = tid; k < kTailXF + kTailYF; k += kThreads) {
+            if (k < kTailXF) {
+                const int fc = k % (kTailW + 1), row = k / (kTailW + 1), f = x0 + fc, iy = y0 + row;
+                if (iy >= ny || f > nx) continue;
+                const bool interior = f > 0 && f < nx;
+                const CellQ &a = cq[row + 1][f > 0 ? fc : fc + 1];      // west cell (east cell at f = 0)
+                const CellQ &b = cq[row + 1][f < nx ? fc + 1 : fc];     // east cell (west cell at f = nx)
+                const size_t fi = XI(f, iy);
+                const FaceOut o = face<FROM_H>(P, L, s, 0, fi, interior, a, b, f > 0 ? a : b);
+                if ((fc < kTailW && f < nx) || f == nx) {
+                    if (interior && FROM_H) {
+                        s.dhdx[fi] = o.dh;
+                        s.dpwdx[fi] = o.dpw;
+                    }
+                    s.q_x[fi] = o.q;
+                    s.Re_x[fi] = o.re;
+                    if (L.kind != SHK_SLIDING_PRESCRIBED) s.taub_x[fi] = o.taub;
+                }
+                fx[k] = FaceSm{o.re, o.ub * o.taub, o.q * o.dh, o.q * o.dpw};
+            } else {
+                const int kk = k - kTailXF, col = kk % kTailW, frow = kk / kTailW, ix = x0 + col, f = y0 + frow;
+                if (ix >= nx || f > ny) continue;
+                const bool interior = f > 0 && f < ny;
+                const CellQ &a = cq[f > 0 ? frow : frow + 1][col + 1];  // south cell (north cell at f = 0)
+                const CellQ &b = cq[f < ny ? frow + 1 : frow][col + 1]; // north cell (south cell at f = ny)
+                const size_t fi = YI(ix, f);
+                const FaceOut o = face<FROM_H>(P, L, s, 1, fi, interior, a, b, f > 0 ? a : b);
+                if ((frow < kTailH && f < ny) || f == ny) {
+                    if (interior && FROM_H) {
+                        s.dhdy[fi] = o.dh;
+                        s.dpwdy[fi] = o.dpw;
+                    }
+                    s.q_y[fi] = o.q;
+                    s.Re_y[fi] = o.re;
+                    if (L.kind != SHK_SLIDING_PRESCRIBED) s.taub_y[fi] = o.taub;
+                }
+                fy[kk] = FaceSm{o.re, o.ub * o.taub, o.q * o.dh, o.q * o.dpw};
             }
-            s.q_x[f] = o.q;
-            s.Re_x[f] = o.re;
-            if (L.kind != SHK_SLIDING_PRESCRIBED) s.taub_x[f] = o.taub;
-        };
-        auto write_y = [&](size_t f, const FaceOut &o, bool interior) {
-            if (interior && FROM_H) {
-                s.dhdy[f] = o.dh;
-                s.dpwdy[f] = o.dpw;
+        }
+        __syncthreads();
+        // (3) cells
+        const int ix = x0 + tx, iy = y0 + ty;
+        if (ix < nx && iy < ny) {
+            const size_t c = CI(ix, iy);
+            const CellQ &q0 = cq[ty + 1][tx + 1];
+            const FaceSm &W = fx[ty * (kTailW + 1) + tx], &E = fx[ty * (kTailW + 1) + tx + 1];
+            const FaceSm &S = fy[ty * kTailW + tx], &Nf = fy[(ty + 1) * kTailW + tx];
+            if (FROM_H) {
+                s.pw[c] = q0.pw;
+                s.N[c] = q0.N;
             }
-            s.q_y[f] = o.q;
-            s.Re_y[f] = o.re;
-            if (L.kind != SHK_SLIDING_PRESCRIBED) s.taub_y[f] = o.taub;
-        };
-        write_x(fW, W, ix > 0);
-        if (ix == nx - 1) write_x(fE, E, false);
-        write_y(fS, S, iy > 0);
-        if (iy == ny - 1) write_y(fN, Nf, false);
-
-        // compute_Re! (src/water_flux.jl:107-112)
-        const double Re_c = (W.re + E.re + S.re + Nf.re) / 4;
-        s.Re[c] = Re_c;
-        // compute_mdot! (src/melt_rate.jl:106-137)
-        const double sh = fabs((E.ub * E.taub + W.ub * W.taub) / 2 + (Nf.ub * Nf.taub + S.ub * S.taub) / 2);
-        const double pot = fabs((E.q * E.dh + W.q * W.dh) / 2 + (Nf.q * Nf.dh + S.q * S.dh) / 2);
-        s.shear[c] = sh;
-        s.potential[c] = pot;
-        if (P.with_sensible) {
-            const double sens = (E.q * E.dpw + W.q * W.dpw) / 2 + (Nf.q * Nf.dpw + S.q * S.dpw) / 2;
-            s.sensible[c] = sens;
-            s.mdot[c] = P.Linv * (s.G[c] + sh + P.rho_w * P.g * pot + P.ct * P.cw * P.rho_w * sens);
-        } else {
-            s.mdot[c] = P.Linv * (s.G[c] + sh + P.rho_w * P.g * pot);
+            // compute_Re! (src/water_flux.jl:107-112)
+            const double Re_c = (W.re + E.re + S.re + Nf.re) / 4;
+            s.Re[c] = Re_c;
+            // compute_mdot! (src/melt_rate.jl:106-137)
+            const double sh = fabs((E.ut + W.ut) / 2 + (Nf.ut + S.ut) / 2);
+            const double pot = fabs((E.qd + W.qd) / 2 + (Nf.qd + S.qd) / 2);
+            s.shear[c] = sh;
+            s.potential[c] = pot;
+            if (P.with_sensible) {
+                const double sens = (E.qp + W.qp) / 2 + (Nf.qp + S.qp) / 2;
+                s.sensible[c] = sens;
+                s.mdot[c] = P.Linv * (s.G[c] + sh + P.rho_w * P.g * pot + P.ct * P.cw * P.rho_w * sens);
+            } else {
+                s.mdot[c] = P.Linv * (s.G[c] + sh + P.rho_w * P.g * pot);
+            }
+            // compute_K! (src/water_flux.jl:221-226)
+            const double bb = s.b[c];
+            s.K[c] = (bb * bb * bb * P.g) / (12 * P.nu * (1 + P.omega * Re_c));
+            if (CHECK) {
+                red[0] = jl_max(red[0], fabs(q0.h - h_prev[c]));
+                red[1] = jl_max(red[1], fabs(q0.h));
+            }
         }
-        // compute_K! (src/water_flux.jl:221-226)
-        const double bb = s.b[c];
-        s.K[c] = (bb * bb * bb * P.g) / (12 * P.nu * (1 + P.omega * Re_c));
-        if (CHECK) {
-            red[0] = jl_max(red[0], fabs(q0.h - h_prev[c]));
-            red[1] = jl_max(red[1], fabs(q0.h));
-        }
+        __syncthreads();  // the next tile reuses the shared arrays
     }
     if (CHECK) {
         double out[2];

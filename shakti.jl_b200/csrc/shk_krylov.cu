@@ -128,13 +128,14 @@ __global__ void __launch_bounds__(kMarchX, 6) k_cg_A(int nx, int ny, int TH, con
                                                   T *__restrict__ Ap, CgDev *cg, double *partials,
                                                   unsigned int *counter, double eps_curv,
                                                   const T *__restrict__ dP = nullptr) {
-    if (*(volatile int *)&cg->done) return;
+    const CgView cv = block_cg_view(cg);
+    if (cv.done) return;
     constexpr int R = kRingRows, W = kMarchX + 2;
     enum { IR = 0, IP = 1, IO = 2, IE = 3, IN = 4, ID = 5, NA = LAPL ? 6 : 5 };
     __shared__ __align__(16) T ring[R][NA][W];
     __shared__ T prow[2][W];
-    const bool first = cg->first != 0;
-    const T beta = (T)cg->beta;
+    const bool first = cv.first != 0;
+    const T beta = (T)cv.beta;
     const int tiles_x = (nx + kMarchX - 1) / kMarchX;
     const int x0 = (blockIdx.x % tiles_x) * kMarchX, y0 = (blockIdx.x / tiles_x) * TH;
     const int tid = threadIdx.x, ix = x0 + tid;
@@ -271,11 +272,12 @@ template <typename T, bool JAC>
 __global__ void __launch_bounds__(kThreads) k_cg_B(int n, const T *__restrict__ aP, const T *__restrict__ p,
                                                    const T *__restrict__ Ap, T *__restrict__ x, T *__restrict__ r,
                                                    CgDev *cg, double *partials, unsigned int *counter) {
-    if (*(volatile int *)&cg->done) return;
+    const CgView cv = block_cg_view(cg);
+    if (cv.done) return;
     using VT = Vec16<T>;
     using V = typename VT::V;
     constexpr int W = VT::W;
-    const T alpha = (T)cg->alpha;
+    const T alpha = (T)cv.alpha;
     double rz = 0.0, rr = 0.0;
     const int nv = n / W;
     const V *aPv = reinterpret_cast<const V *>(aP), *pv = reinterpret_cast<const V *>(p),
@@ -358,7 +360,7 @@ __global__ void __launch_bounds__(kThreads) k_cheb(int nx, int ny, const T *__re
                                                    T *__restrict__ pc_new, T *__restrict__ y, int k,
                                                    const ChebDev *ch, CgDev *cg, double *partials,
                                                    unsigned int *counter) {
-    if (CGM != CG_NONE && *(volatile int *)&cg->done) return;
+    if (CGM != CG_NONE && block_cg_done(&cg->done)) return;
     const T a = (T)ch->calpha[k];
     const T bt = (T)ch->cbeta[k];
     Tiles Tl(nx, ny);

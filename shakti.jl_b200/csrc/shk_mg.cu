@@ -106,7 +106,8 @@ struct Lv {
     const int *done;  // the outer CG's stop flag: V-cycles issued after the stop do no work
 };
 
-__device__ __forceinline__ bool cg_finished(const int *done) { return done && *(const volatile int *)done; }
+// The outer CG's stop flag, read once per block (all threads must call it first).
+__device__ __forceinline__ bool cg_finished(const int *done) { return block_cg_done(done); }
 
 // (A x)_c in Laplacian form, with x given by a functor (so fused kernels can form x on the fly)
 template <typename F>
@@ -199,7 +200,7 @@ template <bool PROLONG>
 __global__ void __launch_bounds__(kThreads) k_mg_last(Lv L, const double *r, const float *xi, const float *xc, int nxc,
                                                       float wc, float w, double *z, CgDev *cg, int init,
                                                       double *partials, unsigned int *counter) {
-    if (*(volatile int *)&cg->done) return;
+    if (block_cg_done(&cg->done)) return;
     double red[2] = {0.0, 0.0};
     GSTRIDE(kk, L.nx * L.ny) {
         const size_t k = (size_t)kk;
@@ -223,6 +224,177 @@ __global__ void __launch_bounds__(kThreads) k_mg_last(Lv L, const double *r, con
     if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
         if (init) cg_init_finish(cg, out[0], cg->rr, cg->bnorm);
         else cg_iter_finish(cg, out[0], out[1]);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused level kernels (nu = 2): the descending half of a level (first sweep from zero, second
+// sweep, residual restriction) and the ascending half (prolongation, two sweeps) each run as one
+// kernel over 32 x 16 tiles with a two-cell halo staged in shared memory, so the level's
+// operator, right-hand side and iterates cross HBM once per half instead of once per sweep.  The
+// arithmetic is the per-sweep kernels' expression for expression, so the results are identical.
+// ---------------------------------------------------------------------------------------------
+constexpr int kFW = 32, kFH = 16, kFR = 2;                  // tile and halo
+constexpr int kFSW = kFW + 2 * kFR, kFSH = kFH + 2 * kFR;   // staged region (36 x 20)
+constexpr int kFCells = kFSW * kFSH;
+
+struct FusedSm {
+    float b[kFSH][kFSW], aP[kFSH][kFSW], dP[kFSH][kFSW], aE[kFSH][kFSW], aN[kFSH][kFSW];
+    float x0[kFSH][kFSW], x1[kFSH][kFSW];
+    uint8_t act[kFSH][kFSW];
+};
+
+// (A X)_c at staged position (hx, hy) = global (gx, gy), same operand order as lapl_apply
+__device__ __forceinline__ float ax_sm(const FusedSm &S, const float (&X)[kFSH][kFSW], int nx, int ny, int hx, int hy,
+                                       int gx, int gy) {
+    const float xc = X[hy][hx];
+    float y = S.dP[hy][hx] * xc;
+    if (gx < nx - 1) y += S.aE[hy][hx] * (xc - X[hy][hx + 1]);
+    if (gx > 0) y += S.aE[hy][hx - 1] * (xc - X[hy][hx - 1]);
+    if (gy < ny - 1) y += S.aN[hy][hx] * (xc - X[hy + 1][hx]);
+    if (gy > 0) y += S.aN[hy - 1][hx] * (xc - X[hy - 1][hx]);
+    return y;
+}
+
+// Stages the level's operator and rhs over the tile and its halo; cells outside the level get
+// act = 0, aP = 1 and zeros (never read as neighbours: the bounds tests above skip them).
+template <typename TB>
+__device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b, int x0, int y0, double *r64) {
+    for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
+        const int hx = k % kFSW, hy = k / kFSW, gx = x0 - kFR + hx, gy = y0 - kFR + hy;
+        if (gx >= 0 && gx < L.nx && gy >= 0 && gy < L.ny) {
+            const size_t q = (size_t)gx + (size_t)gy * L.nx;
+            const TB bq = b[q];
+            if (r64) r64[k] = (double)bq;
+            S.b[hy][hx] = (float)bq;
+            S.aP[hy][hx] = L.aP[q];
+            S.dP[hy][hx] = L.dP[q];
+            S.aE[hy][hx] = L.aE[q];
+            S.aN[hy][hx] = L.aN[q];
+            S.act[hy][hx] = L.act[q];
+        } else {
+            if (r64) r64[k] = 0.0;
+            S.b[hy][hx] = 0.0f;
+            S.aP[hy][hx] = 1.0f;
+            S.dP[hy][hx] = 0.0f;
+            S.aE[hy][hx] = 0.0f;
+            S.aN[hy][hx] = 0.0f;
+            S.act[hy][hx] = 0;
+        }
+    }
+}
+
+// One damped-Jacobi sweep XO = XI + omega (b - A XI)/aP over the staged positions at distance
+// <= reach from the tile (cells inside the level only).
+__device__ __forceinline__ void sweep_sm(FusedSm &S, const float (&XI)[kFSH][kFSW], float (&XO)[kFSH][kFSW], int nx,
+                                         int ny, int x0, int y0, int reach, float w) {
+    const int lo = kFR - reach, wdt = kFW + 2 * reach, hgt = kFH + 2 * reach;
+    for (int k = threadIdx.x; k < wdt * hgt; k += blockDim.x) {
+        const int hx = lo + k % wdt, hy = lo + k / wdt, gx = x0 - kFR + hx, gy = y0 - kFR + hy;
+        if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) continue;
+        const float ax = ax_sm(S, XI, nx, ny, hx, hy, gx, gy);
+        const float om = S.act[hy][hx] ? w : 1.0f;
+        XO[hy][hx] = XI[hy][hx] + om * (S.b[hy][hx] - ax) / S.aP[hy][hx];
+    }
+}
+
+// Descending half of level L: x1 = two sweeps from zero (written to xo), and the coarse rhs
+// bc = restriction of b - A x1.  1D grid striding over 32 x 16 tiles.
+template <typename TB>
+__global__ void __launch_bounds__(256) k_mg_down(Lv L, const TB *b, float *xo, int nxc, int nyc, float *bc, float w) {
+    if (cg_finished(L.done)) return;
+    __shared__ FusedSm S;
+    const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
+        stage_level<TB>(S, L, b, x0, y0, nullptr);
+        __syncthreads();
+        // first sweep from x = 0 on the whole staged region: x0 = omega b / aP
+        for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
+            const int hx = k % kFSW, hy = k / kFSW;
+            S.x0[hy][hx] = (S.act[hy][hx] ? w : 1.0f) * S.b[hy][hx] / S.aP[hy][hx];
+        }
+        __syncthreads();
+        sweep_sm(S, S.x0, S.x1, L.nx, L.ny, x0, y0, 1, w);
+        __syncthreads();
+        for (int k = threadIdx.x; k < kFW * kFH; k += blockDim.x) {
+            const int tx = k % kFW, ty = k / kFW, gx = x0 + tx, gy = y0 + ty;
+            if (gx < L.nx && gy < L.ny) xo[(size_t)gx + (size_t)gy * L.nx] = S.x1[ty + kFR][tx + kFR];
+        }
+        // restriction: one thread per aggregate of the tile
+        for (int k = threadIdx.x; k < (kFW / 2) * (kFH / 2); k += blockDim.x) {
+            const int I = x0 / 2 + k % (kFW / 2), J = y0 / 2 + k / (kFW / 2);
+            if (I >= nxc || J >= nyc) continue;
+            float sres = 0.0f;
+#pragma unroll
+            for (int dj = 0; dj < 2; dj++)
+#pragma unroll
+                for (int di = 0; di < 2; di++) {
+                    const int gx = 2 * I + di, gy = 2 * J + dj;
+                    if (gx >= L.nx || gy >= L.ny) continue;
+                    const int hx = gx - x0 + kFR, hy = gy - y0 + kFR;
+                    if (!S.act[hy][hx]) continue;
+                    sres += S.b[hy][hx] - ax_sm(S, S.x1, L.nx, L.ny, hx, hy, gx, gy);
+                }
+            bc[(size_t)I + (size_t)J * nxc] = sres;
+        }
+        __syncthreads();  // the next tile reuses the staged arrays
+    }
+}
+
+// Ascending half of level L: xt = xi + omega_c P xc, then two sweeps.  LAST (level 0): the second
+// sweep writes z in Float64 and the outer CG's r'z, r'r finish the init or the iteration;
+// otherwise it writes the level's result to xo.
+template <typename TB, bool LAST>
+__global__ void __launch_bounds__(256) k_mg_up(Lv L, const TB *b, const float *xi, const float *xc, int nxc, float wc,
+                                               float w, float *xo, double *z, CgDev *cg, int init, double *partials,
+                                               unsigned int *counter) {
+    if (cg_finished(L.done)) return;
+    __shared__ FusedSm S;
+    __shared__ double r64[LAST ? kFCells : 1];
+    const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
+    double red[2] = {0.0, 0.0};
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
+        stage_level<TB>(S, L, b, x0, y0, LAST ? r64 : nullptr);
+        for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
+            const int hx = k % kFSW, hy = k / kFSW, gx = x0 - kFR + hx, gy = y0 - kFR + hy;
+            float v = 0.0f;
+            if (gx >= 0 && gx < L.nx && gy >= 0 && gy < L.ny) {
+                const size_t q = (size_t)gx + (size_t)gy * L.nx;
+                v = xi[q];
+                if (L.act[q]) v += wc * xc[(size_t)(gx >> 1) + (size_t)(gy >> 1) * nxc];
+            }
+            S.x0[hy][hx] = v;
+        }
+        __syncthreads();
+        sweep_sm(S, S.x0, S.x1, L.nx, L.ny, x0, y0, 1, w);
+        __syncthreads();
+        for (int k = threadIdx.x; k < kFW * kFH; k += blockDim.x) {
+            const int tx = k % kFW, ty = k / kFW, gx = x0 + tx, gy = y0 + ty;
+            if (gx >= L.nx || gy >= L.ny) continue;
+            const int hx = tx + kFR, hy = ty + kFR;
+            const float ax = ax_sm(S, S.x1, L.nx, L.ny, hx, hy, gx, gy);
+            const float om = S.act[hy][hx] ? w : 1.0f;
+            const size_t q = (size_t)gx + (size_t)gy * L.nx;
+            if (LAST) {
+                const double rk = r64[hy * kFSW + hx];
+                const double zk = (double)(S.x1[hy][hx] + om * ((float)rk - ax) / S.aP[hy][hx]);
+                z[q] = zk;
+                red[0] += rk * zk;
+                red[1] += rk * rk;
+            } else {
+                xo[q] = S.x1[hy][hx] + om * (S.b[hy][hx] - ax) / S.aP[hy][hx];
+            }
+        }
+        __syncthreads();
+    }
+    if (LAST) {
+        double out[2];
+        if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
+            if (init) cg_init_finish(cg, out[0], cg->rr, cg->bnorm);
+            else cg_iter_finish(cg, out[0], out[1]);
+        }
     }
 }
 
@@ -342,6 +514,13 @@ static Lv level_view(const MgLevel &m, const int *done) {
     return Lv{m.nx, m.ny, m.aE, m.aN, m.dP, m.aP, m.act, done};
 }
 
+// The fused two-sweep level kernels serve nu = 2 (the default); other nu use the per-sweep kernels.
+static bool fused(const Ctx *c) { return c->mg_fused && c->mg_nu == 2; }
+static int fused_grid(const Ctx *c, const MgLevel &m) {
+    const long long tiles = (long long)((m.nx + kFW - 1) / kFW) * ((m.ny + kFH - 1) / kFH);
+    return (int)std::max(1LL, std::min(tiles, (long long)c->max_blocks));
+}
+
 // First level >= 1 from which the rest of the hierarchy fits the bottom kernel's shared memory.
 static int bottom_level(const Ctx *c) {
     long long rest = 0;
@@ -415,6 +594,19 @@ static int vcycle(Ctx *c, int l, const int *done, int *res) {
         return SHK_OK;
     }
     MgLevel &g = c->mg[l + 1];
+    if (fused(c)) {
+        const int gt = fused_grid(c, m);
+        k_mg_down<float><<<gt, 256, 0, c->stream>>>(L, m.b, m.x[0], g.nx, g.ny, g.b, w);
+        c->launches++;
+        int gres = 0;
+        int rc = vcycle(c, l + 1, done, &gres);
+        if (rc) return rc;
+        k_mg_up<float, false><<<gt, 256, 0, c->stream>>>(L, m.b, m.x[0], g.x[gres], g.nx, wc, w, m.x[1], nullptr,
+                                                         nullptr, 0, nullptr, nullptr);
+        c->launches++;
+        *res = 1;
+        return SHK_OK;
+    }
     const dim3 gf = grid2d(m.nx, m.ny), gc = grid2d(g.nx, g.ny);
     k_mg_pre0<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[0], w);
     int cur = 0;
@@ -449,6 +641,18 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
         return check_launch(c, "multigrid apply");
     }
     MgLevel &g = c->mg[1];
+    if (fused(c)) {
+        const int gt = fused_grid(c, m);
+        k_mg_down<double><<<gt, 256, 0, c->stream>>>(L, r, m.x[0], g.nx, g.ny, g.b, w);
+        c->launches++;
+        int gres = 0;
+        int rc = vcycle(c, 1, &cg->done, &gres);
+        if (rc) return rc;
+        k_mg_up<double, true><<<gt, 256, 0, c->stream>>>(L, r, m.x[0], g.x[gres], g.nx, wc, w, nullptr, z, cg, init,
+                                                         c->partials, c->counter);
+        c->launches++;
+        return check_launch(c, "multigrid apply");
+    }
     const dim3 gf = grid2d(m.nx, m.ny), gc = grid2d(g.nx, g.ny);
     k_mg_pre0<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[0], w);
     int cur = 0;

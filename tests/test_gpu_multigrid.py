@@ -1,0 +1,65 @@
+"""GPU checks of the multigrid preconditioner's kernel variants and of the CG launch modes.
+
+ - The fused two-sweep level kernels (one kernel per half V-cycle level, halo staged in shared
+   memory) against the per-sweep kernels: the V-cycle output is the same arithmetic, so CG iterates
+   agree to the rounding of the r'z reduction order (1e-12), and full solves take the same number
+   of iterations (+-1).
+ - The three ways of issuing CG iterations (direct launches, one CUDA graph per iteration, the whole
+   loop as a graph with a device-side WHILE node) run the same kernels in the same order: bit-equal
+   solutions and equal iteration counts.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def relerr(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b))) / max(float(np.max(np.abs(b))), 1e-300)
+
+
+def ragged_workload(shk):
+    # 301 x 301: odd sizes on every level, tiles cut by the domain edge, LAND/OTHER_BASIN blobs
+    # (identity rows) and moulins; several levels above the one-block bottom of the V-cycle
+    return shk.configs.seasonal(301, 15e3, seed=4242, C=0.25)
+
+
+def solve(shk, w, env, monkeypatch, itmax=0, rtol=1e-8, multigrid=True):
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    g = shk.Grid(w.nx, w.ny, w.lx, w.ly)
+    pm = shk.ModelParameters(**shk.configs.SEASONAL_PARAMS)
+    sl = shk.RegularizedCoulombSlidingLaw(w.sliding_C)
+    s = shk.State(g)
+    shk.set_initial_conditions(s, g, pm, sl, **w.inputs)
+    ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, multigrid=multigrid, stop_rule="relres", rtol=rtol,
+                               atol=0.0, itmax=itmax)
+    stats = shk.solve_elliptic_linear_system(ls, s, g, pm, shk.Arithmetic(), sl)
+    h = s.h.cpu().numpy().copy()
+    for k in env:
+        monkeypatch.delenv(k)
+    return h, stats
+
+
+def test_fused_level_kernels_match_per_sweep_kernels(shk, cuda, monkeypatch):
+    w = ragged_workload(shk)
+    h_f, st_f = solve(shk, w, {"SHK_MG_FUSED": "1"}, monkeypatch, itmax=8, rtol=0.0)
+    h_u, st_u = solve(shk, w, {"SHK_MG_FUSED": "0"}, monkeypatch, itmax=8, rtol=0.0)
+    assert st_f.niter == st_u.niter == 8
+    assert relerr(h_f, h_u) <= 1e-12, relerr(h_f, h_u)
+    h_f, st_f = solve(shk, w, {"SHK_MG_FUSED": "1"}, monkeypatch)
+    h_u, st_u = solve(shk, w, {"SHK_MG_FUSED": "0"}, monkeypatch)
+    assert st_f.status == st_u.status == 0
+    assert abs(st_f.niter - st_u.niter) <= 1, (st_f.niter, st_u.niter)
+    assert relerr(h_f, h_u) <= 1e-9
+
+
+@pytest.mark.parametrize("multigrid", [True, False], ids=["multigrid", "jacobi"])
+def test_cg_launch_modes_are_bit_identical(shk, cuda, monkeypatch, multigrid):
+    w = ragged_workload(shk)
+    out = [solve(shk, w, {"SHK_CG_GRAPHS": m}, monkeypatch, multigrid=multigrid) for m in ("0", "1", "2")]
+    (h0, s0), (h1, s1), (h2, s2) = out
+    assert s0.status == s1.status == s2.status == 0
+    assert s0.niter == s1.niter == s2.niter
+    assert np.array_equal(h0, h1) and np.array_equal(h0, h2)
