@@ -189,13 +189,15 @@ def run_steps(shk, sim, n, record=None):
             record.append(dict(picard=ps.last_iter, converged=ps.converged, cg=ps.cg_iters_total))
 
 
-def mg_vcycle_bytes(nx, ny, nu=2):
-    """Algorithmic bytes of one V-cycle per launch (all levels), for nu = 2 sweeps per side.
-    Level 0 (Float64 residual in, Float64 z out), per fine cell: first sweep 17 B, sweep 33 B,
-    restriction 26 B, prolongation + sweep 34 B, last sweep with z and the dots 37 B.  Coarse
-    levels (Float32), per cell: 13 + 29 + 22 + 30 + 29 B.  The levels that fit in one block's
-    shared memory (29 B per cell, 200 KiB) are read once (operator 17 B + b 4 B per cell) and level
-    lb's result written once (4 B per cell)."""
+def mg_vcycle_bytes(nx, ny, fused=True):
+    """Algorithmic bytes of one V-cycle (all levels, nu = 2 sweeps per side).
+    Fused level kernels (the default): level 0 (Float64 residual in, Float64 z out), per fine cell,
+    descending half 30 B (r 8, activity flag 1, operator aP dP aE aN 16 in; x 4, coarse rhs 1 out)
+    and ascending half 38 B (x 4, coarse x 1, flag 1, operator 16, r 8 in; z 8 out); each coarse
+    level above the bottom, per cell, 26 + 30 B (Float32 rhs).  Per-sweep kernels: level 0
+    17 + 33 + 26 + 34 + 37 B, coarse levels 13 + 29 + 22 + 30 + 29 B.  The levels that fit in one
+    block's shared memory (29 B per cell, 200 KiB) are read once (operator 17 B + rhs 4 B per
+    cell) and level lb's result written once (4 B per cell)."""
     dims = [(nx, ny)]
     while dims[-1] != (1, 1):
         a, b = dims[-1]
@@ -208,9 +210,10 @@ def mg_vcycle_bytes(nx, ny, nu=2):
         if rest * 29 > 200 * 1024:
             break
         lb = l
-    total = 147 * cells[0] if len(dims) > 1 else 37 * cells[0]
+    top, coarse = (68, 56) if fused else (147, 123)
+    total = top * cells[0] if len(dims) > 1 else 37 * cells[0]
     for l in range(1, lb):
-        total += 123 * cells[l]
+        total += coarse * cells[l]
     if len(dims) > 1:
         total += 25 * cells[lb] + sum(17 * cells[l] for l in range(lb + 1, len(dims)))
     return total
@@ -220,7 +223,7 @@ def iteration_bytes(form, nx, ny):
     cells = nx * ny
     b = CG_BYTES[form] * cells
     if form == "multigrid":
-        b += mg_vcycle_bytes(nx, ny)
+        b += mg_vcycle_bytes(nx, ny, fused=os.environ.get("SHK_MG_FUSED", "1") != "0")
     return b
 
 
@@ -267,7 +270,7 @@ def roofline_for(shk, sim, form, w, peaks):
     kernel = {"plain": "k_cg_A + k_cg_B (one Jacobi-PCG iteration, Float64)",
               "fp32cg": "k_cg_A + k_cg_B (one Jacobi-PCG iteration, Float32 Laplacian form)",
               "multigrid": "one multigrid-preconditioned CG iteration: k_cg_A + k_cg_B (Float64) + the Float32 "
-                           "V-cycle (level kernels + k_mg_bottom + k_mg_last)"}[form]
+                           "V-cycle (fused level kernels k_mg_down/k_mg_up + the one-block k_mg_bottom)"}[form]
     r = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
          "frac": round(achieved / peak, 4), "traffic": None, "kernel": kernel,
          "algorithmic_bytes_per_launch": nbytes, "us_per_iteration": round(it_ms * 1e3, 2),

@@ -65,8 +65,8 @@ static int ctx_alloc(Ctx *c) {
     size_t o_x = carve(dN), o_r = carve(dN), o_z = carve(dN), o_p0 = carve(dN), o_p1 = carve(dN), o_Ap = carve(dN);
     size_t o_hprev = carve(dN);
     size_t o_cr0 = carve(dN), o_cr1 = carve(dN), o_cp0 = carve(dN), o_cp1 = carve(dN);
-    size_t o_f[15];
-    for (int i = 0; i < 15; i++) o_f[i] = carve(fN);
+    size_t o_f[16];
+    for (int i = 0; i < 16; i++) o_f[i] = carve(fN);
     // multigrid hierarchy: level 0 aliases the Float32 operator; levels >= 1 own their arrays
     int dims[2 * kMgMaxLevels];
     c->mg_levels = mg_levels_for(c->nx, c->ny, dims, kMgMaxLevels);
@@ -76,7 +76,7 @@ static int ctx_alloc(Ctx *c) {
     for (int l = 1; l < c->mg_levels; l++) {
         const size_t m = (size_t)dims[2 * l] * dims[2 * l + 1];
         for (int k = 0; k < 3; k++) o_mg[l][k] = carve(m * sizeof(double));
-        for (int k = 3; k < 9; k++) o_mg[l][k] = carve(m * sizeof(float)); // aE, aN, dP, aP, x0, x1
+        for (int k = 3; k < 9; k++) o_mg[l][k] = carve(m * sizeof(float)); // aE, aN, dP, wD, x0, x1
         o_mg[l][9] = carve(m * sizeof(float) + m);                       // b, then act bytes
     }
     size_t o_part = carve((size_t)kMaxRedValues * c->max_blocks * sizeof(double));
@@ -94,15 +94,15 @@ static int ctx_alloc(Ctx *c) {
     c->h_prev = (double *)(b + o_hprev);
     c->cr[0] = (double *)(b + o_cr0); c->cr[1] = (double *)(b + o_cr1);
     c->cp[0] = (double *)(b + o_cp0); c->cp[1] = (double *)(b + o_cp1);
-    float **fl[15] = {&c->aP32, &c->aE32, &c->aN32, &c->b32, &c->x32, &c->r32, &c->z32, &c->p32[0], &c->p32[1],
-                      &c->Ap32, &c->cr32[0], &c->cr32[1], &c->cp32[0], &c->cp32[1], &c->dP32};
-    for (int i = 0; i < 15; i++) *fl[i] = (float *)(b + o_f[i]);
+    float **fl[16] = {&c->aP32, &c->aE32, &c->aN32, &c->b32, &c->x32, &c->r32, &c->z32, &c->p32[0], &c->p32[1],
+                      &c->Ap32, &c->cr32[0], &c->cr32[1], &c->cp32[0], &c->cp32[1], &c->dP32, &c->wD32};
+    for (int i = 0; i < 16; i++) *fl[i] = (float *)(b + o_f[i]);
     for (int l = 0; l < c->mg_levels; l++) {
         MgLevel &m = c->mg[l];
         m.nx = dims[2 * l];
         m.ny = dims[2 * l + 1];
         if (l == 0) {
-            m.aE = c->aE32; m.aN = c->aN32; m.dP = c->dP32; m.aP = c->aP32;
+            m.aE = c->aE32; m.aN = c->aN32; m.dP = c->dP32; m.wD = c->wD32;
             m.act = (uint8_t *)(b + o_act0);
             m.x[0] = c->cr32[0]; m.x[1] = c->cr32[1];
             m.b = nullptr;
@@ -111,7 +111,7 @@ static int ctx_alloc(Ctx *c) {
         const size_t cnt = (size_t)m.nx * m.ny;
         m.aE64 = (double *)(b + o_mg[l][0]); m.aN64 = (double *)(b + o_mg[l][1]); m.dP64 = (double *)(b + o_mg[l][2]);
         m.aE = (float *)(b + o_mg[l][3]); m.aN = (float *)(b + o_mg[l][4]); m.dP = (float *)(b + o_mg[l][5]);
-        m.aP = (float *)(b + o_mg[l][6]); m.x[0] = (float *)(b + o_mg[l][7]); m.x[1] = (float *)(b + o_mg[l][8]);
+        m.wD = (float *)(b + o_mg[l][6]); m.x[0] = (float *)(b + o_mg[l][7]); m.x[1] = (float *)(b + o_mg[l][8]);
         m.b = (float *)(b + o_mg[l][9]);
         m.act = (uint8_t *)(b + o_mg[l][9] + cnt * sizeof(float));
     }

@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <float.h>
 
+#include <algorithm>
+
 #include "shk_device.cuh"
 
 namespace shk {
@@ -249,7 +251,7 @@ struct FaceSm {
 };
 
 template <bool FROM_H, bool CHECK>
-__global__ void __launch_bounds__(kThreads) k_tail(int nx, int ny, Params P, Sliding L, shk_state s,
+__global__ void __launch_bounds__(kThreads, 4) k_tail(int nx, int ny, Params P, Sliding L, shk_state s,
                                                    const uint8_t *__restrict__ m8,
                                                    const double *__restrict__ h_prev, double *partials,
                                                    unsigned int *counter, PicDev *pic) {
@@ -520,6 +522,12 @@ int build_mask8(Ctx *c) {
     return check_launch(c, "k_mask8");
 }
 
+// One resident wave of the tail (four 256-thread blocks per SM), striding over the tiles.
+static int tail_grid(const Ctx *c) {
+    const long long tiles = (long long)((c->nx + kTailW - 1) / kTailW) * ((c->ny + kTailH - 1) / kTailH);
+    return (int)std::max(1LL, std::min(tiles, (long long)c->num_sms * 4));
+}
+
 int launch_initial_conditions(Ctx *c) {
     const int nx = c->nx, ny = c->ny, n = nx * ny;
     const long long nf = (long long)(nx + 1) * ny + (long long)nx * (ny + 1);
@@ -538,7 +546,7 @@ int launch_initial_conditions(Ctx *c) {
     k_init_faces<<<flat_grid(c, nf), kThreads, 0, c->stream>>>(nx, ny, c->P, c->st);
     c->launches++;
     if ((rc = check_launch(c, "k_init_faces"))) return rc;
-    k_tail<false, false><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, c->P, c->SL, c->st, c->mask8, nullptr,
+    k_tail<false, false><<<tail_grid(c), kThreads, 0, c->stream>>>(nx, ny, c->P, c->SL, c->st, c->mask8, nullptr,
                                                                        c->partials, c->counter, nullptr);
     c->launches++;
     return check_launch(c, "k_tail<init>");
@@ -566,11 +574,11 @@ int launch_export_mfls(Ctx *c, double *aP, double *aE, double *aW, double *aN, d
 
 int launch_tail(Ctx *c, bool picard_check) {
     if (picard_check)
-        k_tail<true, true><<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->SL, c->st, c->mask8,
+        k_tail<true, true><<<tail_grid(c), kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->SL, c->st, c->mask8,
                                                                         c->h_prev, c->partials, c->counter,
                                                                         &c->dev->pic);
     else
-        k_tail<true, false><<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->SL, c->st, c->mask8,
+        k_tail<true, false><<<tail_grid(c), kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->SL, c->st, c->mask8,
                                                                          nullptr, c->partials, c->counter, nullptr);
     c->launches++;
     return check_launch(c, "k_tail");

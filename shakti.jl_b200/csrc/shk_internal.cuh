@@ -34,8 +34,8 @@ constexpr int kTY = 8;              // tile height
 constexpr int kThreads = kTX * kTY; // 256 threads per block
 constexpr int kMaxRedValues = 4;
 constexpr int kMarchX = 128;        // columns per block of the row-marching stencil kernels
-constexpr int kUnrollB = 2;
-constexpr int kRingRows = 6;        // shared-memory ring depth of the row-marching kernels         // 16-byte vectors in flight per thread in streaming kernels
+constexpr int kUnrollB = 2;         // 16-byte vectors in flight per thread in streaming kernels
+constexpr int kRingRows = 6;        // shared-memory ring depth of the row-marching kernels
 constexpr int kMaxChebSteps = 64;   // chebyshev_nsteps_estimate cap
 constexpr int kMaxChebDegree = 32;
 
@@ -76,7 +76,8 @@ struct DevScalars {
 // One level of the multigrid hierarchy (level 0 aliases the Float32 operator of the mixed form).
 struct MgLevel {
     int nx = 0, ny = 0;
-    float *aE = nullptr, *aN = nullptr, *dP = nullptr, *aP = nullptr;
+    float *aE = nullptr, *aN = nullptr, *dP = nullptr;
+    float *wD = nullptr;  // damped inverse diagonal of the smoother: omega/aP (active rows), 1/aP (identity rows)
     uint8_t *act = nullptr;
     float *x[2] = {nullptr, nullptr};
     float *b = nullptr;
@@ -119,7 +120,7 @@ struct Ctx {
     double *h_prev = nullptr;
     double *cr[2] = {nullptr, nullptr}, *cp[2] = {nullptr, nullptr}; // Chebyshev r/p buffers
     double *r64 = nullptr;                                            // mixed: outer residual
-    float *aP32 = nullptr, *aE32 = nullptr, *aN32 = nullptr, *dP32 = nullptr;
+    float *aP32 = nullptr, *aE32 = nullptr, *aN32 = nullptr, *dP32 = nullptr, *wD32 = nullptr;
     float *b32 = nullptr, *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32[2] = {nullptr, nullptr}, *Ap32 = nullptr;
     float *cr32[2] = {nullptr, nullptr}, *cp32[2] = {nullptr, nullptr};
     double *partials = nullptr;  // kMaxRedValues * max_blocks

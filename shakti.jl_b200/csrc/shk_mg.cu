@@ -30,9 +30,15 @@ namespace shk {
 // Hierarchy construction
 // ---------------------------------------------------------------------------------------------
 
-// Level-0 activity flags: rows assembled by the GROUNDED branch (mask codes 0 and "other").
-__global__ void k_mg_act0(int n, const uint8_t *m8, uint8_t *act) {
-    GSTRIDE(i, n) act[i] = (m8[i] == M_GROUNDED || m8[i] == M_UNKNOWN) ? 1 : 0;
+// Level-0 activity flags (rows assembled by the GROUNDED branch: mask codes 0 and "other") and the
+// smoother's damped inverse diagonal wD = omega/aP on active rows, 1/aP on identity rows, formed in
+// Float64 and rounded once.
+__global__ void k_mg_act0(int n, const uint8_t *m8, const double *aP, double omega, uint8_t *act, float *wD) {
+    GSTRIDE(i, n) {
+        const bool a = m8[i] == M_GROUNDED || m8[i] == M_UNKNOWN;
+        act[i] = a ? 1 : 0;
+        wD[i] = (float)((a ? omega : 1.0) / aP[i]);
+    }
 }
 
 // Fine excess dP = aP - (aE + aW + aN + aS) at level 0 (Float64 operator, 3-array storage).
@@ -83,16 +89,17 @@ __global__ void k_mg_coarsen(int nxf, int nyf, int nxc, int nyc, const double *a
     }
 }
 
-// Float32 copies and the Jacobi diagonal aP = dP + sum of the four couplings.
+// Float32 copies and the smoother's damped inverse diagonal wD = omega/aP with the Jacobi diagonal
+// aP = dP + the four couplings (identity rows: aP = 1, wD = 1).
 __global__ void k_mg_finish_level(int nx, int ny, const double *aE, const double *aN, const double *dP,
-                                  const uint8_t *act, float *fE, float *fN, float *fD, float *fP) {
+                                  const uint8_t *act, double omega, float *fE, float *fN, float *fD, float *fW) {
     GSTRIDE(k, nx * ny) {
         const int ix = k % nx, iy = k / nx;
         const double w = ix > 0 ? aE[k - 1] : 0.0, s = iy > 0 ? aN[k - nx] : 0.0;
         fE[k] = (float)aE[k];
         fN[k] = (float)aN[k];
         fD[k] = (float)dP[k];
-        fP[k] = act[k] ? (float)(dP[k] + (aE[k] + w + aN[k] + s)) : 1.0f;
+        fW[k] = act[k] ? (float)(omega / (dP[k] + (aE[k] + w + aN[k] + s))) : 1.0f;
     }
 }
 
@@ -101,7 +108,7 @@ __global__ void k_mg_finish_level(int nx, int ny, const double *aE, const double
 // ---------------------------------------------------------------------------------------------
 struct Lv {
     int nx, ny;
-    const float *aE, *aN, *dP, *aP;
+    const float *aE, *aN, *dP, *wD;
     const uint8_t *act;
     const int *done;  // the outer CG's stop flag: V-cycles issued after the stop do no work
 };
@@ -120,8 +127,6 @@ __device__ __forceinline__ float lapl_apply(const Lv &L, int ix, int iy, size_t 
     return y;
 }
 
-__device__ __forceinline__ float omega_of(const Lv &L, size_t c, float w) { return L.act[c] ? w : 1.0f; }
-
 // The level kernels use a 2D grid of 32 x 8 blocks, one thread per cell (no div/mod per cell).
 #define CELL2D()                                                                                      \
     if (cg_finished(L.done)) return;                                                                  \
@@ -129,22 +134,22 @@ __device__ __forceinline__ float omega_of(const Lv &L, size_t c, float w) { retu
     const bool inside = ix < L.nx && iy < L.ny;                                                       \
     const size_t k = (size_t)ix + (size_t)iy * L.nx;
 
-// First pre-smoothing sweep from x = 0: x = omega b / aP.  Level 0 reads b in Float64 (the outer
-// residual).
+// First pre-smoothing sweep from x = 0: x = wD b (wD = omega/aP).  Level 0 reads b in Float64 (the
+// outer residual).
 template <typename TB>
-__global__ void k_mg_pre0(Lv L, const TB *b, float *x, float w) {
+__global__ void k_mg_pre0(Lv L, const TB *b, float *x) {
     CELL2D();
-    if (inside) x[k] = omega_of(L, k, w) * (float)b[k] / L.aP[k];
+    if (inside) x[k] = L.wD[k] * (float)b[k];
 }
 
-// One damped-Jacobi sweep: xo = xi + omega (b - A xi) / aP.
+// One damped-Jacobi sweep: xo = xi + wD (b - A xi).
 template <typename TB>
-__global__ void k_mg_sweep(Lv L, const TB *b, const float *xi, float *xo, float w) {
+__global__ void k_mg_sweep(Lv L, const TB *b, const float *xi, float *xo) {
     CELL2D();
     if (!inside) return;
     const float xc = xi[k];
     const float ax = lapl_apply(L, ix, iy, k, xc, [&](size_t q) { return xi[q]; });
-    xo[k] = xc + omega_of(L, k, w) * ((float)b[k] - ax) / L.aP[k];
+    xo[k] = xc + L.wD[k] * ((float)b[k] - ax);
 }
 
 // Restriction of the residual: bc(C) = sum over the active fine cells of aggregate C of (b - A x).
@@ -178,9 +183,9 @@ __device__ __forceinline__ float prolonged(const Lv &L, const float *xi, const f
 }
 
 // Prolongation fused with the first post-smoothing sweep:
-//   xt = xi + omega_c P xc,  xo = xt + omega (b - A xt) / aP.
+//   xt = xi + omega_c P xc,  xo = xt + wD (b - A xt).
 template <typename TB>
-__global__ void k_mg_prolong_sweep(Lv L, const TB *b, const float *xi, const float *xc, int nxc, float wc, float w,
+__global__ void k_mg_prolong_sweep(Lv L, const TB *b, const float *xi, const float *xc, int nxc, float wc,
                                    float *xo) {
     CELL2D();
     if (!inside) return;
@@ -190,16 +195,16 @@ __global__ void k_mg_prolong_sweep(Lv L, const TB *b, const float *xi, const flo
     if (ix > 0) y += L.aE[k - 1] * (xk - prolonged(L, xi, xc, nxc, wc, ix - 1, iy, k - 1));
     if (iy < L.ny - 1) y += L.aN[k] * (xk - prolonged(L, xi, xc, nxc, wc, ix, iy + 1, k + L.nx));
     if (iy > 0) y += L.aN[k - L.nx] * (xk - prolonged(L, xi, xc, nxc, wc, ix, iy - 1, k - L.nx));
-    xo[k] = xk + omega_of(L, k, w) * ((float)b[k] - y) / L.aP[k];
+    xo[k] = xk + L.wD[k] * ((float)b[k] - y);
 }
 
 // Last post-smoothing sweep on level 0, writing z in Float64 and finishing the outer CG's r'z:
-// z = xt + omega (r - A xt)/aP (xt = xi, plus the prolonged coarse correction when PROLONG);
+// z = xt + wD (r - A xt) (xt = xi, plus the prolonged coarse correction when PROLONG);
 // partials r'z, r'r -> init or iteration finish.  1D grid (the grid reduction is 1D).
 template <bool PROLONG>
 __global__ void __launch_bounds__(kThreads) k_mg_last(Lv L, const double *r, const float *xi, const float *xc, int nxc,
-                                                      float wc, float w, double *z, CgDev *cg, int init,
-                                                      double *partials, unsigned int *counter) {
+                                                      float wc, double *z, CgDev *cg, int init, double *partials,
+                                                      unsigned int *counter) {
     if (block_cg_done(&cg->done)) return;
     double red[2] = {0.0, 0.0};
     GSTRIDE(kk, L.nx * L.ny) {
@@ -215,7 +220,7 @@ __global__ void __launch_bounds__(kThreads) k_mg_last(Lv L, const double *r, con
         if (iy < L.ny - 1) y += L.aN[k] * (xk - xt(ix, iy + 1, k + L.nx));
         if (iy > 0) y += L.aN[k - L.nx] * (xk - xt(ix, iy - 1, k - L.nx));
         const double rk = r[k];
-        const double zk = (double)(xk + omega_of(L, k, w) * ((float)rk - y) / L.aP[k]);
+        const double zk = (double)(xk + L.wD[k] * ((float)rk - y));
         z[k] = zk;
         red[0] += rk * zk;
         red[1] += rk * rk;
@@ -239,7 +244,7 @@ constexpr int kFSW = kFW + 2 * kFR, kFSH = kFH + 2 * kFR;   // staged region (36
 constexpr int kFCells = kFSW * kFSH;
 
 struct FusedSm {
-    float b[kFSH][kFSW], aP[kFSH][kFSW], dP[kFSH][kFSW], aE[kFSH][kFSW], aN[kFSH][kFSW];
+    float b[kFSH][kFSW], wD[kFSH][kFSW], dP[kFSH][kFSW], aE[kFSH][kFSW], aN[kFSH][kFSW];
     float x0[kFSH][kFSW], x1[kFSH][kFSW];
     uint8_t act[kFSH][kFSW];
 };
@@ -257,7 +262,7 @@ __device__ __forceinline__ float ax_sm(const FusedSm &S, const float (&X)[kFSH][
 }
 
 // Stages the level's operator and rhs over the tile and its halo; cells outside the level get
-// act = 0, aP = 1 and zeros (never read as neighbours: the bounds tests above skip them).
+// act = 0 and zeros (never read as neighbours: the bounds tests above skip them).
 template <typename TB>
 __device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b, int x0, int y0, double *r64) {
     for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
@@ -267,7 +272,7 @@ __device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b
             const TB bq = b[q];
             if (r64) r64[k] = (double)bq;
             S.b[hy][hx] = (float)bq;
-            S.aP[hy][hx] = L.aP[q];
+            S.wD[hy][hx] = L.wD[q];
             S.dP[hy][hx] = L.dP[q];
             S.aE[hy][hx] = L.aE[q];
             S.aN[hy][hx] = L.aN[q];
@@ -275,7 +280,7 @@ __device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b
         } else {
             if (r64) r64[k] = 0.0;
             S.b[hy][hx] = 0.0f;
-            S.aP[hy][hx] = 1.0f;
+            S.wD[hy][hx] = 0.0f;
             S.dP[hy][hx] = 0.0f;
             S.aE[hy][hx] = 0.0f;
             S.aN[hy][hx] = 0.0f;
@@ -284,24 +289,23 @@ __device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b
     }
 }
 
-// One damped-Jacobi sweep XO = XI + omega (b - A XI)/aP over the staged positions at distance
-// <= reach from the tile (cells inside the level only).
+// One damped-Jacobi sweep XO = XI + wD (b - A XI) over the staged positions at distance <= reach
+// from the tile (cells inside the level only).
 __device__ __forceinline__ void sweep_sm(FusedSm &S, const float (&XI)[kFSH][kFSW], float (&XO)[kFSH][kFSW], int nx,
-                                         int ny, int x0, int y0, int reach, float w) {
+                                         int ny, int x0, int y0, int reach) {
     const int lo = kFR - reach, wdt = kFW + 2 * reach, hgt = kFH + 2 * reach;
     for (int k = threadIdx.x; k < wdt * hgt; k += blockDim.x) {
         const int hx = lo + k % wdt, hy = lo + k / wdt, gx = x0 - kFR + hx, gy = y0 - kFR + hy;
         if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) continue;
         const float ax = ax_sm(S, XI, nx, ny, hx, hy, gx, gy);
-        const float om = S.act[hy][hx] ? w : 1.0f;
-        XO[hy][hx] = XI[hy][hx] + om * (S.b[hy][hx] - ax) / S.aP[hy][hx];
+        XO[hy][hx] = XI[hy][hx] + S.wD[hy][hx] * (S.b[hy][hx] - ax);
     }
 }
 
 // Descending half of level L: x1 = two sweeps from zero (written to xo), and the coarse rhs
 // bc = restriction of b - A x1.  1D grid striding over 32 x 16 tiles.
 template <typename TB>
-__global__ void __launch_bounds__(256) k_mg_down(Lv L, const TB *b, float *xo, int nxc, int nyc, float *bc, float w) {
+__global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo, int nxc, int nyc, float *bc) {
     if (cg_finished(L.done)) return;
     __shared__ FusedSm S;
     const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
@@ -309,13 +313,13 @@ __global__ void __launch_bounds__(256) k_mg_down(Lv L, const TB *b, float *xo, i
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
         stage_level<TB>(S, L, b, x0, y0, nullptr);
         __syncthreads();
-        // first sweep from x = 0 on the whole staged region: x0 = omega b / aP
+        // first sweep from x = 0 on the whole staged region: x0 = wD b
         for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
             const int hx = k % kFSW, hy = k / kFSW;
-            S.x0[hy][hx] = (S.act[hy][hx] ? w : 1.0f) * S.b[hy][hx] / S.aP[hy][hx];
+            S.x0[hy][hx] = S.wD[hy][hx] * S.b[hy][hx];
         }
         __syncthreads();
-        sweep_sm(S, S.x0, S.x1, L.nx, L.ny, x0, y0, 1, w);
+        sweep_sm(S, S.x0, S.x1, L.nx, L.ny, x0, y0, 1);
         __syncthreads();
         for (int k = threadIdx.x; k < kFW * kFH; k += blockDim.x) {
             const int tx = k % kFW, ty = k / kFW, gx = x0 + tx, gy = y0 + ty;
@@ -346,8 +350,8 @@ __global__ void __launch_bounds__(256) k_mg_down(Lv L, const TB *b, float *xo, i
 // sweep writes z in Float64 and the outer CG's r'z, r'r finish the init or the iteration;
 // otherwise it writes the level's result to xo.
 template <typename TB, bool LAST>
-__global__ void __launch_bounds__(256) k_mg_up(Lv L, const TB *b, const float *xi, const float *xc, int nxc, float wc,
-                                               float w, float *xo, double *z, CgDev *cg, int init, double *partials,
+__global__ void __launch_bounds__(256, 6) k_mg_up(Lv L, const TB *b, const float *xi, const float *xc, int nxc, float wc,
+                                               float *xo, double *z, CgDev *cg, int init, double *partials,
                                                unsigned int *counter) {
     if (cg_finished(L.done)) return;
     __shared__ FusedSm S;
@@ -368,23 +372,22 @@ __global__ void __launch_bounds__(256) k_mg_up(Lv L, const TB *b, const float *x
             S.x0[hy][hx] = v;
         }
         __syncthreads();
-        sweep_sm(S, S.x0, S.x1, L.nx, L.ny, x0, y0, 1, w);
+        sweep_sm(S, S.x0, S.x1, L.nx, L.ny, x0, y0, 1);
         __syncthreads();
         for (int k = threadIdx.x; k < kFW * kFH; k += blockDim.x) {
             const int tx = k % kFW, ty = k / kFW, gx = x0 + tx, gy = y0 + ty;
             if (gx >= L.nx || gy >= L.ny) continue;
             const int hx = tx + kFR, hy = ty + kFR;
             const float ax = ax_sm(S, S.x1, L.nx, L.ny, hx, hy, gx, gy);
-            const float om = S.act[hy][hx] ? w : 1.0f;
             const size_t q = (size_t)gx + (size_t)gy * L.nx;
             if (LAST) {
                 const double rk = r64[hy * kFSW + hx];
-                const double zk = (double)(S.x1[hy][hx] + om * ((float)rk - ax) / S.aP[hy][hx]);
+                const double zk = (double)(S.x1[hy][hx] + S.wD[hy][hx] * ((float)rk - ax));
                 z[q] = zk;
                 red[0] += rk * zk;
                 red[1] += rk * rk;
             } else {
-                xo[q] = S.x1[hy][hx] + om * (S.b[hy][hx] - ax) / S.aP[hy][hx];
+                xo[q] = S.x1[hy][hx] + S.wD[hy][hx] * (S.b[hy][hx] - ax);
             }
         }
         __syncthreads();
@@ -400,7 +403,7 @@ __global__ void __launch_bounds__(256) k_mg_up(Lv L, const TB *b, const float *x
 
 // ---------------------------------------------------------------------------------------------
 // Bottom of the V-cycle in one block: every level from `lb` down to the 1 x 1 coarsest level lives
-// in shared memory (29 bytes per cell: aE, aN, dP, aP, x, scratch, b and the activity flag); the
+// in shared memory (29 bytes per cell: aE, aN, dP, wD, x, scratch, b and the activity flag); the
 // block runs the same pre-smoothing / restriction / exact solve / prolongation / post-smoothing
 // sequence as the per-level kernels, separated by __syncthreads, and writes level lb's result to
 // global memory.  This replaces five launches per small level with one launch per V-cycle.
@@ -414,12 +417,12 @@ struct BottomLevel {
 struct BottomPlan {
     int nlev, total;
     BottomLevel lv[kMgMaxLevels];
-    const float *aE[kMgMaxLevels], *aN[kMgMaxLevels], *dP[kMgMaxLevels], *aP[kMgMaxLevels];
+    const float *aE[kMgMaxLevels], *aN[kMgMaxLevels], *dP[kMgMaxLevels], *wD[kMgMaxLevels];
     const uint8_t *act[kMgMaxLevels];
     const int *done;
 };
 
-__global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b_top, float *x_top, int nu, float w,
+__global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b_top, float *x_top, int nu,
                                                     float wc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (cg_finished(P.done)) return;
@@ -433,7 +436,7 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b
             sE[o + i] = P.aE[l][i];
             sN[o + i] = P.aN[l][i];
             sD[o + i] = P.dP[l][i];
-            sP[o + i] = P.aP[l][i];
+            sP[o + i] = P.wD[l][i];
             sA[o + i] = P.act[l][i];
             if (l == 0) sB[o + i] = b_top[i];
         }
@@ -450,11 +453,10 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b
         if (iy > 0) y += sN[o + i - nx] * (xc - X[o + i - nx]);
         return y;
     };
-    auto om = [&](int l, int i) -> float { return sA[P.lv[l].off + i] ? w : 1.0f; };
-    // one damped-Jacobi sweep on level l: Y = X + omega (B - A X)/aP, then X = Y
+    // one damped-Jacobi sweep on level l: Y = X + wD (B - A X), then X = Y (sP holds wD)
     auto sweep = [&](int l) {
         const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
-        for (int i = tid; i < n; i += nt) sY[o + i] = sX[o + i] + om(l, i) * (sB[o + i] - Ax(l, sX, i)) / sP[o + i];
+        for (int i = tid; i < n; i += nt) sY[o + i] = sX[o + i] + sP[o + i] * (sB[o + i] - Ax(l, sX, i));
         __syncthreads();
         for (int i = tid; i < n; i += nt) sX[o + i] = sY[o + i];
         __syncthreads();
@@ -462,7 +464,7 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b
     const int L = P.nlev;
     for (int l = 0; l < L - 1; l++) {  // descend
         const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
-        for (int i = tid; i < n; i += nt) sX[o + i] = om(l, i) * sB[o + i] / sP[o + i];
+        for (int i = tid; i < n; i += nt) sX[o + i] = sP[o + i] * sB[o + i];
         __syncthreads();
         for (int s = 1; s < nu; s++) sweep(l);
         const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, nxc = P.lv[l + 1].nx, nyc = P.lv[l + 1].ny, oc = P.lv[l + 1].off;
@@ -511,14 +513,15 @@ static const dim3 kBlock2d(32, 8);
 static dim3 grid2d(int nx, int ny) { return dim3((unsigned)((nx + 31) / 32), (unsigned)((ny + 7) / 8)); }
 
 static Lv level_view(const MgLevel &m, const int *done) {
-    return Lv{m.nx, m.ny, m.aE, m.aN, m.dP, m.aP, m.act, done};
+    return Lv{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, done};
 }
 
 // The fused two-sweep level kernels serve nu = 2 (the default); other nu use the per-sweep kernels.
 static bool fused(const Ctx *c) { return c->mg_fused && c->mg_nu == 2; }
 static int fused_grid(const Ctx *c, const MgLevel &m) {
     const long long tiles = (long long)((m.nx + kFW - 1) / kFW) * ((m.ny + kFH - 1) / kFH);
-    return (int)std::max(1LL, std::min(tiles, (long long)c->max_blocks));
+    // one resident wave (six 256-thread blocks per SM), striding over the tiles
+    return (int)std::max(1LL, std::min({tiles, (long long)c->max_blocks, (long long)c->num_sms * 6}));
 }
 
 // First level >= 1 from which the rest of the hierarchy fits the bottom kernel's shared memory.
@@ -539,7 +542,7 @@ static size_t bottom_plan(const Ctx *c, int lb, BottomPlan *P) {
     for (int k = 0; k < P->nlev; k++) {
         const MgLevel &m = c->mg[lb + k];
         P->lv[k] = BottomLevel{m.nx, m.ny, off};
-        P->aE[k] = m.aE; P->aN[k] = m.aN; P->dP[k] = m.dP; P->aP[k] = m.aP; P->act[k] = m.act;
+        P->aE[k] = m.aE; P->aN[k] = m.aN; P->dP[k] = m.dP; P->wD[k] = m.wD; P->act[k] = m.act;
         off += m.nx * m.ny;
     }
     P->total = off;
@@ -552,7 +555,8 @@ int mg_setup(Ctx *c) {
     if (grid2d(c->nx, c->ny).y > 65535u) return fail(c, SHK_BAD_ARG, "multigrid needs ny <= 524280");
     MgLevel *lv = c->mg;
     const int n0 = c->nx * c->ny;
-    k_mg_act0<<<mg_grid(c, n0), kThreads, 0, c->stream>>>(n0, c->mask8, lv[0].act);
+    k_mg_act0<<<mg_grid(c, n0), kThreads, 0, c->stream>>>(n0, c->mask8, c->aP, (double)c->mg_omega, lv[0].act,
+                                                           lv[0].wD);
     c->launches++;
     for (int l = 0; l + 1 < c->mg_levels; l++) {
         const MgLevel &f = lv[l];
@@ -562,7 +566,8 @@ int mg_setup(Ctx *c) {
         k_mg_coarsen<<<mg_grid(c, (long long)g.nx * g.ny), kThreads, 0, c->stream>>>(
             f.nx, f.ny, g.nx, g.ny, aEf, aNf, dPf, c->aP, f.act, g.aE64, g.aN64, g.dP64, g.act);
         k_mg_finish_level<<<mg_grid(c, (long long)g.nx * g.ny), kThreads, 0, c->stream>>>(
-            g.nx, g.ny, g.aE64, g.aN64, g.dP64, g.act, (float *)g.aE, (float *)g.aN, (float *)g.dP, (float *)g.aP);
+            g.nx, g.ny, g.aE64, g.aN64, g.dP64, g.act, (double)c->mg_omega, (float *)g.aE, (float *)g.aN,
+            (float *)g.dP, (float *)g.wD);
         c->launches += 2;
     }
     if (c->mg_levels > 1) {
@@ -583,12 +588,12 @@ int mg_setup(Ctx *c) {
 static int vcycle(Ctx *c, int l, const int *done, int *res) {
     MgLevel &m = c->mg[l];
     const Lv L = level_view(m, done);
-    const float w = c->mg_omega, wc = c->mg_omega_c;
+    const float wc = c->mg_omega_c;
     if (l == bottom_level(c)) {
         BottomPlan P;
         const size_t smem = bottom_plan(c, l, &P);
         P.done = done;
-        k_mg_bottom<<<1, 1024, smem, c->stream>>>(P, m.b, m.x[0], c->mg_nu, w, wc);
+        k_mg_bottom<<<1, 1024, smem, c->stream>>>(P, m.b, m.x[0], c->mg_nu, wc);
         c->launches++;
         *res = 0;
         return SHK_OK;
@@ -596,32 +601,32 @@ static int vcycle(Ctx *c, int l, const int *done, int *res) {
     MgLevel &g = c->mg[l + 1];
     if (fused(c)) {
         const int gt = fused_grid(c, m);
-        k_mg_down<float><<<gt, 256, 0, c->stream>>>(L, m.b, m.x[0], g.nx, g.ny, g.b, w);
+        k_mg_down<float><<<gt, 256, 0, c->stream>>>(L, m.b, m.x[0], g.nx, g.ny, g.b);
         c->launches++;
         int gres = 0;
         int rc = vcycle(c, l + 1, done, &gres);
         if (rc) return rc;
-        k_mg_up<float, false><<<gt, 256, 0, c->stream>>>(L, m.b, m.x[0], g.x[gres], g.nx, wc, w, m.x[1], nullptr,
+        k_mg_up<float, false><<<gt, 256, 0, c->stream>>>(L, m.b, m.x[0], g.x[gres], g.nx, wc, m.x[1], nullptr,
                                                          nullptr, 0, nullptr, nullptr);
         c->launches++;
         *res = 1;
         return SHK_OK;
     }
     const dim3 gf = grid2d(m.nx, m.ny), gc = grid2d(g.nx, g.ny);
-    k_mg_pre0<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[0], w);
+    k_mg_pre0<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[0]);
     int cur = 0;
     for (int s = 1; s < c->mg_nu; s++, cur ^= 1)
-        k_mg_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1], w);
+        k_mg_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1]);
     k_mg_restrict<float><<<gc, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], g.nx, g.ny, g.b);
     c->launches += 1 + c->mg_nu;
     int gres = 0;
     int rc = vcycle(c, l + 1, done, &gres);
     if (rc) return rc;
-    k_mg_prolong_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], g.x[gres], g.nx, wc, w,
+    k_mg_prolong_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], g.x[gres], g.nx, wc,
                                                               m.x[cur ^ 1]);
     cur ^= 1;
     for (int s = 1; s < c->mg_nu; s++, cur ^= 1)
-        k_mg_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1], w);
+        k_mg_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1]);
     c->launches += c->mg_nu;
     *res = cur;
     return SHK_OK;
@@ -632,10 +637,10 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
     MgLevel &m = c->mg[0];
     const Lv L = level_view(m, &cg->done);
     const int n = m.nx * m.ny;
-    const float w = c->mg_omega, wc = c->mg_omega_c;
+    const float wc = c->mg_omega_c;
     const int gl = std::min(c->max_blocks, std::max(1, std::min(c->num_sms * 8, (n + kThreads - 1) / kThreads)));
     if (c->mg_levels == 1) {
-        k_mg_last<false><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[0], nullptr, 1, wc, w, z, cg, init, c->partials,
+        k_mg_last<false><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[0], nullptr, 1, wc, z, cg, init, c->partials,
                                                          c->counter);
         c->launches++;
         return check_launch(c, "multigrid apply");
@@ -643,37 +648,37 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
     MgLevel &g = c->mg[1];
     if (fused(c)) {
         const int gt = fused_grid(c, m);
-        k_mg_down<double><<<gt, 256, 0, c->stream>>>(L, r, m.x[0], g.nx, g.ny, g.b, w);
+        k_mg_down<double><<<gt, 256, 0, c->stream>>>(L, r, m.x[0], g.nx, g.ny, g.b);
         c->launches++;
         int gres = 0;
         int rc = vcycle(c, 1, &cg->done, &gres);
         if (rc) return rc;
-        k_mg_up<double, true><<<gt, 256, 0, c->stream>>>(L, r, m.x[0], g.x[gres], g.nx, wc, w, nullptr, z, cg, init,
+        k_mg_up<double, true><<<gt, 256, 0, c->stream>>>(L, r, m.x[0], g.x[gres], g.nx, wc, nullptr, z, cg, init,
                                                          c->partials, c->counter);
         c->launches++;
         return check_launch(c, "multigrid apply");
     }
     const dim3 gf = grid2d(m.nx, m.ny), gc = grid2d(g.nx, g.ny);
-    k_mg_pre0<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[0], w);
+    k_mg_pre0<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[0]);
     int cur = 0;
     for (int s = 1; s < c->mg_nu; s++, cur ^= 1)
-        k_mg_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1], w);
+        k_mg_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1]);
     k_mg_restrict<double><<<gc, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], g.nx, g.ny, g.b);
     c->launches += 1 + c->mg_nu;
     int gres = 0;
     int rc = vcycle(c, 1, &cg->done, &gres);
     if (rc) return rc;
     if (c->mg_nu == 1) {
-        k_mg_last<true><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[cur], g.x[gres], g.nx, wc, w, z, cg, init,
+        k_mg_last<true><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[cur], g.x[gres], g.nx, wc, z, cg, init,
                                                         c->partials, c->counter);
         c->launches++;
     } else {
-        k_mg_prolong_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], g.x[gres], g.nx, wc, w,
+        k_mg_prolong_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], g.x[gres], g.nx, wc,
                                                                    m.x[cur ^ 1]);
         cur ^= 1;
         for (int s = 2; s < c->mg_nu; s++, cur ^= 1)
-            k_mg_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1], w);
-        k_mg_last<false><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[cur], nullptr, 1, wc, w, z, cg, init, c->partials,
+            k_mg_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1]);
+        k_mg_last<false><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[cur], nullptr, 1, wc, z, cg, init, c->partials,
                                                          c->counter);
         c->launches += c->mg_nu;
     }
