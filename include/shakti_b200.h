@@ -232,6 +232,42 @@ SHK_API int shk_run(void *ctx, int head_scheme, double dt, int tsteps, double *t
 SHK_API long shk_kernel_launches(const void *ctx);
 
 /* ---------------------------------------------------------------------------------------------
+ * Ensembles.  The reference advances one Simulation at a time; a caller with many independent
+ * simulations (parameter sweeps, uncertainty ensembles) loops run! over them
+ * (src/run.jl:21-63).  These calls advance N instances together on one GPU: each batched kernel is
+ * one launch over every instance, and each timestep is one CUDA graph launch whose Picard and CG
+ * loops run on the device (instances that have converged skip the remaining iterations).
+ *
+ * Each instance is an ordinary context (shk_create ... shk_set_initial_conditions), of any grid
+ * size; all on the same device.  The ensemble runs the elliptic head scheme with Float64 Jacobi
+ * CG, no head relaxation, and a constant melt input (update_ieb! is then a no-op), and gives each
+ * instance the same fields as its own shk_step would, up to the rounding of the reductions'
+ * block counts.
+ * --------------------------------------------------------------------------------------------- */
+typedef struct {
+    long long steps, steps_converged;   /* timesteps run / with a converged Picard loop */
+    long long picard_iters, cg_iters;   /* totals over those timesteps */
+    int last_picard_iters, last_converged;
+    int march_th;                       /* row-marching tile height in use (autotuned) */
+    int pad;
+    double max_dh, max_h;               /* last Picard check of the last timestep */
+} shk_ensemble_stats;
+
+/* N contexts -> one ensemble (the contexts stay owned by the caller and must outlive it). */
+SHK_API int shk_ensemble_create(int n, void *const *ctxs, void *stream, void **ens_out);
+SHK_API int shk_ensemble_destroy(void *ens);
+SHK_API const char *shk_ensemble_last_error(const void *ens);
+/* Measured choice of the CG stencil kernel's tile height per grid size; th_out (n) may be NULL. */
+SHK_API int shk_ensemble_autotune(void *ens, int iters, int *th_out);
+/* tsteps timesteps of dt for every instance (step!, src/run.jl:82-88).  per_instance (n entries)
+ * may be NULL.  Returns SHK_NOT_CONVERGED if any instance's Picard loop did not converge. */
+SHK_API int shk_ensemble_run(void *ens, double dt, int tsteps, const shk_picard_opts *po,
+                             const shk_cg_opts *o, shk_ensemble_stats *per_instance);
+/* Blocks per launch of each batched kernel family (stencil, row-marching, streaming, flat). */
+SHK_API int shk_ensemble_launch_counts(const void *ens, int *stencil, int *march, int *stream,
+                                       int *flat);
+
+/* ---------------------------------------------------------------------------------------------
  * Allocation-free solve.  No counterpart in the reference: it exists for callers that cannot
  * allocate device memory when they solve -- an application whose device memory all belongs to its
  * own pool allocator, a real-time loop that cannot afford the device-wide synchronisation of

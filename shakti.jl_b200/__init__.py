@@ -22,6 +22,7 @@ from .simulation import (AbstractHeadScheme, EllipticHeadScheme, ParabolicHeadSc
                          NoSensibleHeat, AbstractOpenBySlidingScheme, WithOpenBySliding, NoOpenBySliding,
                          AbstractObserver, NoObserver, LiveObserver, Simulation, run, step, step_h, step_b,
                          update_ieb, picard_status, set_initial_conditions)
+from .ensemble import Ensemble
 from . import configs
 
 backend = "CUDA"

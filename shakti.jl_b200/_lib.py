@@ -64,6 +64,12 @@ class shk_picard_stats(C.Structure):
                 ("cg_solves", C.c_int), ("cg_breakdowns", C.c_int), ("max_dh", C.c_double), ("max_h", C.c_double)]
 
 
+class shk_ensemble_stats(C.Structure):
+    _fields_ = [("steps", C.c_longlong), ("steps_converged", C.c_longlong), ("picard_iters", C.c_longlong),
+                ("cg_iters", C.c_longlong), ("last_picard_iters", C.c_int), ("last_converged", C.c_int),
+                ("march_th", C.c_int), ("pad", C.c_int), ("max_dh", C.c_double), ("max_h", C.c_double)]
+
+
 # Every symbol include/shakti_b200.h declares, with (restype, argtypes).
 VP = C.c_void_p
 SIGNATURES = {
@@ -102,6 +108,14 @@ SIGNATURES = {
     "shk_kernel_launches": (C.c_long, [VP]),
     "shk_cg_solve_static": (C.c_int, [C.c_int, C.c_int, VP, VP, VP, VP, VP, C.POINTER(shk_cg_opts),
                                       C.POINTER(shk_cg_stats), VP]),
+    "shk_ensemble_create": (C.c_int, [C.c_int, C.POINTER(VP), VP, C.POINTER(VP)]),
+    "shk_ensemble_destroy": (C.c_int, [VP]),
+    "shk_ensemble_last_error": (C.c_char_p, [VP]),
+    "shk_ensemble_autotune": (C.c_int, [VP, C.c_int, C.POINTER(C.c_int)]),
+    "shk_ensemble_run": (C.c_int, [VP, C.c_double, C.c_int, C.POINTER(shk_picard_opts), C.POINTER(shk_cg_opts),
+                                   C.POINTER(shk_ensemble_stats)]),
+    "shk_ensemble_launch_counts": (C.c_int, [VP, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                             C.POINTER(C.c_int)]),
 }
 
 _LIB = None

@@ -110,19 +110,27 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV]) {
     __syncthreads();
 }
 
-// Grid reduction without inter-block waiting.  Returns true in exactly one block (the last to
-// arrive); there, thread 0 holds the totals in out[] (other threads: unspecified).
+// A block's place among the blocks that work on one instance: the single-instance kernels use
+// their whole grid; the ensemble kernels give each instance a contiguous range of one grid.
+struct Blk {
+    int id, n;
+};
+__device__ __forceinline__ Blk grid_blk() { return Blk{(int)blockIdx.x, (int)gridDim.x}; }
+
+// Grid reduction without inter-block waiting over the B.n blocks of one instance.  Returns true in
+// exactly one block (the last to arrive); there, thread 0 holds the totals in out[] (other threads:
+// unspecified).
 template <int NV, bool MAX>
-__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, unsigned int *counter,
+__device__ __forceinline__ bool grid_reduce(Blk B, double (&v)[NV], double *partials, unsigned int *counter,
                                             double (&out)[NV]) {
     __shared__ int am_last;
     block_reduce<NV, MAX>(v);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < NV; k++) partials[(size_t)k * gridDim.x + blockIdx.x] = v[k];
+        for (int k = 0; k < NV; k++) partials[(size_t)k * B.n + B.id] = v[k];
         __threadfence();
         unsigned int prev = atomicAdd(counter, 1u);
-        am_last = (prev == gridDim.x - 1);
+        am_last = (prev == (unsigned int)B.n - 1);
     }
     __syncthreads();
     if (!am_last) return false;
@@ -131,8 +139,8 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, u
 #pragma unroll
     for (int k = 0; k < NV; k++) {
         acc[k] = 0.0;
-        for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
-            acc[k] = red_op<MAX>(acc[k], __ldcg(&partials[(size_t)k * gridDim.x + i]));
+        for (int i = threadIdx.x; i < B.n; i += blockDim.x)
+            acc[k] = red_op<MAX>(acc[k], __ldcg(&partials[(size_t)k * B.n + i]));
     }
     block_reduce<NV, MAX>(acc);
     if (threadIdx.x == 0) {
@@ -142,6 +150,12 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, u
         __threadfence();
     }
     return true;
+}
+
+template <int NV, bool MAX>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, unsigned int *counter,
+                                            double (&out)[NV]) {
+    return grid_reduce<NV, MAX>(grid_blk(), v, partials, counter, out);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -172,6 +186,19 @@ __device__ __forceinline__ bool block_cg_done(const int *done) {
     if (threadIdx.x == 0 && threadIdx.y == 0) d = done ? *(const volatile int *)done : 0;
     __syncthreads();
     return d != 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Ensemble kernels: the block's instance descriptor, copied to shared memory once per block, and
+// the block's place among that instance's blocks of kernel family FAM.
+// ---------------------------------------------------------------------------------------------
+static_assert(sizeof(EnsInst) % 8 == 0, "EnsInst is copied in 8-byte words");
+__device__ __forceinline__ Blk ens_stage(EnsInst &dst, const EnsInst *E, const int *b2i, int fam) {
+    const long long *src = reinterpret_cast<const long long *>(&E[b2i[blockIdx.x]]);
+    long long *d = reinterpret_cast<long long *>(&dst);
+    for (int k = threadIdx.x; k < (int)(sizeof(EnsInst) / 8); k += blockDim.x) d[k] = src[k];
+    __syncthreads();
+    return Blk{(int)blockIdx.x - dst.blk0[fam], dst.nblk[fam]};
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -251,16 +251,16 @@ struct FaceSm {
 };
 
 template <bool FROM_H, bool CHECK>
-__global__ void __launch_bounds__(kThreads, 4) k_tail(int nx, int ny, Params P, Sliding L, shk_state s,
-                                                   const uint8_t *__restrict__ m8,
-                                                   const double *__restrict__ h_prev, double *partials,
-                                                   unsigned int *counter, PicDev *pic) {
+__device__ __forceinline__ void tail_body(Blk B, int nx, int ny, const Params &P, const Sliding &L,
+                                          const shk_state &s, const uint8_t *__restrict__ m8,
+                                          const double *__restrict__ h_prev, double *partials, unsigned int *counter,
+                                          PicDev *pic) {
     __shared__ CellQ cq[kTailHH][kTailHW];
     __shared__ FaceSm fx[kTailXF], fy[kTailYF];
     const int tiles_x = (nx + kTailW - 1) / kTailW, ntiles = tiles_x * ((ny + kTailH - 1) / kTailH);
     const int tid = threadIdx.x, tx = tid % kTailW, ty = tid / kTailW;
     double red[2] = {0.0, 0.0};
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (int t = B.id; t < ntiles; t += B.n) {
         const int x0 = (t % tiles_x) * kTailW, y0 = (t / tiles_x) * kTailH;
         // (1) cells of the tile and its halo
         for (int k = tid; k < kTailHH * kTailHW; k += kThreads) {
@@ -349,11 +349,19 @@ __global__ void __launch_bounds__(kThreads, 4) k_tail(int nx, int ny, Params P, 
     }
     if (CHECK) {
         double out[2];
-        if (grid_reduce<2, true>(red, partials, counter, out) && threadIdx.x == 0) {
+        if (grid_reduce<2, true>(B, red, partials, counter, out) && threadIdx.x == 0) {
             pic->dmax = out[0];
             pic->hmax = out[1];
         }
     }
+}
+
+template <bool FROM_H, bool CHECK>
+__global__ void __launch_bounds__(kThreads, 4) k_tail(int nx, int ny, Params P, Sliding L, shk_state s,
+                                                      const uint8_t *__restrict__ m8,
+                                                      const double *__restrict__ h_prev, double *partials,
+                                                      unsigned int *counter, PicDev *pic) {
+    tail_body<FROM_H, CHECK>(grid_blk(), nx, ny, P, L, s, m8, h_prev, partials, counter, pic);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -376,13 +384,13 @@ __device__ __forceinline__ double bK(int kfs, double K1, double K2, uint8_t m2) 
 }
 
 template <bool PARABOLIC>
-__global__ void __launch_bounds__(kThreads) k_assemble(int nx, int ny, Params P, int kfs, double dt,
-                                                       shk_state s, const uint8_t *__restrict__ m8,
-                                                       double *__restrict__ aP, double *__restrict__ aE,
-                                                       double *__restrict__ aN, double *__restrict__ rhs,
-                                                       double *__restrict__ h_prev) {
+__device__ __forceinline__ void assemble_body(Blk B, int nx, int ny, const Params &P, int kfs, double dt,
+                                              const shk_state &s, const uint8_t *__restrict__ m8,
+                                              double *__restrict__ aP, double *__restrict__ aE,
+                                              double *__restrict__ aN, double *__restrict__ rhs,
+                                              double *__restrict__ h_prev) {
     Tiles T(nx, ny);
-    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+    for (int t = B.id; t < T.ntiles; t += B.n) {
         int ix, iy;
         T.cell(t, ix, iy);
         if (ix >= nx || iy >= ny) continue;
@@ -434,6 +442,15 @@ __global__ void __launch_bounds__(kThreads) k_assemble(int nx, int ny, Params P,
     }
 }
 
+template <bool PARABOLIC>
+__global__ void __launch_bounds__(kThreads) k_assemble(int nx, int ny, Params P, int kfs, double dt,
+                                                       shk_state s, const uint8_t *__restrict__ m8,
+                                                       double *__restrict__ aP, double *__restrict__ aE,
+                                                       double *__restrict__ aN, double *__restrict__ rhs,
+                                                       double *__restrict__ h_prev) {
+    assemble_body<PARABOLIC>(grid_blk(), nx, ny, P, kfs, dt, s, m8, aP, aE, aN, rhs, h_prev);
+}
+
 __global__ void k_export_mfls(int nx, int ny, const double *aP, const double *aE, const double *aN,
                               const double *rhs, double *oP, double *oE, double *oW, double *oN, double *oS,
                               double *orhs) {
@@ -457,8 +474,8 @@ __global__ void k_relax(int n, double alpha, double *h, const double *h_prev) {
 
 // compute_b_implicit/explicit_kernel! (src/gap_height.jl:117-135) then compute_beta! (:47-52).
 template <bool IMPLICIT>
-__global__ void k_gap_b(int n, Params P, double dt, shk_state s, const uint8_t *__restrict__ m8) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+__device__ __forceinline__ void gap_b_body(Blk B, int n, const Params &P, double dt, const shk_state &s) {
+    for (int i = B.id * blockDim.x + threadIdx.x; i < n; i += B.n * blockDim.x) {
         double b = s.b[i];
         if (s.mask[i] == 0.0) {
             const double Nc = s.N[i];
@@ -475,11 +492,16 @@ __global__ void k_gap_b(int n, Params P, double dt, shk_state s, const uint8_t *
     }
 }
 
+template <bool IMPLICIT>
+__global__ void k_gap_b(int n, Params P, double dt, shk_state s, const uint8_t *__restrict__ m8) {
+    gap_b_body<IMPLICIT>(grid_blk(), n, P, dt, s);
+}
+
 // compute_b_x!/compute_b_y! (src/gap_height.jl:75-108)
-__global__ void k_gap_faces(int nx, int ny, shk_state s) {
+__device__ __forceinline__ void gap_faces_body(Blk B, int nx, int ny, const shk_state &s) {
     const long long nxf = (long long)(nx + 1) * ny, nyf = (long long)nx * (ny + 1);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nxf + nyf;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = B.id * (long long)blockDim.x + threadIdx.x; i < nxf + nyf;
+         i += (long long)B.n * blockDim.x) {
         if (i < nxf) {
             int f = (int)(i % (nx + 1)), iy = (int)(i / (nx + 1));
             double v;
@@ -498,6 +520,7 @@ __global__ void k_gap_faces(int nx, int ny, shk_state s) {
         }
     }
 }
+__global__ void k_gap_faces(int nx, int ny, shk_state s) { gap_faces_body(grid_blk(), nx, ny, s); }
 
 __global__ void k_fill(size_t n, double *dst, double v, const double *base) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -616,6 +639,50 @@ int launch_fill_plus_base(Ctx *c, double *dst, double v, const double *base, siz
     k_fill<<<flat_grid(c, (long long)n), kThreads, 0, c->stream>>>(n, dst, v, base);
     c->launches++;
     return check_launch(c, "k_fill");
+}
+
+// ---------------------------------------------------------------------------------------------
+// Ensemble: the same bodies over every instance in one grid (block -> instance table per family).
+// Instances whose Picard loop has finished this timestep return at once.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_ens_assemble(EnsInst *E, const int *b2i) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_STENCIL);
+    if (!I.pic_active) return;
+    assemble_body<false>(B, I.nx, I.ny, I.P, I.kfs, 0.0, I.st, I.mask8, I.aP, I.aE, I.aN, I.rhs, I.h_prev);
+}
+
+__global__ void __launch_bounds__(kThreads, 4) k_ens_tail(EnsInst *E, const int *b2i) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_TAIL);
+    if (!I.pic_active) return;
+    tail_body<true, true>(B, I.nx, I.ny, I.P, I.SL, I.st, I.mask8, I.h_prev, I.partials, I.counter, I.pic);
+}
+
+// step_b!: gap update of the cells, then the face averages (two launches: the faces read
+// neighbouring cells' new b)
+__global__ void __launch_bounds__(kThreads) k_ens_gap_cells(EnsInst *E, const int *b2i, const EnsCtl *ctl) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_FLAT);
+    const double dt = ctl->dt;
+    if (I.gap == SHK_GAP_IMPLICIT) gap_b_body<true>(B, I.nx * I.ny, I.P, dt, I.st);
+    else gap_b_body<false>(B, I.nx * I.ny, I.P, dt, I.st);
+}
+__global__ void __launch_bounds__(kThreads) k_ens_gap_faces(EnsInst *E, const int *b2i) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_FLAT);
+    gap_faces_body(B, I.nx, I.ny, I.st);
+}
+
+void ens_assemble(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks) {
+    k_ens_assemble<<<nblocks, kThreads, 0, s>>>(E, b2i);
+}
+void ens_tail(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks) {
+    k_ens_tail<<<nblocks, kThreads, 0, s>>>(E, b2i);
+}
+void ens_gap(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, const EnsCtl *ctl) {
+    k_ens_gap_cells<<<nblocks, kThreads, 0, s>>>(E, b2i, ctl);
+    k_ens_gap_faces<<<nblocks, kThreads, 0, s>>>(E, b2i);
 }
 
 } // namespace shk

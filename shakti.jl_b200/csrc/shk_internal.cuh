@@ -155,6 +155,44 @@ struct Ctx {
 };
 
 // ---------------------------------------------------------------------------------------------
+// Ensemble of independent instances (shk_ensemble.cu).  Each batched kernel runs one grid over
+// every instance: the blocks of a kernel family are split into contiguous per-instance ranges
+// (blk0, nblk), and a block-to-instance table maps a block to its instance.  An instance's state,
+// workspace and device scalars are those of its own context.
+// ---------------------------------------------------------------------------------------------
+// Families, each with the grid its single-instance kernel uses, so that every reduction of an
+// instance sums the same per-block partials in the same order as its own context would.
+enum { EF_STENCIL = 0, EF_TAIL = 1, EF_MARCH = 2, EF_STREAM = 3, EF_FLAT = 4, EF_N = 5 };
+
+struct alignas(8) EnsInst {
+    int nx, ny, kfs, gap, march_th, size_class;
+    int blk0[EF_N], nblk[EF_N];
+    Params P;
+    Sliding SL;
+    shk_state st;
+    const uint8_t *mask8;
+    double *aP, *aE, *aN, *rhs, *x, *r, *p0, *p1, *Ap, *h_prev;
+    double *partials;
+    unsigned int *counter;
+    CgDev *cg;
+    PicDev *pic;
+    // loop control and statistics, written on the device
+    int pic_active, pic_iter, pic_converged, cg_breakdowns;
+    long long cg_iters, cg_solves;
+    long long total_picard, total_cg, steps_converged, steps;
+    double max_dh, max_h;
+};
+
+struct alignas(8) EnsCtl {
+    int n;                      // instances
+    int picard_iters, check_every, stop_rule;
+    double picard_tol, atol, rtol;
+    long long itmax;            // 0: 2 n cells per instance
+    unsigned int pic_trips, cg_trips;
+    double dt;
+};
+
+// ---------------------------------------------------------------------------------------------
 // Host helpers
 // ---------------------------------------------------------------------------------------------
 int fail(Ctx *c, int status, const std::string &msg);
@@ -179,6 +217,18 @@ int cheb_set_bounds(Ctx *c, double lmin, double lmax);
 int launch_chebyshev_apply_standalone(Ctx *c, int degree, const double *x, double *y);
 int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st);
 int read_scalars(Ctx *c);
+
+// ensemble kernels: shk_fields.cu
+void ens_assemble(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks);
+void ens_tail(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks);
+void ens_gap(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, const EnsCtl *ctl);
+// ensemble kernels: shk_krylov.cu
+void ens_cg_reset(cudaStream_t s, EnsInst *E, EnsCtl *ctl, int n);
+void ens_cg_init(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks);
+void ens_cg_A(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, int parity);
+void ens_cg_B(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, int parity);
+void ens_cg_finish(cudaStream_t s, EnsInst *E, const EnsCtl *ctl, int n, const int *b2i, int nblocks);
+void ens_cg_cond(cudaStream_t s, EnsInst *E, EnsCtl *ctl, int n, cudaGraphConditionalHandle h);
 
 // shk_mg.cu
 int mg_levels_for(int nx, int ny, int *dims, int maxl);

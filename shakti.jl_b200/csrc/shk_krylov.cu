@@ -64,12 +64,12 @@ __global__ void __launch_bounds__(kThreads) k_matvec(int nx, int ny, const T *aP
 // r = b - A x0 (x0 == nullptr: r = b), x = 0; JAC: partials r'z, r'r, b'b -> init finish;
 // otherwise partials r'r, b'b are parked for the Chebyshev init pass.
 template <typename T, bool JAC>
-__global__ void __launch_bounds__(kThreads) k_cg_init(int nx, int ny, const T *aP, const T *aE, const T *aN,
-                                                      const double *x0, const T *b, T *r, T *x, CgDev *cg,
-                                                      double *partials, unsigned int *counter) {
+__device__ __forceinline__ void cg_init_body(Blk B, int nx, int ny, const T *aP, const T *aE, const T *aN,
+                                             const double *x0, const T *b, T *r, T *x, CgDev *cg, double *partials,
+                                             unsigned int *counter) {
     Tiles Tl(nx, ny);
     double red[3] = {0.0, 0.0, 0.0};
-    for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
+    for (int t = B.id; t < Tl.ntiles; t += B.n) {
         int ix, iy;
         Tl.cell(t, ix, iy);
         if (ix >= nx || iy >= ny) continue;
@@ -92,13 +92,20 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(int nx, int ny, const T *a
         red[2] += (double)bc * (double)bc;
     }
     double out[3];
-    if (grid_reduce<3, false>(red, partials, counter, out) && threadIdx.x == 0) {
+    if (grid_reduce<3, false>(B, red, partials, counter, out) && threadIdx.x == 0) {
         if (JAC) cg_init_finish(cg, out[0], out[1], out[2]);
         else {
             cg->rr = out[1];    // parked: squared norms, consumed by the Chebyshev init pass
             cg->bnorm = out[2];
         }
     }
+}
+
+template <typename T, bool JAC>
+__global__ void __launch_bounds__(kThreads) k_cg_init(int nx, int ny, const T *aP, const T *aE, const T *aN,
+                                                      const double *x0, const T *b, T *r, T *x, CgDev *cg,
+                                                      double *partials, unsigned int *counter) {
+    cg_init_body<T, JAC>(grid_blk(), nx, ny, aP, aE, aN, x0, b, r, x, cg, partials, counter);
 }
 
 // A: p_new = z + beta*p_old (p_new = z on the first iteration), Ap = A p_new, partial p'Ap.
@@ -120,14 +127,13 @@ __device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
 // the diagonal excess computed in Float64 and rounded once.  Storing edge conductances and the
 // excess (rather than aP and the couplings) keeps the rounded operator accurate entry by entry
 // for this nearly singular M-matrix, whatever its condition number.
-template <typename T, bool JAC, bool LAPL = false>
-__global__ void __launch_bounds__(kMarchX, 6) k_cg_A(int nx, int ny, int TH, const T *__restrict__ aP,
-                                                  const T *__restrict__ aE, const T *__restrict__ aN,
-                                                  const T *__restrict__ r, const T *__restrict__ zbuf,
-                                                  const T *__restrict__ p_old, T *__restrict__ p_new,
-                                                  T *__restrict__ Ap, CgDev *cg, double *partials,
-                                                  unsigned int *counter, double eps_curv,
-                                                  const T *__restrict__ dP = nullptr) {
+template <typename T, bool JAC, bool LAPL>
+__device__ __forceinline__ void cg_A_body(Blk B, int nx, int ny, int TH, const T *__restrict__ aP,
+                                          const T *__restrict__ aE, const T *__restrict__ aN,
+                                          const T *__restrict__ r, const T *__restrict__ zbuf,
+                                          const T *__restrict__ p_old, T *__restrict__ p_new, T *__restrict__ Ap,
+                                          CgDev *cg, double *partials, unsigned int *counter, double eps_curv,
+                                          const T *__restrict__ dP) {
     const CgView cv = block_cg_view(cg);
     if (cv.done) return;
     constexpr int R = kRingRows, W = kMarchX + 2;
@@ -137,7 +143,7 @@ __global__ void __launch_bounds__(kMarchX, 6) k_cg_A(int nx, int ny, int TH, con
     const bool first = cv.first != 0;
     const T beta = (T)cv.beta;
     const int tiles_x = (nx + kMarchX - 1) / kMarchX;
-    const int x0 = (blockIdx.x % tiles_x) * kMarchX, y0 = (blockIdx.x / tiles_x) * TH;
+    const int x0 = (B.id % tiles_x) * kMarchX, y0 = (B.id / tiles_x) * TH;
     const int tid = threadIdx.x, ix = x0 + tid;
     const bool inx = ix < nx;
     const int y1 = min(y0 + TH, ny);
@@ -235,7 +241,7 @@ __global__ void __launch_bounds__(kMarchX, 6) k_cg_A(int nx, int ny, int TH, con
     }
     __pipeline_wait_prior(0);
     double red[1] = {acc}, out[1];
-    if (grid_reduce<1, false>(red, partials, counter, out) && threadIdx.x == 0) {
+    if (grid_reduce<1, false>(B, red, partials, counter, out) && threadIdx.x == 0) {
         const double pAp = out[0];
         cg->pAp = pAp;
         const double lim = eps_curv * cg->pNorm2;
@@ -246,6 +252,18 @@ __global__ void __launch_bounds__(kMarchX, 6) k_cg_A(int nx, int ny, int TH, con
             cg->alpha = cg->gamma / pAp;
         }
     }
+}
+
+template <typename T, bool JAC, bool LAPL = false>
+__global__ void __launch_bounds__(kMarchX, 6) k_cg_A(int nx, int ny, int TH, const T *__restrict__ aP,
+                                                  const T *__restrict__ aE, const T *__restrict__ aN,
+                                                  const T *__restrict__ r, const T *__restrict__ zbuf,
+                                                  const T *__restrict__ p_old, T *__restrict__ p_new,
+                                                  T *__restrict__ Ap, CgDev *cg, double *partials,
+                                                  unsigned int *counter, double eps_curv,
+                                                  const T *__restrict__ dP = nullptr) {
+    cg_A_body<T, JAC, LAPL>(grid_blk(), nx, ny, TH, aP, aE, aN, r, zbuf, p_old, p_new, Ap, cg, partials, counter,
+                            eps_curv, dP);
 }
 
 // 16-byte vectors for the streaming kernels.
@@ -269,9 +287,9 @@ template <> struct Vec16<float> {
 // 16-byte loads, kUnrollB vectors in flight per thread; scalar tail for n not a multiple of the
 // vector width.
 template <typename T, bool JAC>
-__global__ void __launch_bounds__(kThreads) k_cg_B(int n, const T *__restrict__ aP, const T *__restrict__ p,
-                                                   const T *__restrict__ Ap, T *__restrict__ x, T *__restrict__ r,
-                                                   CgDev *cg, double *partials, unsigned int *counter) {
+__device__ __forceinline__ void cg_B_body(Blk B, int n, const T *__restrict__ aP, const T *__restrict__ p,
+                                          const T *__restrict__ Ap, T *__restrict__ x, T *__restrict__ r, CgDev *cg,
+                                          double *partials, unsigned int *counter) {
     const CgView cv = block_cg_view(cg);
     if (cv.done) return;
     using VT = Vec16<T>;
@@ -283,8 +301,8 @@ __global__ void __launch_bounds__(kThreads) k_cg_B(int n, const T *__restrict__ 
     const V *aPv = reinterpret_cast<const V *>(aP), *pv = reinterpret_cast<const V *>(p),
             *Apv = reinterpret_cast<const V *>(Ap);
     V *xv = reinterpret_cast<V *>(x), *rv = reinterpret_cast<V *>(r);
-    const int stride = gridDim.x * blockDim.x;
-    for (int base = blockIdx.x * blockDim.x + threadIdx.x; base < nv; base += stride * kUnrollB) {
+    const int stride = B.n * blockDim.x;
+    for (int base = B.id * blockDim.x + threadIdx.x; base < nv; base += stride * kUnrollB) {
         V X[kUnrollB], P[kUnrollB], R[kUnrollB], AP[kUnrollB], D[kUnrollB];
 #pragma unroll
         for (int u = 0; u < kUnrollB; u++) {
@@ -318,7 +336,7 @@ __global__ void __launch_bounds__(kThreads) k_cg_B(int n, const T *__restrict__ 
             }
         }
     }
-    for (int i = nv * W + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    for (int i = nv * W + B.id * blockDim.x + threadIdx.x; i < n; i += stride) {
         T xi = x[i] + alpha * p[i];
         T ri = r[i] + (-alpha) * Ap[i];
         x[i] = xi;
@@ -331,14 +349,23 @@ __global__ void __launch_bounds__(kThreads) k_cg_B(int n, const T *__restrict__ 
     }
     if (JAC) {
         double red[2] = {rz, rr}, out[2];
-        if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) cg_iter_finish(cg, out[0], out[1]);
+        if (grid_reduce<2, false>(B, red, partials, counter, out) && threadIdx.x == 0)
+            cg_iter_finish(cg, out[0], out[1]);
     }
 }
 
-// h = x + h (Krylov adds the warm start back at the end; then s.h .= x).
-__global__ void k_cg_finish(int n, const double *x, double *h) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) h[i] = x[i] + h[i];
+template <typename T, bool JAC>
+__global__ void __launch_bounds__(kThreads) k_cg_B(int n, const T *__restrict__ aP, const T *__restrict__ p,
+                                                   const T *__restrict__ Ap, T *__restrict__ x, T *__restrict__ r,
+                                                   CgDev *cg, double *partials, unsigned int *counter) {
+    cg_B_body<T, JAC>(grid_blk(), n, aP, p, Ap, x, r, cg, partials, counter);
 }
+
+// h = x + h (Krylov adds the warm start back at the end; then s.h .= x).
+__device__ __forceinline__ void cg_finish_body(Blk B, int n, const double *x, double *h) {
+    for (int i = B.id * blockDim.x + threadIdx.x; i < n; i += B.n * blockDim.x) h[i] = x[i] + h[i];
+}
+__global__ void k_cg_finish(int n, const double *x, double *h) { cg_finish_body(grid_blk(), n, x, h); }
 
 // ---------------------------------------------------------------------------------------------
 // Chebyshev preconditioner ldiv! (src/preconditioner.jl:239-267): y ~ A^-1 x by the degree-d
@@ -1136,7 +1163,122 @@ static int static_scratch_address(int device, void **out) {
     return SHK_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Ensemble CG: the Jacobi-PCG bodies over every instance in one grid.  Instances whose Picard loop
+// has finished, or whose CG has stopped, return at once.
+// ---------------------------------------------------------------------------------------------
+
+// Krylov state of a new solve for every instance still in its Picard loop (make_cg_init), and a
+// fresh trip count for the solve's loop.
+__global__ void k_ens_cg_reset(EnsInst *E, EnsCtl *ctl) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->cg_trips = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ctl->n; i += gridDim.x * blockDim.x) {
+        if (!E[i].pic_active) continue;
+        CgDev *g = E[i].cg;
+        memset(g, 0, sizeof(CgDev));
+        g->atol = ctl->atol;
+        g->rtol = ctl->rtol;
+        g->itmax = ctl->itmax > 0 ? ctl->itmax : 2LL * E[i].nx * E[i].ny;
+        g->stop_rule = ctl->stop_rule;
+        g->status = SHK_OK;
+        g->first = 1;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_ens_cg_init(EnsInst *E, const int *b2i) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_STENCIL);
+    if (!I.pic_active) return;
+    cg_init_body<double, true>(B, I.nx, I.ny, I.aP, I.aE, I.aN, I.st.h, I.rhs, I.r, I.x, I.cg, I.partials,
+                               I.counter);
+}
+
+__global__ void __launch_bounds__(kMarchX, 6) k_ens_cg_A(EnsInst *E, const int *b2i, int parity) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_MARCH);
+    if (!I.pic_active) return;
+    const double *p_old = parity ? I.p1 : I.p0;
+    double *p_new = parity ? I.p0 : I.p1;
+    cg_A_body<double, true, false>(B, I.nx, I.ny, I.march_th, I.aP, I.aE, I.aN, I.r, nullptr, p_old, p_new, I.Ap,
+                                   I.cg, I.partials, I.counter, DBL_EPSILON, nullptr);
+}
+
+__global__ void __launch_bounds__(kThreads) k_ens_cg_B(EnsInst *E, const int *b2i, int parity) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_STREAM);
+    if (!I.pic_active) return;
+    const double *p_new = parity ? I.p0 : I.p1;
+    cg_B_body<double, true>(B, I.nx * I.ny, I.aP, p_new, I.Ap, I.x, I.r, I.cg, I.partials, I.counter);
+}
+
+// h = x + h, then (one thread per instance, after the solve) the solve's statistics
+__global__ void __launch_bounds__(kThreads) k_ens_cg_finish(EnsInst *E, const int *b2i) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_FLAT);
+    if (!I.pic_active) return;
+    cg_finish_body(B, I.nx * I.ny, I.x, I.st.h);
+}
+__global__ void k_ens_cg_stats(EnsInst *E, const EnsCtl *ctl) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ctl->n; i += gridDim.x * blockDim.x) {
+        if (!E[i].pic_active) continue;
+        const CgDev *g = E[i].cg;
+        E[i].cg_iters += g->iter;
+        E[i].cg_solves += 1;
+        if (g->status == SHK_BREAKDOWN) E[i].cg_breakdowns += 1;
+    }
+}
+
+// Condition of the ensemble's CG loop (two iterations per trip): another trip while any instance
+// in its Picard loop has a CG still running, and never more than the largest itmax/2 + 8 trips.
+// Launched once before the loop as well: a conditional's default value is applied once per graph
+// launch, not each time a nested loop starts, so every solve sets its loop's condition itself.
+__global__ void k_ens_cg_cond(EnsInst *E, EnsCtl *ctl, cudaGraphConditionalHandle h) {
+    __shared__ int any;
+    __shared__ long long cap;
+    if (threadIdx.x == 0) {
+        any = 0;
+        cap = 0;
+    }
+    __syncthreads();
+    int mine = 0;
+    long long mcap = 0;
+    for (int i = threadIdx.x; i < ctl->n; i += blockDim.x) {
+        const CgDev *g = E[i].cg;
+        if (E[i].pic_active && !*(const volatile int *)&g->done) mine = 1;
+        mcap = mcap > g->itmax ? mcap : g->itmax;
+    }
+    if (mine) atomicOr(&any, 1);
+    atomicMax(reinterpret_cast<unsigned long long *>(&cap), (unsigned long long)mcap);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int t = ++ctl->cg_trips;
+        const bool more = any && 2LL * (long long)t < cap + 16;
+        cudaGraphSetConditional(h, more ? 1u : 0u);
+    }
+}
+
+void ens_cg_reset(cudaStream_t s, EnsInst *E, EnsCtl *ctl, int n) {
+    k_ens_cg_reset<<<(n + 255) / 256, 256, 0, s>>>(E, ctl);
+}
+void ens_cg_init(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks) {
+    k_ens_cg_init<<<nblocks, kThreads, 0, s>>>(E, b2i);
+}
+void ens_cg_A(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, int parity) {
+    k_ens_cg_A<<<nblocks, kMarchX, 0, s>>>(E, b2i, parity);
+}
+void ens_cg_B(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, int parity) {
+    k_ens_cg_B<<<nblocks, kThreads, 0, s>>>(E, b2i, parity);
+}
+void ens_cg_finish(cudaStream_t s, EnsInst *E, const EnsCtl *ctl, int n, const int *b2i, int nblocks) {
+    k_ens_cg_finish<<<nblocks, kThreads, 0, s>>>(E, b2i);
+    k_ens_cg_stats<<<(n + 255) / 256, 256, 0, s>>>(E, ctl);
+}
+void ens_cg_cond(cudaStream_t s, EnsInst *E, EnsCtl *ctl, int n, cudaGraphConditionalHandle h) {
+    k_ens_cg_cond<<<1, 256, 0, s>>>(E, ctl, h);
+}
+
 } // namespace shk
+
 
 extern "C" SHK_API int shk_cg_solve_static(int nx, int ny, const double *aP, const double *aE, const double *aN,
                                            const double *rhs, double *x, const shk_cg_opts *o, shk_cg_stats *st,

@@ -49,7 +49,7 @@ def test_struct_layouts_match_header(shk, tmp_path):
     structs = {"shk_params": _lib.shk_params, "shk_state": _lib.shk_state, "shk_cg_opts": _lib.shk_cg_opts,
                "shk_cg_stats": _lib.shk_cg_stats, "shk_picard_opts": _lib.shk_picard_opts,
                "shk_picard_stats": _lib.shk_picard_stats, "shk_melt_input": _lib.shk_melt_input,
-               "shk_sliding_law": _lib.shk_sliding_law}
+               "shk_sliding_law": _lib.shk_sliding_law, "shk_ensemble_stats": _lib.shk_ensemble_stats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
