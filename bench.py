@@ -59,6 +59,11 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--out", default=None, help="also write the JSON line here")
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="ensemble mode: this many instances of the ragged ensemble workload (sizes 128^2..1024^2); "
+                         "prints its own JSON line instead of the 4096^2 one")
+    ap.add_argument("--ens-sequential", type=int, default=32,
+                    help="ensemble mode: instances also run one after another through the single-instance path")
     ap.add_argument("--profile-cg", type=int, default=0,
                     help="profiling case: initialise the workload, assemble once and run exactly this many CG "
                          "iterations of each form, then exit")
@@ -560,10 +565,114 @@ def profile_cg(args):
     print(json.dumps({"profile_cg": out, "workload": w.name, "cells": w.nx * w.ny}))
 
 
+def ensemble_bench(args):
+    """Ragged ensemble: converged instance-timesteps/s of `args.ensemble` instances (sizes drawn
+    from 128^2..1024^2, per-instance slope, melt, C, b0) advanced together by shk.Ensemble, beside
+    the same instances advanced one after another through the single-instance path.  Both arms run
+    the same K timesteps from the instances' initial states (graph set-up and the tile autotune
+    are outside the timed region)."""
+    import torch
+    shk = entry.load_package()
+    specs = shk.configs.ensemble_specs(args.ensemble)
+    params = dict(shk.configs.SEASONAL_PARAMS)
+
+    def make(sp):
+        w = shk.configs.ensemble_member(**sp)
+        g = shk.Grid(w.nx, w.ny, w.lx, w.ly)
+        pm = shk.ModelParameters(**params)
+        sl = shk.RegularizedCoulombSlidingLaw(w.sliding_C)
+        st = shk.State(g)
+        shk.set_initial_conditions(st, g, pm, sl, **w.inputs)
+        ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, stop_rule="relres", rtol=1e-8, atol=0.0)
+        ps = shk.PicardSolver(500, 1e-6, ls, g)
+        return shk.Simulation(g, st, args.steps, args.dt, pm, "implicit", [], shk.ConstantMeltInput(), sl, ps=ps)
+
+    sims = [make(sp) for sp in specs]
+    cells = sum(s.grid.nx * s.grid.ny for s in sims)
+    t0 = time.perf_counter()
+    ens = shk.Ensemble(sims, autotune_iters=8)
+    setup_s = time.perf_counter() - t0
+    ens.run(0)  # builds the timestep graph outside the timed region
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    stats = ens.run(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    conv = sum(s["steps_converged"] for s in stats)
+    by_size = {}
+    for sp, th in zip(specs, ens.march_th):
+        by_size.setdefault(sp["nx"], th)
+    line = {"metric": "converged instance-timesteps/s, ragged ensemble (128^2..1024^2), rel-res 1e-8",
+            "value": round(conv / (ms / 1e3), 3), "unit": "instance-timesteps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": 0, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": f"ensemble of {len(sims)} instances, sizes "
+                                   f"{dict(sorted((k, sum(1 for s in specs if s['nx'] == k)) for k in by_size))}, "
+                                   f"{cells / 1e6:.1f} M cells in total",
+                       "form": "batched Float64 Jacobi CG, one launch per kernel over all instances, one CUDA graph "
+                               "per timestep (device-side Picard and CG loops)",
+                       "params": params, "picard": "500 iters, tol 1e-6", "dt_s": args.dt,
+                       "timing": "the same K steps from the initial states in both arms"},
+            "march_th_by_size": by_size, "setup_s": round(setup_s, 2),
+            "instance_steps": len(sims) * args.steps, "converged_instance_steps": conv,
+            "picard_iters": sum(s["picard_iters"] for s in stats), "cg_iters": sum(s["cg_iters"] for s in stats),
+            "clocks": clk}
+    ens.close()
+    del sims, ens
+    torch.cuda.empty_cache()
+    if args.ens_sequential:
+        # the same first M instances both ways: batched, and one after another
+        sub = specs[:args.ens_sequential]
+        ens_sims = [make(sp) for sp in sub]
+        sub_ens = shk.Ensemble(ens_sims, autotune_iters=8)
+        sub_ens.run(0)
+        torch.cuda.synchronize()
+        e0.record()
+        st2 = sub_ens.run(args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_ens = e0.elapsed_time(e1)
+        conv_ens = sum(x["steps_converged"] for x in st2)
+        sub_ens.close()
+        del ens_sims, sub_ens
+        seq = [make(sp) for sp in sub]
+        torch.cuda.synchronize()
+        e0.record()
+        done = 0
+        for sim in seq:
+            for _ in range(args.steps):
+                shk.step(sim)
+                sim.total_time += sim.dt
+                done += int(sim.hs.ps.converged)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_seq = e0.elapsed_time(e1)
+        line["same_instances_both_ways"] = {
+            "instances": len(sub), "cells": sum(x.grid.nx * x.grid.ny for x in seq),
+            "ensemble": {"value": round(conv_ens / (ms_ens / 1e3), 3), "ms": round(ms_ens, 1)},
+            "one_after_another": {"value": round(done / (ms_seq / 1e3), 3), "ms": round(ms_seq, 1)},
+            "unit": "instance-timesteps/s", "speedup": round(ms_seq / ms_ens, 2),
+            "note": "the first instances of the ensemble; one after another = the single-instance path "
+                    "(shk_step per instance, device-side CG loop per solve)"}
+    return line
+
+
 def main():
     args = parse()
     if args.profile_cg:
         return profile_cg(args)
+    if args.ensemble:
+        line = ensemble_bench(args)
+        s = json.dumps(line)
+        print(s, flush=True)
+        if args.out:
+            Path(args.out).write_text(s + "\n")
+        return
     world, rank, local, pg = dist_setup(args) if args.impl == "ours" else (
         int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0, None)
     try:

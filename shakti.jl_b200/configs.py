@@ -184,5 +184,38 @@ def seasonal1024() -> Workload:
     return seasonal_bench(1024, 50e3)
 
 
+def ensemble_member(nx: int, seed: int, slope: float, melt: float, C: float, b0: float) -> Workload:
+    """One instance of the ensemble workload: the plain generator at dx = 156.25 m (the 64x64 /
+    10 km spacing) with its own bed slope, constant melt (ieb, m/s), sliding coefficient C and
+    initial gap b0 (+-20 % seeded noise)."""
+    ny = nx
+    lx = ly = 156.25 * (nx - 1)
+    rng = np.random.default_rng(seed)
+    x = np.arange(nx) * (lx / (nx - 1))
+    X = np.repeat(x.reshape(nx, 1), ny, axis=1)
+    mask = np.full((nx, ny), GROUNDED, order="F")
+    mask[0, :] = OCEAN
+    zb = np.asfortranarray(slope * (lx - X) + rng.normal(0.0, 5.0, size=(ny, nx)).T)
+    zs = np.asfortranarray(zb + 6.0 * np.sqrt(X + 5000.0))
+    b = np.asfortranarray(b0 * (1.0 + rng.uniform(-0.2, 0.2, size=(ny, nx)).T))
+    inputs = dict(mask=mask, A_visc=np.full((nx, ny), A_VISC, order="F"), zb=zb, zs=zs, b=b,
+                  G=np.full((nx, ny), 0.05, order="F"),
+                  ub_x=np.full((nx + 1, ny), 30.0 / SECONDS_PER_YEAR, order="F"), ub_y=_zeros(nx, ny + 1),
+                  ieb=np.full((nx, ny), melt, order="F"), taub_x=_zeros(nx + 1, ny), taub_y=_zeros(nx, ny + 1))
+    return Workload(f"member{nx}", nx, ny, lx, ly, inputs, sliding_C=C, seed=seed)
+
+
+def ensemble_specs(n: int = 256, seed: int = 20263, sizes=(128, 256, 512, 1024)) -> list[dict]:
+    """The ragged ensemble: n instances, sizes drawn uniformly from `sizes`; per-instance bed slope
+    U(0.005, 0.02), melt U(1e-9, 1e-7) m/s, C U(5e3, 5e4), initial gap U(0.001, 0.01) m."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        out.append(dict(nx=int(rng.choice(sizes)), seed=seed + 1 + k, slope=float(rng.uniform(0.005, 0.02)),
+                        melt=float(rng.uniform(1e-9, 1e-7)), C=float(rng.uniform(5e3, 5e4)),
+                        b0=float(rng.uniform(0.001, 0.01))))
+    return out
+
+
 WORKLOADS = {"fixture6": fixture6, "plain64": plain64, "plain1024": plain1024, "seasonal1024": seasonal1024, "seasonal2048": seasonal2048,
              "seasonal4096": seasonal4096}
