@@ -64,6 +64,13 @@ def parse():
                          "prints its own JSON line instead of the 4096^2 one")
     ap.add_argument("--ens-sequential", type=int, default=32,
                     help="ensemble mode: instances also run one after another through the single-instance path")
+    ap.add_argument("--warmstart", action="store_true",
+                    help="learned-warm-start mode: generate first-Picard-iterate pairs from an ensemble run, train "
+                         "the network with the library's kernels, and compare seeded and unseeded timesteps on a "
+                         "2048^2 instance; prints its own JSON line")
+    ap.add_argument("--ws-instances", type=int, default=96)
+    ap.add_argument("--ws-steps", type=int, default=48)
+    ap.add_argument("--ws-train", type=int, default=4000)
     ap.add_argument("--profile-cg", type=int, default=0,
                     help="profiling case: initialise the workload, assemble once and run exactly this many CG "
                          "iterations of each form, then exit")
@@ -662,8 +669,76 @@ def ensemble_bench(args):
     return line
 
 
+def warmstart_bench(args):
+    """Learned warm start: training pairs (first Picard iterate increments) from an ensemble run of
+    the plain solver on 128^2 instances, training by the library's BF16 tensor-core kernels, then
+    the same 2048^2 instance advanced seeded and unseeded with the multigrid-preconditioned Float64
+    CG at rel-res 1e-8: CG and Picard iterations per step, device time per step, and the seeded
+    head's error against the unseeded one."""
+    import numpy as np
+    import torch
+    shk = entry.load_package()
+    from shakti_b200 import warmstart as ws
+    t0 = time.perf_counter()
+    net = ws.WarmStartNet(seed=0)
+    specs = shk.configs.ensemble_specs(args.ws_instances, seed=99, sizes=(128,))
+    X, T, M = ws.generate_pairs(shk, net, specs, steps=args.ws_steps, crops=8)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    losses = []
+    per = max(1, args.ws_train // 4)
+    for lr in (1e-3, 5e-4, 2.5e-4, 1e-4):
+        losses += net.train(X, T, M, steps=per, batch=64, lr=lr)
+    e1.record()
+    torch.cuda.synchronize()
+    train_ms = e0.elapsed_time(e1)
+    spec = dict(nx=2048, seed=556, slope=0.018, melt=8e-8, C=4e4, b0=0.007)
+    sim = ws.member_sim(shk, spec, multigrid=True)
+    Xp = net.pack(sim.state)
+    net.forward(Xp)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(5):
+        net.forward(Xp)
+    e1.record()
+    torch.cuda.synchronize()
+    infer_ms = e0.elapsed_time(e1) / 5
+    del sim
+    ev = ws.evaluate(shk, net, spec, steps=args.steps, settle=2, multigrid=True)
+    line = {"metric": "learned warm start at 2048^2: CG iterations and time per converged timestep, seeded vs "
+                      "unseeded (rel-res 1e-8)",
+            "value": round(ev["seeded"]["cg_per_step"], 2), "unit": "CG iterations/step (seeded)",
+            "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": 2,
+            "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": "ensemble member at 2048x2048 (dx 156 m), multigrid-preconditioned Float64 CG",
+                       "network": "4-level conv encoder-decoder, 32 base channels, BF16 weights/activations, "
+                                  "Float32 accumulation (mma.sync m16n8k16)",
+                       "training": f"{X.shape[0]} pairs of 32x32 crops from {len(specs)} 128^2 instances x "
+                                   f"{args.ws_steps} steps, {len(losses)} Adam steps of batch 64"},
+            "unseeded": {k: ev["unseeded"][k] for k in ("cg_per_step", "picard_per_step", "ms_per_step")},
+            "seeded": {k: ev["seeded"][k] for k in ("cg_per_step", "picard_per_step", "ms_per_step")},
+            "seed_accepted": ev["seeded"]["seed"]["seeded"],
+            "initial_residual_ratio": [round(b / a, 3) for a, b in zip(ev["seeded"]["seed"]["r_prev"],
+                                                                        ev["seeded"]["seed"]["r_seed"])],
+            "h_relerr_vs_unseeded": ev["h_relerr_vs_unseeded"],
+            "training": {"pairs": int(X.shape[0]), "data_s": round(gen_s, 1), "train_ms": round(train_ms, 1),
+                         "loss_first": round(float(np.mean(losses[:50])), 4),
+                         "loss_last": round(float(np.mean(losses[-200:])), 4)},
+            "inference_ms_2048": round(infer_ms, 3)}
+    return line
+
+
 def main():
     args = parse()
+    if args.warmstart:
+        line = warmstart_bench(args)
+        s = json.dumps(line)
+        print(s, flush=True)
+        if args.out:
+            Path(args.out).write_text(s + "\n")
+        return
     if args.profile_cg:
         return profile_cg(args)
     if args.ensemble:

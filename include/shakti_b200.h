@@ -263,9 +263,77 @@ SHK_API int shk_ensemble_autotune(void *ens, int iters, int *th_out);
  * may be NULL.  Returns SHK_NOT_CONVERGED if any instance's Picard loop did not converge. */
 SHK_API int shk_ensemble_run(void *ens, double dt, int tsteps, const shk_picard_opts *po,
                              const shk_cg_opts *o, shk_ensemble_stats *per_instance);
+/* Per-instance device buffers (n pointers, nx*ny doubles each; NULL entries: none) that receive h
+ * after each timestep's first Picard iteration (training data for the learned warm start). */
+SHK_API int shk_ensemble_set_snapshots(void *ens, double *const *bufs);
 /* Blocks per launch of each batched kernel family (stencil, row-marching, streaming, flat). */
 SHK_API int shk_ensemble_launch_counts(const void *ens, int *stencil, int *march, int *stream,
                                        int *flat);
+
+/* ---------------------------------------------------------------------------------------------
+ * Learned warm start: BF16 tensor-core kernels of a small convolutional encoder-decoder that
+ * predicts the head increment of the coming timestep.  No counterpart in the reference, which
+ * seeds each solve with the current head (cg! x0 = vec(h), src/linear_solver.jl:876-881); the
+ * prediction only seeds Picard/CG, which still converge to their tolerances.
+ *
+ * Tensors are device pointers in NHWC order (channels innermost).  BF16 tensors are passed as
+ * void*; Float32 tensors as float*.  Weights: [9][Cout][Cin] (3x3 taps row-major), BF16 for the
+ * tensor cores, Float32 master copies for the optimiser.  stream may be NULL.
+ * --------------------------------------------------------------------------------------------- */
+/* Y = act(conv3x3(X, W) + bias) with zero padding; Y (BF16) and/or Yf (Float32) may be NULL.
+ * Cin % 16 == 0, Cout % 8 == 0.  flip = 1 negates the tap offsets: with the per-tap transposed
+ * weights [9][Cin][Cout] this is the input gradient of the forward convolution. */
+SHK_API int shk_nn_conv3x3(const void *X, const void *Wt, const float *bias, void *Y, float *Yf, int N,
+                           int H, int W, int Cin, int Cout, int relu, int flip, void *stream);
+/* dW[tap][co][ci] += sum_p dY[p][co] X[p + off(tap)][ci]   (Cout % 16 == 0, Cin % 8 == 0) */
+SHK_API int shk_nn_conv3x3_wgrad(const void *X, const void *dY, float *dW, int N, int H, int W, int Cin,
+                                 int Cout, void *stream);
+/* dYm = dY * (Y > 0) (relu = 0: dY) as BF16; db[c] += sum over the P pixels (db may be NULL) */
+SHK_API int shk_nn_relu_grad(const float *dY, const void *Y, void *dYm, float *db, long long P, int C,
+                             int relu, void *stream);
+/* 2x2 average pooling (H, W: input size) and its gradient (acc = 1 adds into dX) */
+SHK_API int shk_nn_pool2(const void *X, void *Y, int N, int H, int W, int C, void *stream);
+SHK_API int shk_nn_pool2_grad(const float *dY, float *dX, int N, int H, int W, int C, int acc,
+                              void *stream);
+/* Y = nearest 2x upsampling of X plus S (S may be NULL; H, W: output size), and the upsampling's
+ * gradient (H, W: the coarse size) */
+SHK_API int shk_nn_up2_add(const void *X, const void *S, void *Y, int N, int H, int W, int C,
+                           void *stream);
+SHK_API int shk_nn_up2_grad(const float *dY, float *dX, int N, int H, int W, int C, void *stream);
+/* y = x (acc = 0) or y += x (acc = 1), Float32 */
+SHK_API int shk_nn_axpy(const float *x, float *y, long long n, int acc, void *stream);
+/* mean squared error of channel 0 of Yf (C channels per pixel) against T (weights wgt, may be
+ * NULL); writes the gradient dY and adds the loss (already scaled by inv_count) to *loss */
+SHK_API int shk_nn_mse(const float *Yf, const float *T, const float *wgt, float *dY, float *loss,
+                       long long P, int C, float inv_count, void *stream);
+/* one Adam step (bias-corrected at `step` >= 1) on Float32 weights w with gradient g; refreshes the
+ * BF16 copy wb and the per-tap transposed copy wt when given (both may be NULL) */
+SHK_API int shk_nn_adam(float *w, const float *g, float *m, float *v, void *wb, void *wt, long long n,
+                        int Cout, int Cin, float lr, float b1, float b2, float eps, int step,
+                        void *stream);
+SHK_API int shk_nn_wcast(const float *w, void *wb, void *wt, long long n, int Cout, int Cin,
+                         void *stream);
+SHK_API int shk_nn_zero(float *p, long long n, void *stream);
+/* the network input from a State: channels h, b, N, zb, zs, ieb, mask as (v - norm[2c]) *
+ * norm[2c+1] (norm: 14 floats on the device), zero-padded to 16 channels and Hp x Wp pixels */
+SHK_API int shk_nn_pack_state(const shk_state *st, int nx, int ny, int Hp, int Wp, const float *norm,
+                              void *X, void *stream);
+/* out = h + dh_scale * Yf[channel 0] on GROUNDED cells (mask 0), h elsewhere */
+SHK_API int shk_nn_apply_increment(const float *Yf, int C, int nx, int ny, int Wp, double dh_scale,
+                                   const double *h, const double *mask, double *out, void *stream);
+/* ||rhs - A h||_2 and ||rhs||_2 of the elliptic system assembled at the context's current h (the
+ * initial residual a Picard iteration would start from); assembles into the context's workspace. */
+SHK_API int shk_initial_residual(void *ctx, double *rnorm, double *bnorm);
+/* ||rhs - A x||_2 (and ||rhs||_2) of the system last assembled in the context, for a device vector x
+ * of nx*ny doubles. */
+SHK_API int shk_residual_of(void *ctx, const double *x, double *rnorm, double *bnorm);
+/* `sweeps` damped Jacobi sweeps x <- x + omega (rhs - A x) / aP on the system last assembled in the
+ * context (x and tmp: nx*ny doubles, device): removes the rough part of an initial guess's error. */
+SHK_API int shk_smooth_guess(void *ctx, double *x, double *tmp, int sweeps, double omega);
+/* A one-shot initial guess (nx*ny doubles, device, caller-owned until the solve) for the next
+ * Float64 CG solve of the context in place of the current head (cg! x0, src/linear_solver.jl:
+ * 876-881); the solve's result still replaces h.  NULL clears it. */
+SHK_API int shk_set_cg_warm_start(void *ctx, const double *x0);
 
 /* ---------------------------------------------------------------------------------------------
  * Allocation-free solve.  No counterpart in the reference: it exists for callers that cannot

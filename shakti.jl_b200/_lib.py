@@ -72,6 +72,7 @@ class shk_ensemble_stats(C.Structure):
 
 # Every symbol include/shakti_b200.h declares, with (restype, argtypes).
 VP = C.c_void_p
+FP = C.POINTER(C.c_float)
 SIGNATURES = {
     "shk_version": (C.c_int, []),
     "shk_status_string": (C.c_char_p, [C.c_int]),
@@ -108,8 +109,29 @@ SIGNATURES = {
     "shk_kernel_launches": (C.c_long, [VP]),
     "shk_cg_solve_static": (C.c_int, [C.c_int, C.c_int, VP, VP, VP, VP, VP, C.POINTER(shk_cg_opts),
                                       C.POINTER(shk_cg_stats), VP]),
+    "shk_nn_conv3x3": (C.c_int, [VP, VP, FP, VP, FP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                 C.c_int, VP]),
+    "shk_nn_conv3x3_wgrad": (C.c_int, [VP, VP, FP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, VP]),
+    "shk_nn_relu_grad": (C.c_int, [FP, VP, VP, FP, C.c_longlong, C.c_int, C.c_int, VP]),
+    "shk_nn_pool2": (C.c_int, [VP, VP, C.c_int, C.c_int, C.c_int, C.c_int, VP]),
+    "shk_nn_pool2_grad": (C.c_int, [FP, FP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, VP]),
+    "shk_nn_up2_add": (C.c_int, [VP, VP, VP, C.c_int, C.c_int, C.c_int, C.c_int, VP]),
+    "shk_nn_up2_grad": (C.c_int, [FP, FP, C.c_int, C.c_int, C.c_int, C.c_int, VP]),
+    "shk_nn_axpy": (C.c_int, [FP, FP, C.c_longlong, C.c_int, VP]),
+    "shk_nn_mse": (C.c_int, [FP, FP, FP, FP, FP, C.c_longlong, C.c_int, C.c_float, VP]),
+    "shk_nn_adam": (C.c_int, [FP, FP, FP, FP, VP, VP, C.c_longlong, C.c_int, C.c_int, C.c_float, C.c_float,
+                              C.c_float, C.c_float, C.c_int, VP]),
+    "shk_nn_wcast": (C.c_int, [FP, VP, VP, C.c_longlong, C.c_int, C.c_int, VP]),
+    "shk_nn_zero": (C.c_int, [FP, C.c_longlong, VP]),
+    "shk_nn_pack_state": (C.c_int, [C.POINTER(shk_state), C.c_int, C.c_int, C.c_int, C.c_int, FP, VP, VP]),
+    "shk_nn_apply_increment": (C.c_int, [FP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, VP, VP, VP, VP]),
+    "shk_initial_residual": (C.c_int, [VP, DP, DP]),
+    "shk_residual_of": (C.c_int, [VP, VP, DP, DP]),
+    "shk_smooth_guess": (C.c_int, [VP, VP, VP, C.c_int, C.c_double]),
+    "shk_set_cg_warm_start": (C.c_int, [VP, VP]),
     "shk_ensemble_create": (C.c_int, [C.c_int, C.POINTER(VP), VP, C.POINTER(VP)]),
     "shk_ensemble_destroy": (C.c_int, [VP]),
+    "shk_ensemble_set_snapshots": (C.c_int, [VP, C.POINTER(VP)]),
     "shk_ensemble_last_error": (C.c_char_p, [VP]),
     "shk_ensemble_autotune": (C.c_int, [VP, C.c_int, C.POINTER(C.c_int)]),
     "shk_ensemble_run": (C.c_int, [VP, C.c_double, C.c_int, C.POINTER(shk_picard_opts), C.POINTER(shk_cg_opts),

@@ -16,7 +16,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libshakti_b200.so"
-SOURCES = ["shk_api.cu", "shk_fields.cu", "shk_krylov.cu", "shk_mg.cu", "shk_ensemble.cu"]
+SOURCES = ["shk_api.cu", "shk_fields.cu", "shk_krylov.cu", "shk_mg.cu", "shk_ensemble.cu", "shk_nn.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

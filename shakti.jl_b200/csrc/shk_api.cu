@@ -507,6 +507,41 @@ SHK_API int shk_picard_solve(void *ctx, const shk_picard_opts *po, const shk_cg_
     return status;
 }
 
+SHK_API int shk_initial_residual(void *ctx, double *rnorm, double *bnorm) {
+    Ctx *c = as_ctx(ctx);
+    REQUIRE_CTX(c);
+    int rc = require_ready(c);
+    if (rc) return rc;
+    if (!c->initialized && (rc = build_mask8(c))) return rc;
+    if ((rc = launch_assemble(c, 0, 0.0, false))) return rc;
+    c->assembled = true;
+    c->assembled_parabolic = false;
+    return residual_norms(c, nullptr, rnorm, bnorm);
+}
+
+SHK_API int shk_residual_of(void *ctx, const double *x, double *rnorm, double *bnorm) {
+    Ctx *c = as_ctx(ctx);
+    REQUIRE_CTX(c);
+    if (!x) return fail(c, SHK_BAD_ARG, "null vector");
+    if (!c->assembled) return fail(c, SHK_NOT_BOUND, "no assembled system: call shk_assemble or shk_initial_residual");
+    return residual_norms(c, x, rnorm, bnorm);
+}
+
+SHK_API int shk_smooth_guess(void *ctx, double *x, double *tmp, int sweeps, double omega) {
+    Ctx *c = as_ctx(ctx);
+    REQUIRE_CTX(c);
+    if (!x || !tmp || sweeps < 0) return fail(c, SHK_BAD_ARG, "bad smoothing arguments");
+    if (!c->assembled) return fail(c, SHK_NOT_BOUND, "no assembled system: call shk_assemble or shk_initial_residual");
+    return jacobi_smooth(c, x, tmp, sweeps, omega);
+}
+
+SHK_API int shk_set_cg_warm_start(void *ctx, const double *x0) {
+    Ctx *c = as_ctx(ctx);
+    REQUIRE_CTX(c);
+    c->ws_x0 = x0;
+    return SHK_OK;
+}
+
 // parabolic_solver! (src/parabolic_solver.jl:16-38)
 SHK_API int shk_parabolic_step(void *ctx, double dt, const shk_cg_opts *o, shk_cg_stats *st) {
     Ctx *c = as_ctx(ctx);

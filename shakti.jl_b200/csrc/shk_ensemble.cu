@@ -85,6 +85,17 @@ __global__ void k_ens_picard_cond(EnsInst *E, EnsCtl *ctl, cudaGraphConditionalH
     }
 }
 
+// After the first Picard iteration of the timestep (before its Picard test), a copy of h for the
+// instances that asked for one: the first Picard iterate, the learned warm start's target.
+__global__ void __launch_bounds__(kThreads) k_ens_snapshot(EnsInst *E, const int *b2i) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_FLAT);
+    if (!I.pic_active || !I.snap || I.pic_iter != 0) return;
+    const long long n = (long long)I.nx * I.ny;
+    for (long long i = (long long)B.id * blockDim.x + threadIdx.x; i < n; i += (long long)B.n * blockDim.x)
+        I.snap[i] = I.st.h[i];
+}
+
 struct Ens {
     int n = 0, device = 0;
     std::vector<Ctx *> ctx;
@@ -217,6 +228,7 @@ static int ens_build_graph(Ens *e) {
             r = add_while(e->cap[1], h2, &body2);
         }
         ens_cg_finish(e->cap[1], E, C, e->n, e->b2i[EF_FLAT], e->nb[EF_FLAT]);
+        k_ens_snapshot<<<e->nb[EF_FLAT], kThreads, 0, e->cap[1]>>>(E, e->b2i[EF_FLAT]);
         ens_tail(e->cap[1], E, e->b2i[EF_TAIL], e->nb[EF_TAIL]);
         k_ens_picard_cond<<<1, 256, 0, e->cap[1]>>>(E, C, h1);
         cudaGraph_t g = nullptr;
@@ -477,6 +489,20 @@ SHK_API int shk_ensemble_run(void *ens, double dt, int tsteps, const shk_picard_
         }
     }
     return status;
+}
+
+// Per-instance buffers (nx*ny doubles, device; NULL entries: none) that receive h after each
+// timestep's first Picard iteration.
+SHK_API int shk_ensemble_set_snapshots(void *ens, double *const *bufs) {
+    Ens *e = reinterpret_cast<Ens *>(ens);
+    if (!e) return SHK_BAD_ARG;
+    for (int i = 0; i < e->n; i++) {
+        e->hE[i].snap = bufs ? bufs[i] : nullptr;
+        int rc = echeck(e, cudaMemcpy(&e->dE[i].snap, &e->hE[i].snap, sizeof(double *), cudaMemcpyHostToDevice),
+                        "set snapshots");
+        if (rc) return rc;
+    }
+    return SHK_OK;
 }
 
 SHK_API int shk_ensemble_launch_counts(const void *ens, int *stencil, int *march, int *stream, int *flat) {

@@ -152,6 +152,7 @@ struct Ctx {
     std::string err;
     bool assembled = false;
     bool assembled_parabolic = false;
+    const double *ws_x0 = nullptr;  // one-shot CG warm start for the next Float64 solve (caller-owned)
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -176,6 +177,7 @@ struct alignas(8) EnsInst {
     unsigned int *counter;
     CgDev *cg;
     PicDev *pic;
+    double *snap;  // optional copy of h after each timestep's first Picard iteration
     // loop control and statistics, written on the device
     int pic_active, pic_iter, pic_converged, cg_breakdowns;
     long long cg_iters, cg_solves;
@@ -217,6 +219,8 @@ int cheb_set_bounds(Ctx *c, double lmin, double lmax);
 int launch_chebyshev_apply_standalone(Ctx *c, int degree, const double *x, double *y);
 int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st);
 int read_scalars(Ctx *c);
+int residual_norms(Ctx *c, const double *x, double *rnorm, double *bnorm);
+int jacobi_smooth(Ctx *c, double *x, double *tmp, int sweeps, double omega);
 
 // ensemble kernels: shk_fields.cu
 void ens_assemble(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks);

@@ -366,6 +366,61 @@ __device__ __forceinline__ void cg_finish_body(Blk B, int n, const double *x, do
     for (int i = B.id * blockDim.x + threadIdx.x; i < n; i += B.n * blockDim.x) h[i] = x[i] + h[i];
 }
 __global__ void k_cg_finish(int n, const double *x, double *h) { cg_finish_body(grid_blk(), n, x, h); }
+// h = x + x0 for a warm start x0 other than h
+__global__ void k_cg_finish_from(int n, const double *x, const double *x0, double *h) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) h[i] = x[i] + x0[i];
+}
+
+// One damped Jacobi sweep on the assembled system: xo = xi + omega (b - A xi) / aP
+__global__ void __launch_bounds__(kThreads) k_jacobi_sweep(int nx, int ny, const double *aP, const double *aE,
+                                                           const double *aN, const double *b, const double *xi,
+                                                           double *xo, double omega) {
+    Tiles Tl(nx, ny);
+    for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
+        int ix, iy;
+        Tl.cell(t, ix, iy);
+        if (ix >= nx || iy >= ny) continue;
+        size_t c = (size_t)ix + (size_t)iy * nx;
+        double ax = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, xi[c], [&](size_t k) { return xi[k]; });
+        xo[c] = xi[c] + omega * (b[c] - ax) / aP[c];
+    }
+}
+
+int jacobi_smooth(Ctx *c, double *x, double *tmp, int sweeps, double omega) {
+    for (int k = 0; k < sweeps; k++) {
+        const double *xi = (k & 1) ? tmp : x;
+        double *xo = (k & 1) ? x : tmp;
+        k_jacobi_sweep<<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->aP, c->aE, c->aN, c->rhs, xi, xo,
+                                                                    omega);
+        c->launches++;
+    }
+    if (sweeps & 1)
+        cudaMemcpyAsync(x, tmp, (size_t)c->nx * c->ny * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    return check_launch(c, "jacobi smoothing");
+}
+
+// ||rhs - A x||^2 and ||rhs||^2 of the assembled system for a given x (Float64)
+__global__ void __launch_bounds__(kThreads) k_residual_of(int nx, int ny, const double *aP, const double *aE,
+                                                          const double *aN, const double *x, const double *b,
+                                                          DevScalars *dv, double *partials, unsigned int *counter) {
+    Tiles Tl(nx, ny);
+    double red[2] = {0.0, 0.0};
+    for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
+        int ix, iy;
+        Tl.cell(t, ix, iy);
+        if (ix >= nx || iy >= ny) continue;
+        size_t c = (size_t)ix + (size_t)iy * nx;
+        double ax = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, x[c], [&](size_t k) { return x[k]; });
+        double rc = b[c] - ax;
+        red[0] += rc * rc;
+        red[1] += b[c] * b[c];
+    }
+    double out[2];
+    if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
+        dv->ref_rr = out[0];
+        dv->ref_bb = out[1];
+    }
+}
 
 // ---------------------------------------------------------------------------------------------
 // Chebyshev preconditioner ldiv! (src/preconditioner.jl:239-267): y ~ A^-1 x by the degree-d
@@ -645,6 +700,19 @@ static int stream_grid(Ctx *c, long long n, size_t elem) {
     if (b > cap) b = cap;
     if (b < 1) b = 1;
     return (int)b;
+}
+
+// ||rhs - A x||_2 and ||rhs||_2 of the assembled system (x: the current h when null; Float64).
+int residual_norms(Ctx *c, const double *x, double *rnorm, double *bnorm) {
+    k_residual_of<<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->aP, c->aE, c->aN, x ? x : c->st.h,
+                                                              c->rhs, c->dev, c->partials, c->counter);
+    c->launches++;
+    int rc = check_launch(c, "residual norm");
+    if (rc) return rc;
+    if ((rc = read_scalars(c))) return rc;
+    if (rnorm) *rnorm = sqrt(c->host_dev->ref_rr);
+    if (bnorm) *bnorm = sqrt(c->host_dev->ref_bb);
+    return SHK_OK;
 }
 
 int read_scalars(Ctx *c) {
@@ -966,6 +1034,8 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
 
 int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
     const int nx = c->nx, ny = c->ny, n = nx * ny;
+    const double *ws = c->ws_x0;  // consumed by this solve (Float64 forms; ignored by the mixed form)
+    c->ws_x0 = nullptr;
     if (o->precond != SHK_PRECOND_JACOBI && o->precond != SHK_PRECOND_CHEBYSHEV && o->precond != SHK_PRECOND_MULTIGRID)
         return fail(c, SHK_BAD_ARG, "unknown preconditioner");
     if (o->precond == SHK_PRECOND_MULTIGRID) {
@@ -989,10 +1059,15 @@ int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
         CgDev *cgh = &c->host_dev->cg;
         *cgh = make_cg_init(o, n, false, 0.0);
         long it = 0;
-        int rc = cg_core<double>(c, o, &c->dev->cg, cgh, c->aP, c->aE, c->aN, c->st.h, c->rhs, c->x, c->r, c->z, c->p,
+        // warm start: the head, or a one-shot caller-provided guess (shk_set_cg_warm_start)
+        const double *x0 = ws ? ws : c->st.h;
+        int rc = cg_core<double>(c, o, &c->dev->cg, cgh, c->aP, c->aE, c->aN, x0, c->rhs, c->x, c->r, c->z, c->p,
                                  c->Ap, c->cr, c->cp, &it);
         if (rc) return rc;
-        k_cg_finish<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->x, c->st.h);
+        if (x0 == c->st.h)
+            k_cg_finish<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->x, c->st.h);
+        else
+            k_cg_finish_from<<<flat_grid(c, n), kThreads, 0, c->stream>>>(n, c->x, x0, c->st.h);
         c->launches++;
         if ((rc = check_launch(c, "cg finish"))) return rc;
         if ((rc = read_scalars(c))) return rc;

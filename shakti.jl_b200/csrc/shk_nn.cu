@@ -1,0 +1,463 @@
+// shk_nn.cu -- BF16 tensor-core kernels of the learned warm start (training and inference).
+//
+// No counterpart in the reference: the reference warm-starts each solve from the current head
+// (cg! x0 = vec(h), src/linear_solver.jl:876-881).  Here a small convolutional encoder-decoder
+// predicts the head increment of the coming timestep from the state; the prediction only seeds
+// Picard/CG (the solve still runs to its tolerance) and is dropped when its initial residual is
+// worse than the previous head's.
+//
+// Tensors are NHWC (channels innermost): activations BF16, gradients Float32, weights BF16 for the
+// tensor cores with a Float32 master copy for the optimiser.  A 3x3 convolution is an implicit
+// GEMM on mma.sync m16n8k16 (BF16 inputs, Float32 accumulation):
+//   forward      Y[p, co]  = sum_{tap, ci} X[p + off(tap), ci] W[tap, co, ci]        (+ bias, ReLU)
+//   input grad   dX[p, ci] = sum_{tap, co} dY[p - off(tap), co] W[tap, co, ci]       (the forward
+//                kernel on the per-tap transposed weights with the offsets negated)
+//   weight grad  dW[tap, co, ci] = sum_p dY[p, co] X[p + off(tap), ci]                (split over
+//                pixel chunks, Float32 atomics)
+// with zero padding at each image's border.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/shakti_b200.h"
+
+namespace shk {
+namespace nn {
+
+typedef __nv_bfloat16 bf16;
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ uint32_t ld_pair(const bf16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
+__device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// ---------------------------------------------------------------------------------------------
+// 3x3 convolution, forward form.  One block: 64 consecutive pixels (flattened n, y, x) x NT output
+// channels; warp w owns pixels 16w..16w+15 of the block.  Lane (g = lane/4, t = lane%4) holds the
+// A fragment rows g, g+8 (pixels) and columns 2t, 2t+1, 2t+8, 2t+9 (input channels), and the B
+// fragment column g (output channel) rows 2t, 2t+1, 2t+8, 2t+9.  FLIP negates the tap offsets (the
+// input-gradient form).  Cin % 16 == 0, Cout % NT == 0.
+// ---------------------------------------------------------------------------------------------
+template <int NT>
+__global__ void __launch_bounds__(128) k_conv3x3(const bf16 *__restrict__ X, const bf16 *__restrict__ Wt,
+                                                 const float *__restrict__ bias, bf16 *__restrict__ Y,
+                                                 float *__restrict__ Yf, int N, int H, int W, int Cin, int Cout,
+                                                 int relu, int flip) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const long long P = (long long)N * H * W;
+    const long long p0 = (long long)blockIdx.x * 64 + warp * 16;
+    const int co0 = blockIdx.y * NT;
+    const long long r0 = p0 + g, r1 = p0 + g + 8;
+    int n0 = 0, y0 = 0, x0 = 0, n1 = 0, y1 = 0, x1 = 0;
+    const bool v0 = r0 < P, v1 = r1 < P;
+    if (v0) { n0 = (int)(r0 / ((long long)H * W)); const int q = (int)(r0 % ((long long)H * W)); y0 = q / W; x0 = q % W; }
+    if (v1) { n1 = (int)(r1 / ((long long)H * W)); const int q = (int)(r1 % ((long long)H * W)); y1 = q / W; x1 = q % W; }
+    float acc[NT / 8][4];
+#pragma unroll
+    for (int j = 0; j < NT / 8; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+    for (int tap = 0; tap < 9; tap++) {
+        int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        if (flip) { dy = -dy; dx = -dx; }
+        const int sy0 = y0 + dy, sx0 = x0 + dx, sy1 = y1 + dy, sx1 = x1 + dx;
+        const bool ok0 = v0 && sy0 >= 0 && sy0 < H && sx0 >= 0 && sx0 < W;
+        const bool ok1 = v1 && sy1 >= 0 && sy1 < H && sx1 >= 0 && sx1 < W;
+        const bf16 *a0p = X + (((long long)n0 * H + (ok0 ? sy0 : 0)) * W + (ok0 ? sx0 : 0)) * Cin + 2 * t;
+        const bf16 *a1p = X + (((long long)n1 * H + (ok1 ? sy1 : 0)) * W + (ok1 ? sx1 : 0)) * Cin + 2 * t;
+        const bf16 *bp = Wt + ((long long)tap * Cout + co0 + g) * Cin + 2 * t;
+        for (int c = 0; c < Cin; c += 16) {
+            uint32_t a[4];
+            a[0] = ok0 ? ld_pair(a0p + c) : 0u;
+            a[1] = ok1 ? ld_pair(a1p + c) : 0u;
+            a[2] = ok0 ? ld_pair(a0p + c + 8) : 0u;
+            a[3] = ok1 ? ld_pair(a1p + c + 8) : 0u;
+#pragma unroll
+            for (int j = 0; j < NT / 8; j++) {
+                const bf16 *q = bp + (long long)j * 8 * Cin + c;
+                uint32_t b[2] = {ld_pair(q), ld_pair(q + 8)};
+                mma_bf16(acc[j], a, b);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NT / 8; j++) {
+        const int co = co0 + j * 8 + 2 * t;
+        const float b0 = bias ? bias[co] : 0.0f, b1 = bias ? bias[co + 1] : 0.0f;
+        float o[4] = {acc[j][0] + b0, acc[j][1] + b1, acc[j][2] + b0, acc[j][3] + b1};
+        if (relu)
+#pragma unroll
+            for (int k = 0; k < 4; k++) o[k] = o[k] > 0.0f ? o[k] : 0.0f;
+        if (v0) {
+            if (Y) *reinterpret_cast<uint32_t *>(Y + r0 * Cout + co) = pack2(__float2bfloat16(o[0]), __float2bfloat16(o[1]));
+            if (Yf) { Yf[r0 * Cout + co] = o[0]; Yf[r0 * Cout + co + 1] = o[1]; }
+        }
+        if (v1) {
+            if (Y) *reinterpret_cast<uint32_t *>(Y + r1 * Cout + co) = pack2(__float2bfloat16(o[2]), __float2bfloat16(o[3]));
+            if (Yf) { Yf[r1 * Cout + co] = o[2]; Yf[r1 * Cout + co + 1] = o[3]; }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Weight gradient dW[tap, co, ci] += sum over a chunk of pixels of dY[p, co] X[p + off(tap), ci].
+// GEMM M = co (16 per block), N = ci (64 per block, 16 per warp), K = pixels (16 per step).  The
+// fragments gather pixel pairs (NHWC keeps channels, not pixels, contiguous), so they are built
+// from 16-bit loads.  grid = (pixel chunks, Cout/16 * ceil(Cin/64), 9).
+// ---------------------------------------------------------------------------------------------
+constexpr int kWgChunk = 1024;
+
+__global__ void __launch_bounds__(128) k_conv3x3_wgrad(const bf16 *__restrict__ X, const bf16 *__restrict__ dY,
+                                                       float *__restrict__ dW, int N, int H, int W, int Cin,
+                                                       int Cout) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const int tap = blockIdx.z, dy = tap / 3 - 1, dx = tap % 3 - 1;
+    const int ntile_ci = (Cin + 63) / 64;
+    const int co0 = (blockIdx.y / ntile_ci) * 16, ci_blk = (blockIdx.y % ntile_ci) * 64;
+    const int ciw = ci_blk + warp * 16;  // this warp's 16 input channels (two n-tiles of 8)
+    if (ciw >= Cin) return;
+    const long long P = (long long)N * H * W;
+    const long long pbeg = (long long)blockIdx.x * kWgChunk, pend = min(P, pbeg + kWgChunk);
+    float acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    const unsigned short *dYs = reinterpret_cast<const unsigned short *>(dY);
+    const unsigned short *Xs = reinterpret_cast<const unsigned short *>(X);
+    // source offset of pixel p shifted by the tap, or -1 outside the image
+    auto src = [&](long long p) -> long long {
+        if (p >= pend) return -1;
+        const long long hw = (long long)H * W;
+        const int n = (int)(p / hw), q = (int)(p % hw), y = q / W + dy, x = q % W + dx;
+        if (y < 0 || y >= H || x < 0 || x >= W) return -1;
+        return ((long long)n * H + y) * W + x;
+    };
+    for (long long k0 = pbeg; k0 < pend; k0 += 16) {
+        const long long pk[4] = {k0 + 2 * t, k0 + 2 * t + 1, k0 + 2 * t + 8, k0 + 2 * t + 9};
+        unsigned short av[2][4];  // A rows g and g+8 (co), k columns pk[]
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const bool in = pk[i] < pend;
+            av[0][i] = in ? dYs[pk[i] * Cout + co0 + g] : (unsigned short)0;
+            av[1][i] = in ? dYs[pk[i] * Cout + co0 + g + 8] : (unsigned short)0;
+        }
+        uint32_t a[4] = {(uint32_t)av[0][0] | ((uint32_t)av[0][1] << 16), (uint32_t)av[1][0] | ((uint32_t)av[1][1] << 16),
+                         (uint32_t)av[0][2] | ((uint32_t)av[0][3] << 16), (uint32_t)av[1][2] | ((uint32_t)av[1][3] << 16)};
+        long long s[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) s[i] = src(pk[i]);
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int ci = ciw + j * 8 + g;
+            unsigned short bv[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) bv[i] = (s[i] >= 0 && ci < Cin) ? Xs[s[i] * Cin + ci] : (unsigned short)0;
+            uint32_t b[2] = {(uint32_t)bv[0] | ((uint32_t)bv[1] << 16), (uint32_t)bv[2] | ((uint32_t)bv[3] << 16)};
+            mma_bf16(acc[j], a, b);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const int ci = ciw + j * 8 + 2 * t;
+        if (ci >= Cin) continue;
+        float *w0 = dW + ((long long)tap * Cout + co0 + g) * Cin + ci;
+        float *w1 = dW + ((long long)tap * Cout + co0 + g + 8) * Cin + ci;
+        atomicAdd(w0, acc[j][0]);
+        atomicAdd(w0 + 1, acc[j][1]);
+        atomicAdd(w1, acc[j][2]);
+        atomicAdd(w1 + 1, acc[j][3]);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Point-wise and resampling kernels
+// ---------------------------------------------------------------------------------------------
+#define NN_GSTRIDE(i, n) \
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+// dYm = dY * (Y > 0) (ReLU; relu == 0: identity) in BF16; db[c] += sum of dYm over pixels.
+__global__ void k_relu_grad(const float *__restrict__ dY, const bf16 *__restrict__ Y, bf16 *__restrict__ dYm,
+                            float *__restrict__ db, long long P, int C, int relu) {
+    extern __shared__ float sdb[];
+    for (int c = threadIdx.x; c < C; c += blockDim.x) sdb[c] = 0.0f;
+    __syncthreads();
+    NN_GSTRIDE(i, P * C) {
+        float v = dY[i];
+        if (relu && !(__bfloat162float(Y[i]) > 0.0f)) v = 0.0f;
+        dYm[i] = __float2bfloat16(v);
+        if (db) atomicAdd(&sdb[i % C], v);
+    }
+    __syncthreads();
+    if (db)
+        for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(&db[c], sdb[c]);
+}
+
+// 2x2 average pooling (H, W even): Y[n, y, x, c] = mean of X[n, 2y+i, 2x+j, c]
+__global__ void k_pool2(const bf16 *__restrict__ X, bf16 *__restrict__ Y, int N, int H, int W, int C) {
+    const int h = H / 2, w = W / 2;
+    NN_GSTRIDE(i, (long long)N * h * w * C) {
+        const int c = (int)(i % C);
+        long long q = i / C;
+        const int x = (int)(q % w);
+        q /= w;
+        const int y = (int)(q % h);
+        const int n = (int)(q / h);
+        const long long b = (((long long)n * H + 2 * y) * W + 2 * x) * C + c;
+        const float s = __bfloat162float(X[b]) + __bfloat162float(X[b + C]) + __bfloat162float(X[b + (long long)W * C]) +
+                        __bfloat162float(X[b + (long long)W * C + C]);
+        Y[i] = __float2bfloat16(0.25f * s);
+    }
+}
+// dX[n, y, x, c] (+)= dY[n, y/2, x/2, c] / 4   (acc: add into dX)
+__global__ void k_pool2_grad(const float *__restrict__ dY, float *__restrict__ dX, int N, int H, int W, int C, int acc) {
+    NN_GSTRIDE(i, (long long)N * H * W * C) {
+        const int c = (int)(i % C);
+        long long q = i / C;
+        const int x = (int)(q % W);
+        q /= W;
+        const int y = (int)(q % H);
+        const int n = (int)(q / H);
+        const float v = 0.25f * dY[(((long long)n * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c];
+        dX[i] = acc ? dX[i] + v : v;
+    }
+}
+// nearest 2x upsampling plus a skip tensor: Y[n, y, x, c] = X[n, y/2, x/2, c] + S[n, y, x, c]
+// (S may be null), computed in Float32, stored BF16.  (H, W: output size)
+__global__ void k_up2_add(const bf16 *__restrict__ X, const bf16 *__restrict__ S, bf16 *__restrict__ Y, int N, int H,
+                          int W, int C) {
+    NN_GSTRIDE(i, (long long)N * H * W * C) {
+        const int c = (int)(i % C);
+        long long q = i / C;
+        const int x = (int)(q % W);
+        q /= W;
+        const int y = (int)(q % H);
+        const int n = (int)(q / H);
+        float v = __bfloat162float(X[(((long long)n * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c]);
+        if (S) v += __bfloat162float(S[i]);
+        Y[i] = __float2bfloat16(v);
+    }
+}
+// dX[n, y, x, c] = sum over the 2x2 children of dY   (H, W: the coarse size)
+__global__ void k_up2_grad(const float *__restrict__ dY, float *__restrict__ dX, int N, int H, int W, int C) {
+    NN_GSTRIDE(i, (long long)N * H * W * C) {
+        const int c = (int)(i % C);
+        long long q = i / C;
+        const int x = (int)(q % W);
+        q /= W;
+        const int y = (int)(q % H);
+        const int n = (int)(q / H);
+        const long long W2 = 2LL * W;
+        const long long b = (((long long)n * 2 * H + 2 * y) * W2 + 2 * x) * C + c;
+        dX[i] = dY[b] + dY[b + C] + dY[b + W2 * C] + dY[b + W2 * C + C];
+    }
+}
+// y (+)= x (Float32)
+__global__ void k_axpy(const float *__restrict__ x, float *__restrict__ y, long long n, int acc) {
+    NN_GSTRIDE(i, n) y[i] = acc ? y[i] + x[i] : x[i];
+}
+// mean squared error of channel 0 of Yf (C channels) against T over `count` pixels (mask: weights,
+// may be null); dY gets 2 (y - t) w / count in channel 0 and 0 elsewhere; *loss += the sum.
+__global__ void k_mse(const float *__restrict__ Yf, const float *__restrict__ T, const float *__restrict__ wgt,
+                      float *__restrict__ dY, float *__restrict__ loss, long long P, int C, float inv_count) {
+    float s = 0.0f;
+    NN_GSTRIDE(i, P) {
+        const float w = wgt ? wgt[i] : 1.0f;
+        const float d = (Yf[i * C] - T[i]) * w;
+        s += d * (Yf[i * C] - T[i]);
+        dY[i * C] = 2.0f * d * inv_count;
+        for (int c = 1; c < C; c++) dY[i * C + c] = 0.0f;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, s * inv_count);
+}
+// Adam (bias-corrected), Float32 master weights; refreshes the BF16 copy and, when WT is given,
+// the per-tap transposed copy used by the input-gradient convolution (layout [9][Cout][Cin] ->
+// [9][Cin][Cout]).
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m, float *__restrict__ v,
+                       bf16 *__restrict__ wb, bf16 *__restrict__ wt, long long n, int Cout, int Cin, float lr,
+                       float b1, float b2, float eps, float c1, float c2) {
+    NN_GSTRIDE(i, n) {
+        float gi = g[i];
+        float mi = b1 * m[i] + (1.0f - b1) * gi;
+        float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        w[i] = wi;
+        const bf16 b = __float2bfloat16(wi);
+        if (wb) wb[i] = b;
+        if (wt) {
+            const long long per = (long long)Cout * Cin;
+            const long long tap = i / per, r = i % per;
+            const int co = (int)(r / Cin), ci = (int)(r % Cin);
+            wt[tap * per + (long long)ci * Cout + co] = b;
+        }
+    }
+}
+// BF16 copy and per-tap transpose of a weight tensor (no update)
+__global__ void k_wcast(const float *__restrict__ w, bf16 *__restrict__ wb, bf16 *__restrict__ wt, long long n,
+                        int Cout, int Cin) {
+    NN_GSTRIDE(i, n) {
+        const bf16 b = __float2bfloat16(w[i]);
+        wb[i] = b;
+        if (wt) {
+            const long long per = (long long)Cout * Cin;
+            const long long tap = i / per, r = i % per;
+            const int co = (int)(r / Cin), ci = (int)(r % Cin);
+            wt[tap * per + (long long)ci * Cout + co] = b;
+        }
+    }
+}
+__global__ void k_zero(float *p, long long n) { NN_GSTRIDE(i, n) p[i] = 0.0f; }
+
+// Input stack of the network from a State (column-major, x fastest = NHWC row order): channels
+// h, b, N, zb, zs, ieb, mask, each (v - shift_c) * scale_c, padded with zeros to 16 channels and
+// to Hp x Wp pixels.
+__global__ void k_pack_state(const shk_state s, int nx, int ny, int Hp, int Wp, const float *__restrict__ norm,
+                             bf16 *__restrict__ X) {
+    NN_GSTRIDE(i, (long long)Hp * Wp) {
+        const int x = (int)(i % Wp), y = (int)(i / Wp);
+        float v[16];
+#pragma unroll
+        for (int c = 0; c < 16; c++) v[c] = 0.0f;
+        if (x < nx && y < ny) {
+            const size_t k = (size_t)x + (size_t)y * nx;
+            const double f[7] = {s.h[k], s.b[k], s.N[k], s.zb[k], s.zs[k], s.ieb[k], s.mask[k]};
+#pragma unroll
+            for (int c = 0; c < 7; c++) v[c] = (float)((f[c] - (double)norm[2 * c]) * (double)norm[2 * c + 1]);
+        }
+        uint32_t *o = reinterpret_cast<uint32_t *>(X + i * 16);
+#pragma unroll
+        for (int c = 0; c < 8; c++) o[c] = pack2(__float2bfloat16(v[2 * c]), __float2bfloat16(v[2 * c + 1]));
+    }
+}
+// h_seed = h + dh_scale * Yf[ch 0] on GROUNDED cells (mask == 0), h elsewhere
+__global__ void k_apply_increment(const float *__restrict__ Yf, int C, int nx, int ny, int Wp, double dh_scale,
+                                  const double *__restrict__ h, const double *__restrict__ mask,
+                                  double *__restrict__ out) {
+    NN_GSTRIDE(i, (long long)nx * ny) {
+        const int x = (int)(i % nx), y = (int)(i / nx);
+        const double dh = (double)Yf[((long long)y * Wp + x) * C] * dh_scale;
+        out[i] = mask[i] == 0.0 ? h[i] + dh : h[i];
+    }
+}
+
+static int grid_for(long long n) {
+    long long b = (n + 255) / 256;
+    return (int)(b < 1 ? 1 : (b > 148 * 16 ? 148 * 16 : b));
+}
+
+} // namespace nn
+} // namespace shk
+
+using namespace shk::nn;
+
+extern "C" {
+
+SHK_API int shk_nn_conv3x3(const void *X, const void *Wt, const float *bias, void *Y, float *Yf, int N, int H, int W,
+                           int Cin, int Cout, int relu, int flip, void *stream) {
+    if (!X || !Wt || (!Y && !Yf) || N < 1 || H < 1 || W < 1 || Cin % 16 || Cout % 8) return SHK_BAD_ARG;
+    const long long P = (long long)N * H * W;
+    const int NT = Cout % 64 == 0 ? 64 : (Cout % 32 == 0 ? 32 : 8);
+    dim3 grid((unsigned)((P + 63) / 64), (unsigned)(Cout / NT));
+    cudaStream_t s = (cudaStream_t)stream;
+    const bf16 *x = (const bf16 *)X, *w = (const bf16 *)Wt;
+    bf16 *y = (bf16 *)Y;
+    if (NT == 64) k_conv3x3<64><<<grid, 128, 0, s>>>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip);
+    else if (NT == 32) k_conv3x3<32><<<grid, 128, 0, s>>>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip);
+    else k_conv3x3<8><<<grid, 128, 0, s>>>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_conv3x3_wgrad(const void *X, const void *dY, float *dW, int N, int H, int W, int Cin, int Cout,
+                                 void *stream) {
+    if (!X || !dY || !dW || Cin % 8 || Cout % 16) return SHK_BAD_ARG;
+    const long long P = (long long)N * H * W;
+    dim3 grid((unsigned)((P + kWgChunk - 1) / kWgChunk), (unsigned)((Cout / 16) * ((Cin + 63) / 64)), 9);
+    k_conv3x3_wgrad<<<grid, 128, 0, (cudaStream_t)stream>>>((const bf16 *)X, (const bf16 *)dY, dW, N, H, W, Cin,
+                                                            Cout);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_relu_grad(const float *dY, const void *Y, void *dYm, float *db, long long P, int C, int relu,
+                             void *stream) {
+    if (C < 1 || C > 4096) return SHK_BAD_ARG;
+    k_relu_grad<<<grid_for(P * C), 256, C * sizeof(float), (cudaStream_t)stream>>>(dY, (const bf16 *)Y, (bf16 *)dYm,
+                                                                                   db, P, C, relu);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_pool2(const void *X, void *Y, int N, int H, int W, int C, void *stream) {
+    if (H % 2 || W % 2) return SHK_BAD_ARG;
+    k_pool2<<<grid_for((long long)N * H * W * C / 4), 256, 0, (cudaStream_t)stream>>>((const bf16 *)X, (bf16 *)Y, N,
+                                                                                        H, W, C);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_pool2_grad(const float *dY, float *dX, int N, int H, int W, int C, int acc, void *stream) {
+    k_pool2_grad<<<grid_for((long long)N * H * W * C), 256, 0, (cudaStream_t)stream>>>(dY, dX, N, H, W, C, acc);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_up2_add(const void *X, const void *S, void *Y, int N, int H, int W, int C, void *stream) {
+    if (H % 2 || W % 2) return SHK_BAD_ARG;
+    k_up2_add<<<grid_for((long long)N * H * W * C), 256, 0, (cudaStream_t)stream>>>((const bf16 *)X, (const bf16 *)S,
+                                                                                      (bf16 *)Y, N, H, W, C);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_up2_grad(const float *dY, float *dX, int N, int H, int W, int C, void *stream) {
+    k_up2_grad<<<grid_for((long long)N * H * W * C), 256, 0, (cudaStream_t)stream>>>(dY, dX, N, H, W, C);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_axpy(const float *x, float *y, long long n, int acc, void *stream) {
+    k_axpy<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(x, y, n, acc);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_mse(const float *Yf, const float *T, const float *wgt, float *dY, float *loss, long long P, int C,
+                       float inv_count, void *stream) {
+    k_mse<<<grid_for(P), 256, 0, (cudaStream_t)stream>>>(Yf, T, wgt, dY, loss, P, C, inv_count);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_adam(float *w, const float *g, float *m, float *v, void *wb, void *wt, long long n, int Cout,
+                        int Cin, float lr, float b1, float b2, float eps, int step, void *stream) {
+    if (step < 1) return SHK_BAD_ARG;
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    k_adam<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(w, g, m, v, (bf16 *)wb, (bf16 *)wt, n, Cout, Cin, lr, b1, b2,
+                                                          eps, c1, c2);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_wcast(const float *w, void *wb, void *wt, long long n, int Cout, int Cin, void *stream) {
+    k_wcast<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(w, (bf16 *)wb, (bf16 *)wt, n, Cout, Cin);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_zero(float *p, long long n, void *stream) {
+    k_zero<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(p, n);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_pack_state(const shk_state *st, int nx, int ny, int Hp, int Wp, const float *norm, void *X,
+                              void *stream) {
+    if (!st || Hp < ny || Wp < nx) return SHK_BAD_ARG;
+    k_pack_state<<<grid_for((long long)Hp * Wp), 256, 0, (cudaStream_t)stream>>>(*st, nx, ny, Hp, Wp, norm, (bf16 *)X);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+SHK_API int shk_nn_apply_increment(const float *Yf, int C, int nx, int ny, int Wp, double dh_scale, const double *h,
+                                   const double *mask, double *out, void *stream) {
+    k_apply_increment<<<grid_for((long long)nx * ny), 256, 0, (cudaStream_t)stream>>>(Yf, C, nx, ny, Wp, dh_scale, h,
+                                                                                     mask, out);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+} // extern "C"

@@ -79,8 +79,16 @@ class Ensemble:
             ps.converged = bool(s.last_converged)
             ps.last_iter = int(s.last_picard_iters)
             out.append(dict(steps=s.steps, steps_converged=s.steps_converged, picard_iters=s.picard_iters,
-                            cg_iters=s.cg_iters, last_picard_iters=s.last_picard_iters, march_th=s.march_th))
+                            cg_iters=s.cg_iters, last_picard_iters=s.last_picard_iters,
+                            last_converged=bool(s.last_converged), march_th=s.march_th))
         return out
+
+    def set_snapshots(self, bufs):
+        """Per-instance tensors (like each state's h, or None) that receive h after each timestep's
+        first Picard iteration."""
+        arr = (C.c_void_p * len(self.sims))(*[(b.data_ptr() if b is not None else None) for b in bufs])
+        self._bufs_snap = list(bufs)
+        self._check(self.L.shk_ensemble_set_snapshots(self.h, arr))
 
     def launch_blocks(self) -> dict:
         v = [C.c_int() for _ in range(4)]
