@@ -104,11 +104,15 @@ def barrier(pg):
         pg.barrier()
 
 
+def _dev(pg):
+    return "cpu" if pg.get_backend() == "gloo" else "cuda"
+
+
 def max_over_ranks(pg, x: float) -> float:
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_dev(pg))
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -117,9 +121,16 @@ def sum_over_ranks(pg, x: float) -> float:
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_dev(pg))
     pg.all_reduce(t, op=pg.ReduceOp.SUM)
     return float(t.item())
+
+
+def replica_value(pg, world: int, steps: int, ms_local: float):
+    """Whole-job timesteps/s of `world` independent replicas, each running `steps` steps: all
+    ranks' steps over the slowest rank's device time (the max over ranks)."""
+    ms = max_over_ranks(pg, ms_local)
+    return world * steps / (ms / 1e3), ms
 
 
 # ---------------------------------------------------------------------------------------------
@@ -339,7 +350,7 @@ def ours(args, world, rank, local, pg):
 
     # ---- device-resident pass of the chosen form ---------------------------------------------
     main = timed_pass(shk, w, args, args.form, pg, ClockSampler(torch.cuda.current_device()))
-    value = world * args.steps / (main["ms_max"] / 1e3)
+    value, _ = replica_value(pg, world, args.steps, main["ms"])
     roofline = roofline_for(shk, main["sim"], args.form, w, peaks)
     state_after = main.pop("h_after")
     del main["sim"]

@@ -242,6 +242,9 @@ __device__ __forceinline__ FaceOut face(const Params &P, const Sliding &L, const
 // (Re, ub*taub, q*dh, q*dpw) stay in shared memory; (3) each cell sums its four faces.
 // ---------------------------------------------------------------------------------------------
 constexpr int kTailW = kTX, kTailH = kTY;           // cells per tile
+// 288 threads: the tile's 552 faces take two rounds (with 256 threads the third round would keep
+// only 40 threads busy while the rest waited at the barrier)
+constexpr int kTailThreads = 288;
 constexpr int kTailHW = kTailW + 2, kTailHH = kTailH + 2; // with the halo
 constexpr int kTailXF = (kTailW + 1) * kTailH;      // x-faces of a tile
 constexpr int kTailYF = kTailW * (kTailH + 1);      // y-faces of a tile
@@ -263,7 +266,7 @@ __device__ __forceinline__ void tail_body(Blk B, int nx, int ny, const Params &P
     for (int t = B.id; t < ntiles; t += B.n) {
         const int x0 = (t % tiles_x) * kTailW, y0 = (t / tiles_x) * kTailH;
         // (1) cells of the tile and its halo
-        for (int k = tid; k < kTailHH * kTailHW; k += kThreads) {
+        for (int k = tid; k < kTailHH * kTailHW; k += kTailThreads) {
             const int hx = k % kTailHW, hy = k / kTailHW, ix = x0 - 1 + hx, iy = y0 - 1 + hy;
             const bool corner = (hx == 0 || hx == kTailHW - 1) && (hy == 0 || hy == kTailHH - 1);
             if (corner || ix < 0 || ix >= nx || iy < 0 || iy >= ny) continue;
@@ -271,7 +274,7 @@ __device__ __forceinline__ void tail_body(Blk B, int nx, int ny, const Params &P
         }
         __syncthreads();
         // (2) faces
-        for (int k = tid; k < kTailXF + kTailYF; k += kThreads) {
+        for (int k = tid; k < kTailXF + kTailYF; k += kTailThreads) {
             if (k < kTailXF) {
                 const int fc = k % (kTailW + 1), row = k / (kTailW + 1), f = x0 + fc, iy = y0 + row;
                 if (iy >= ny || f > nx) continue;
@@ -313,7 +316,7 @@ __device__ __forceinline__ void tail_body(Blk B, int nx, int ny, const Params &P
         __syncthreads();
         // (3) cells
         const int ix = x0 + tx, iy = y0 + ty;
-        if (ix < nx && iy < ny) {
+        if (tid < kTailW * kTailH && ix < nx && iy < ny) {
             const size_t c = CI(ix, iy);
             const CellQ &q0 = cq[ty + 1][tx + 1];
             const FaceSm &W = fx[ty * (kTailW + 1) + tx], &E = fx[ty * (kTailW + 1) + tx + 1];
@@ -357,7 +360,7 @@ __device__ __forceinline__ void tail_body(Blk B, int nx, int ny, const Params &P
 }
 
 template <bool FROM_H, bool CHECK>
-__global__ void __launch_bounds__(kThreads, 4) k_tail(int nx, int ny, Params P, Sliding L, shk_state s,
+__global__ void __launch_bounds__(kTailThreads, 3) k_tail(int nx, int ny, Params P, Sliding L, shk_state s,
                                                       const uint8_t *__restrict__ m8,
                                                       const double *__restrict__ h_prev, double *partials,
                                                       unsigned int *counter, PicDev *pic) {
@@ -545,10 +548,10 @@ int build_mask8(Ctx *c) {
     return check_launch(c, "k_mask8");
 }
 
-// One resident wave of the tail (four 256-thread blocks per SM), striding over the tiles.
+// One resident wave of the tail (three blocks per SM), striding over the tiles.
 static int tail_grid(const Ctx *c) {
     const long long tiles = (long long)((c->nx + kTailW - 1) / kTailW) * ((c->ny + kTailH - 1) / kTailH);
-    return (int)std::max(1LL, std::min(tiles, (long long)c->num_sms * 4));
+    return (int)std::max(1LL, std::min(tiles, (long long)c->num_sms * 3));
 }
 
 int launch_initial_conditions(Ctx *c) {
@@ -569,7 +572,7 @@ int launch_initial_conditions(Ctx *c) {
     k_init_faces<<<flat_grid(c, nf), kThreads, 0, c->stream>>>(nx, ny, c->P, c->st);
     c->launches++;
     if ((rc = check_launch(c, "k_init_faces"))) return rc;
-    k_tail<false, false><<<tail_grid(c), kThreads, 0, c->stream>>>(nx, ny, c->P, c->SL, c->st, c->mask8, nullptr,
+    k_tail<false, false><<<tail_grid(c), kTailThreads, 0, c->stream>>>(nx, ny, c->P, c->SL, c->st, c->mask8, nullptr,
                                                                        c->partials, c->counter, nullptr);
     c->launches++;
     return check_launch(c, "k_tail<init>");
@@ -597,11 +600,11 @@ int launch_export_mfls(Ctx *c, double *aP, double *aE, double *aW, double *aN, d
 
 int launch_tail(Ctx *c, bool picard_check) {
     if (picard_check)
-        k_tail<true, true><<<tail_grid(c), kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->SL, c->st, c->mask8,
+        k_tail<true, true><<<tail_grid(c), kTailThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->SL, c->st, c->mask8,
                                                                         c->h_prev, c->partials, c->counter,
                                                                         &c->dev->pic);
     else
-        k_tail<true, false><<<tail_grid(c), kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->SL, c->st, c->mask8,
+        k_tail<true, false><<<tail_grid(c), kTailThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->SL, c->st, c->mask8,
                                                                          nullptr, c->partials, c->counter, nullptr);
     c->launches++;
     return check_launch(c, "k_tail");
@@ -652,7 +655,7 @@ __global__ void __launch_bounds__(kThreads) k_ens_assemble(EnsInst *E, const int
     assemble_body<false>(B, I.nx, I.ny, I.P, I.kfs, 0.0, I.st, I.mask8, I.aP, I.aE, I.aN, I.rhs, I.h_prev);
 }
 
-__global__ void __launch_bounds__(kThreads, 4) k_ens_tail(EnsInst *E, const int *b2i) {
+__global__ void __launch_bounds__(kTailThreads, 3) k_ens_tail(EnsInst *E, const int *b2i) {
     __shared__ EnsInst I;
     const Blk B = ens_stage(I, E, b2i, EF_TAIL);
     if (!I.pic_active) return;
@@ -678,7 +681,7 @@ void ens_assemble(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks) {
     k_ens_assemble<<<nblocks, kThreads, 0, s>>>(E, b2i);
 }
 void ens_tail(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks) {
-    k_ens_tail<<<nblocks, kThreads, 0, s>>>(E, b2i);
+    k_ens_tail<<<nblocks, kTailThreads, 0, s>>>(E, b2i);
 }
 void ens_gap(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, const EnsCtl *ctl) {
     k_ens_gap_cells<<<nblocks, kThreads, 0, s>>>(E, b2i, ctl);
