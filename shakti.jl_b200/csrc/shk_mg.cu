@@ -249,20 +249,23 @@ struct FusedSm {
     uint8_t act[kFSH][kFSW];
 };
 
-// (A X)_c at staged position (hx, hy) = global (gx, gy), same operand order as lapl_apply
-__device__ __forceinline__ float ax_sm(const FusedSm &S, const float (&X)[kFSH][kFSW], int nx, int ny, int hx, int hy,
-                                       int gx, int gy) {
+// (A X)_c at staged position (hx, hy), same operand order as lapl_apply.  No bounds tests: the
+// couplings across the level's edge are zero in every assembled and coarsened operator (the
+// east/north entries of the last column/row, and the staged zeros outside the level), so those
+// terms add 0 * (finite) = 0.
+__device__ __forceinline__ float ax_sm(const FusedSm &S, const float (&X)[kFSH][kFSW], int hx, int hy) {
     const float xc = X[hy][hx];
     float y = S.dP[hy][hx] * xc;
-    if (gx < nx - 1) y += S.aE[hy][hx] * (xc - X[hy][hx + 1]);
-    if (gx > 0) y += S.aE[hy][hx - 1] * (xc - X[hy][hx - 1]);
-    if (gy < ny - 1) y += S.aN[hy][hx] * (xc - X[hy + 1][hx]);
-    if (gy > 0) y += S.aN[hy - 1][hx] * (xc - X[hy - 1][hx]);
+    y += S.aE[hy][hx] * (xc - X[hy][hx + 1]);
+    y += S.aE[hy][hx - 1] * (xc - X[hy][hx - 1]);
+    y += S.aN[hy][hx] * (xc - X[hy + 1][hx]);
+    y += S.aN[hy - 1][hx] * (xc - X[hy - 1][hx]);
     return y;
 }
 
-// Stages the level's operator and rhs over the tile and its halo; cells outside the level get
-// act = 0 and zeros (never read as neighbours: the bounds tests above skip them).
+// Stages the level's operator and rhs over the tile and its halo; cells outside the level are
+// zeros (act = 0, wD = 0), so every sweep leaves them at 0.  (Flat loops over the staged region
+// keep every lane busy; the divisions are by a compile-time constant.)
 template <typename TB>
 __device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b, int x0, int y0, double *r64) {
     for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
@@ -289,16 +292,13 @@ __device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b
     }
 }
 
-// One damped-Jacobi sweep XO = XI + wD (b - A XI) over the staged positions at distance <= reach
-// from the tile (cells inside the level only).
-__device__ __forceinline__ void sweep_sm(FusedSm &S, const float (&XI)[kFSH][kFSW], float (&XO)[kFSH][kFSW], int nx,
-                                         int ny, int x0, int y0, int reach) {
-    const int lo = kFR - reach, wdt = kFW + 2 * reach, hgt = kFH + 2 * reach;
+// One damped-Jacobi sweep XO = XI + wD (b - A XI) over the staged positions within distance 1 of
+// the tile.
+__device__ __forceinline__ void sweep_sm(FusedSm &S, const float (&XI)[kFSH][kFSW], float (&XO)[kFSH][kFSW]) {
+    constexpr int wdt = kFW + 2, hgt = kFH + 2;
     for (int k = threadIdx.x; k < wdt * hgt; k += blockDim.x) {
-        const int hx = lo + k % wdt, hy = lo + k / wdt, gx = x0 - kFR + hx, gy = y0 - kFR + hy;
-        if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) continue;
-        const float ax = ax_sm(S, XI, nx, ny, hx, hy, gx, gy);
-        XO[hy][hx] = XI[hy][hx] + S.wD[hy][hx] * (S.b[hy][hx] - ax);
+        const int hx = kFR - 1 + k % wdt, hy = kFR - 1 + k / wdt;
+        XO[hy][hx] = XI[hy][hx] + S.wD[hy][hx] * (S.b[hy][hx] - ax_sm(S, XI, hx, hy));
     }
 }
 
@@ -308,6 +308,7 @@ template <typename TB>
 __global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo, int nxc, int nyc, float *bc) {
     if (cg_finished(L.done)) return;
     __shared__ FusedSm S;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // output rows: 32 x 8 threads
     const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
@@ -319,28 +320,28 @@ __global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo
             S.x0[hy][hx] = S.wD[hy][hx] * S.b[hy][hx];
         }
         __syncthreads();
-        sweep_sm(S, S.x0, S.x1, L.nx, L.ny, x0, y0, 1);
+        sweep_sm(S, S.x0, S.x1);
         __syncthreads();
-        for (int k = threadIdx.x; k < kFW * kFH; k += blockDim.x) {
-            const int tx = k % kFW, ty = k / kFW, gx = x0 + tx, gy = y0 + ty;
-            if (gx < L.nx && gy < L.ny) xo[(size_t)gx + (size_t)gy * L.nx] = S.x1[ty + kFR][tx + kFR];
+        for (int r = ty; r < kFH; r += 8) {
+            const int gx = x0 + tx, gy = y0 + r;
+            if (gx < L.nx && gy < L.ny) xo[(size_t)gx + (size_t)gy * L.nx] = S.x1[r + kFR][tx + kFR];
         }
-        // restriction: one thread per aggregate of the tile
-        for (int k = threadIdx.x; k < (kFW / 2) * (kFH / 2); k += blockDim.x) {
-            const int I = x0 / 2 + k % (kFW / 2), J = y0 / 2 + k / (kFW / 2);
-            if (I >= nxc || J >= nyc) continue;
-            float sres = 0.0f;
+        // restriction: one thread per aggregate of the tile (16 x 8 aggregates, 128 threads)
+        if (threadIdx.x < (kFW / 2) * (kFH / 2)) {
+            const int ai = threadIdx.x % (kFW / 2), aj = threadIdx.x / (kFW / 2);
+            const int I = x0 / 2 + ai, J = y0 / 2 + aj;
+            if (I < nxc && J < nyc) {
+                float sres = 0.0f;
 #pragma unroll
-            for (int dj = 0; dj < 2; dj++)
+                for (int dj = 0; dj < 2; dj++)
 #pragma unroll
-                for (int di = 0; di < 2; di++) {
-                    const int gx = 2 * I + di, gy = 2 * J + dj;
-                    if (gx >= L.nx || gy >= L.ny) continue;
-                    const int hx = gx - x0 + kFR, hy = gy - y0 + kFR;
-                    if (!S.act[hy][hx]) continue;
-                    sres += S.b[hy][hx] - ax_sm(S, S.x1, L.nx, L.ny, hx, hy, gx, gy);
-                }
-            bc[(size_t)I + (size_t)J * nxc] = sres;
+                    for (int di = 0; di < 2; di++) {
+                        const int hx = 2 * ai + di + kFR, hy = 2 * aj + dj + kFR;
+                        if (!S.act[hy][hx]) continue;  // inactive, and every cell outside the level
+                        sres += S.b[hy][hx] - ax_sm(S, S.x1, hx, hy);
+                    }
+                bc[(size_t)I + (size_t)J * nxc] = sres;
+            }
         }
         __syncthreads();  // the next tile reuses the staged arrays
     }
@@ -351,11 +352,12 @@ __global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo
 // otherwise it writes the level's result to xo.
 template <typename TB, bool LAST>
 __global__ void __launch_bounds__(256, 6) k_mg_up(Lv L, const TB *b, const float *xi, const float *xc, int nxc, float wc,
-                                               float *xo, double *z, CgDev *cg, int init, double *partials,
-                                               unsigned int *counter) {
+                                                  float *xo, double *z, CgDev *cg, int init, double *partials,
+                                                  unsigned int *counter) {
     if (cg_finished(L.done)) return;
     __shared__ FusedSm S;
     __shared__ double r64[LAST ? kFCells : 1];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // output rows: 32 x 8 threads
     const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
     double red[2] = {0.0, 0.0};
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -372,13 +374,13 @@ __global__ void __launch_bounds__(256, 6) k_mg_up(Lv L, const TB *b, const float
             S.x0[hy][hx] = v;
         }
         __syncthreads();
-        sweep_sm(S, S.x0, S.x1, L.nx, L.ny, x0, y0, 1);
+        sweep_sm(S, S.x0, S.x1);
         __syncthreads();
-        for (int k = threadIdx.x; k < kFW * kFH; k += blockDim.x) {
-            const int tx = k % kFW, ty = k / kFW, gx = x0 + tx, gy = y0 + ty;
+        for (int r = ty; r < kFH; r += 8) {
+            const int gx = x0 + tx, gy = y0 + r;
             if (gx >= L.nx || gy >= L.ny) continue;
-            const int hx = tx + kFR, hy = ty + kFR;
-            const float ax = ax_sm(S, S.x1, L.nx, L.ny, hx, hy, gx, gy);
+            const int hx = tx + kFR, hy = r + kFR;
+            const float ax = ax_sm(S, S.x1, hx, hy);
             const size_t q = (size_t)gx + (size_t)gy * L.nx;
             if (LAST) {
                 const double rk = r64[hy * kFSW + hx];
