@@ -266,20 +266,32 @@ __device__ __forceinline__ float ax_sm(const FusedSm &S, const float (&X)[kFSH][
 // Stages the level's operator and rhs over the tile and its halo; cells outside the level are
 // zeros (act = 0, wD = 0), so every sweep leaves them at 0.  (Flat loops over the staged region
 // keep every lane busy; the divisions are by a compile-time constant.)
-template <typename TB>
-__device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b, int x0, int y0, double *r64) {
+// X0 (the first iterate over the whole region) is formed in the same pass: DOWN, the first sweep
+// from zero, wD b; UP, the fine iterate plus the prolonged coarse correction.
+template <typename TB, bool UP>
+__device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b, int x0, int y0, double *r64,
+                                            const float *xi, const float *xc, int nxc, float wc) {
     for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
         const int hx = k % kFSW, hy = k / kFSW, gx = x0 - kFR + hx, gy = y0 - kFR + hy;
         if (gx >= 0 && gx < L.nx && gy >= 0 && gy < L.ny) {
             const size_t q = (size_t)gx + (size_t)gy * L.nx;
             const TB bq = b[q];
             if (r64) r64[k] = (double)bq;
-            S.b[hy][hx] = (float)bq;
-            S.wD[hy][hx] = L.wD[q];
+            const float bf = (float)bq, wd = L.wD[q];
+            const uint8_t a = L.act[q];
+            S.b[hy][hx] = bf;
+            S.wD[hy][hx] = wd;
             S.dP[hy][hx] = L.dP[q];
             S.aE[hy][hx] = L.aE[q];
             S.aN[hy][hx] = L.aN[q];
-            S.act[hy][hx] = L.act[q];
+            S.act[hy][hx] = a;
+            if (UP) {
+                float v = xi[q];
+                if (a) v += wc * xc[(size_t)(gx >> 1) + (size_t)(gy >> 1) * nxc];
+                S.x0[hy][hx] = v;
+            } else {
+                S.x0[hy][hx] = wd * bf;
+            }
         } else {
             if (r64) r64[k] = 0.0;
             S.b[hy][hx] = 0.0f;
@@ -288,6 +300,7 @@ __device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b
             S.aE[hy][hx] = 0.0f;
             S.aN[hy][hx] = 0.0f;
             S.act[hy][hx] = 0;
+            S.x0[hy][hx] = 0.0f;
         }
     }
 }
@@ -312,34 +325,30 @@ __global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo
     const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
-        stage_level<TB>(S, L, b, x0, y0, nullptr);
-        __syncthreads();
-        // first sweep from x = 0 on the whole staged region: x0 = wD b
-        for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
-            const int hx = k % kFSW, hy = k / kFSW;
-            S.x0[hy][hx] = S.wD[hy][hx] * S.b[hy][hx];
-        }
+        stage_level<TB, false>(S, L, b, x0, y0, nullptr, nullptr, nullptr, 0, 0.0f);
         __syncthreads();
         sweep_sm(S, S.x0, S.x1);
         __syncthreads();
+        // x1 out, and each tile cell's residual (0 on inactive cells) into the x0 array, which
+        // the restriction then sums per aggregate
         for (int r = ty; r < kFH; r += 8) {
-            const int gx = x0 + tx, gy = y0 + r;
-            if (gx < L.nx && gy < L.ny) xo[(size_t)gx + (size_t)gy * L.nx] = S.x1[r + kFR][tx + kFR];
+            const int gx = x0 + tx, gy = y0 + r, hx = tx + kFR, hy = r + kFR;
+            if (gx < L.nx && gy < L.ny) xo[(size_t)gx + (size_t)gy * L.nx] = S.x1[hy][hx];
+            S.x0[hy][hx] = S.act[hy][hx] ? S.b[hy][hx] - ax_sm(S, S.x1, hx, hy) : 0.0f;
         }
-        // restriction: one thread per aggregate of the tile (16 x 8 aggregates, 128 threads)
+        __syncthreads();
+        // restriction: one thread per aggregate of the tile (16 x 8 aggregates, 128 threads), in the
+        // per-sweep kernel's order (dj outer, di inner)
         if (threadIdx.x < (kFW / 2) * (kFH / 2)) {
             const int ai = threadIdx.x % (kFW / 2), aj = threadIdx.x / (kFW / 2);
             const int I = x0 / 2 + ai, J = y0 / 2 + aj;
             if (I < nxc && J < nyc) {
+                const int hx = 2 * ai + kFR, hy = 2 * aj + kFR;
                 float sres = 0.0f;
-#pragma unroll
-                for (int dj = 0; dj < 2; dj++)
-#pragma unroll
-                    for (int di = 0; di < 2; di++) {
-                        const int hx = 2 * ai + di + kFR, hy = 2 * aj + dj + kFR;
-                        if (!S.act[hy][hx]) continue;  // inactive, and every cell outside the level
-                        sres += S.b[hy][hx] - ax_sm(S, S.x1, hx, hy);
-                    }
+                sres += S.x0[hy][hx];
+                sres += S.x0[hy][hx + 1];
+                sres += S.x0[hy + 1][hx];
+                sres += S.x0[hy + 1][hx + 1];
                 bc[(size_t)I + (size_t)J * nxc] = sres;
             }
         }
@@ -362,17 +371,7 @@ __global__ void __launch_bounds__(256, 6) k_mg_up(Lv L, const TB *b, const float
     double red[2] = {0.0, 0.0};
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
-        stage_level<TB>(S, L, b, x0, y0, LAST ? r64 : nullptr);
-        for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
-            const int hx = k % kFSW, hy = k / kFSW, gx = x0 - kFR + hx, gy = y0 - kFR + hy;
-            float v = 0.0f;
-            if (gx >= 0 && gx < L.nx && gy >= 0 && gy < L.ny) {
-                const size_t q = (size_t)gx + (size_t)gy * L.nx;
-                v = xi[q];
-                if (L.act[q]) v += wc * xc[(size_t)(gx >> 1) + (size_t)(gy >> 1) * nxc];
-            }
-            S.x0[hy][hx] = v;
-        }
+        stage_level<TB, true>(S, L, b, x0, y0, LAST ? r64 : nullptr, xi, xc, nxc, wc);
         __syncthreads();
         sweep_sm(S, S.x0, S.x1);
         __syncthreads();
