@@ -43,6 +43,7 @@ static void derive_params(Ctx *c) {
     if (P.n_int < 0) P.n_int = -1;
     if (P.nm1_int < 0) P.nm1_int = -1;
     P.with_sensible = !(p.ct == 0.0 || p.cw == 0.0); // src/simulation.jl:132
+    P.root3 = p.n == 3.0;
     P.Linv = 1 / p.L;
     P.dx = c->dx;
     P.dy = c->dy;

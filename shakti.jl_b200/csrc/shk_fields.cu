@@ -3,8 +3,8 @@
 //
 // Every value is produced with the reference's formula and evaluation order (the library is
 // compiled with --fmad=false, so no a*b+c is contracted), which makes these kernels bit-identical
-// to the reference's unfused kernels except for x^(1/n), where CUDA's pow and Julia's pow may
-// differ in the last bit.  Fusion never changes a value: a face quantity needed by two cells is
+// to the reference's unfused kernels except for x^(1/n) (cbrt for n = 3, pow otherwise), which may
+// differ from Julia's x^(1/n) in the last bit.  Fusion never changes a value: a face quantity needed by two cells is
 // computed once from the same operands and shared.
 #include <cuda_runtime.h>
 #include <float.h>
@@ -161,7 +161,10 @@ __device__ __forceinline__ double taub_face(const Params &P, const Sliding &L, d
     if (L.kind == SHK_SLIDING_LINEAR) return Cf * Nf * ub;
     if (!(abs_v > 0)) return 0.0;
     double denom = (L.kind == SHK_SLIDING_REG_COULOMB_V0) ? L.v0 : jl_pow(fabs(Nf), P.n, P.n_int) * lf;
-    return Nf * Cf * jl_pow(abs_v / (abs_v + denom), P.inv_n, -1) * (ub / abs_v);
+    // x^(1/n): for n = 3, cbrt (a fraction of pow's cost; it differs from pow(x, 1/3.0) by at most
+    // about an ulp, within the tolerance the parity tests hold the pow-dependent fields to)
+    const double ratio = abs_v / (abs_v + denom);
+    return Nf * Cf * (P.root3 ? cbrt(ratio) : jl_pow(ratio, P.inv_n, -1)) * (ub / abs_v);
 }
 
 // Cell-centred quantities needed by faces.

@@ -90,6 +90,7 @@ struct Params {
     double nm1, inv_n;   // n-1, 1/n
     int n_int, nm1_int;  // integer-valued exponents (-1 if not integral)
     int with_sensible;   // ct*cw != 0
+    int root3;           // n == 3: x^(1/n) as cbrt(x) (within an ulp of pow(x, 1/3.0))
     double Linv;         // 1/L
     double dx, dy, dx2, dy2;
 };
