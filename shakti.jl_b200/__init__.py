@@ -21,7 +21,7 @@ from .simulation import (AbstractHeadScheme, EllipticHeadScheme, ParabolicHeadSc
                          ExplicitGapScheme, ImplicitGapScheme, AbstractSensibleHeatScheme, WithSensibleHeat,
                          NoSensibleHeat, AbstractOpenBySlidingScheme, WithOpenBySliding, NoOpenBySliding,
                          AbstractObserver, NoObserver, LiveObserver, Simulation, run, step, step_h, step_b,
-                         update_ieb, picard_status, set_initial_conditions)
+                         update_ieb, picard_status, set_initial_conditions, save_checkpoint, load_checkpoint)
 from .ensemble import Ensemble
 from . import configs
 

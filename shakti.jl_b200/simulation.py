@@ -75,6 +75,10 @@ class AbstractObserver:
     def prepare(self, state):
         pass
 
+    def resume(self, state, t):
+        """resume! (src/observer.jl): continue an interrupted run's observation after timestep t."""
+        pass
+
     def observe(self, state, t, total_time):
         pass
 
@@ -208,13 +212,52 @@ def step(sim: Simulation) -> None:
     step_b(sim)
 
 
-def run(sim: Simulation) -> None:
-    """run!(sim) (src/run.jl:21-63) without checkpointing."""
-    sim.total_time = 0.0
-    sim.observer.prepare(sim.state)
-    sim.observer.observe(sim.state, 0, sim.total_time)
+# ---------------------------------------------------------------------------------------------
+# Checkpoint/restart (src/checkpoint.jl:26-64): the full State and total_time, keyed as the
+# reference keys them ("t", "total_time", one key per State field); a numpy .npz container (JLD2
+# needs Julia).  Written to path + ".tmp" and renamed into place, so a crash mid-write leaves the
+# previous checkpoint intact.
+# ---------------------------------------------------------------------------------------------
+def save_checkpoint(path: str, sim: Simulation, t: int) -> None:
+    import os
+    host = {("lambda" if k == "lambda_" else k): v for k, v in sim.state.to_numpy().items()}
+    tmp = path + ".tmp"
+    with open(tmp, "wb") as f:
+        np.savez(f, t=np.int64(t), total_time=np.float64(sim.total_time), **host)
+    os.replace(tmp, path)
+
+
+def load_checkpoint(sim: Simulation, path: str) -> int:
+    """Restores sim.state and sim.total_time in place; returns the timestep saved."""
+    import torch
+    with np.load(path) as f:
+        for name in _lib.STATE_FIELDS:
+            key = "lambda" if name == "lambda_" else name
+            dst = sim.state[name]
+            a = np.asarray(f[key], dtype=np.float64)
+            if a.shape != tuple(dst.shape):
+                raise ValueError(f"checkpoint field {name} has shape {a.shape}, the state {tuple(dst.shape)}")
+            dst.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+        t, total_time = int(f["t"]), float(f["total_time"])
+    sim.total_time = total_time
+    return t
+
+
+def run(sim: Simulation, checkpoint_every: int | None = None, checkpoint_path: str | None = None,
+        restart_path: str | None = None) -> None:
+    """run!(sim; checkpoint_every, checkpoint_path, restart_path) (src/run.jl:21-63)."""
+    if (checkpoint_every is None) != (checkpoint_path is None):
+        raise ValueError("checkpoint_every and checkpoint_path must be given together")
+    if restart_path is None:
+        sim.total_time = 0.0
+        sim.observer.prepare(sim.state)
+        sim.observer.observe(sim.state, 0, sim.total_time)
+        start_t = 0
+    else:
+        start_t = load_checkpoint(sim, restart_path)
+        sim.observer.resume(sim.state, start_t)
     sim.step_stats = []
-    for t in range(1, sim.tsteps + 1):
+    for t in range(start_t + 1, sim.tsteps + 1):
         t0 = time.perf_counter()
         step(sim)
         sim.total_time += sim.dt
@@ -223,6 +266,8 @@ def run(sim: Simulation) -> None:
         sim.step_stats.append(dict(converged=conv, last_iter=last,
                                    cg_iters=(sim.hs.ps.cg_iters_total if isinstance(sim.hs, EllipticHeadScheme)
                                              else sim.hs.ls.stats.niter)))
+        if checkpoint_every is not None and t % checkpoint_every == 0:
+            save_checkpoint(checkpoint_path, sim, t)
         if sim.verbose:
             import torch
             torch.cuda.synchronize()

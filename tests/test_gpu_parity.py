@@ -363,3 +363,35 @@ def test_multigrid_run_matches_oracle_tight(shk, orc, cuda):
     shk.run(sim)
     orc.run(st, None, osl, 5, 3600.0, cgspec=orc.CgSpec(precond=0, stop_rule=1, rtol=1e-13, atol=0.0))
     assert_fields_close(s, st, tol=1e-8)
+
+
+def test_checkpoint_restart_continues_the_run(shk, orc, cuda, tmp_path):
+    """run! with checkpoint_every writes the full State and total_time (keys as the reference's:
+    "t", "total_time", one per State field); a fresh Simulation restarted from the step-3 checkpoint
+    and run to step 6 ends bit-identical to the uninterrupted six steps (src/run.jl:21-63,
+    src/checkpoint.jl:26-64)."""
+    w = shk.configs.plain64()
+
+    def make(tsteps):
+        g, pm, sl, osl, s, st = setup_pair(shk, orc, cuda, w)
+        ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem)
+        ps = shk.PicardSolver(500, 1e-6, ls, g)
+        return shk.Simulation(g, s, tsteps, 3600.0, pm, "implicit", [], shk.ConstantMeltInput(), sl, ps=ps)
+
+    with pytest.raises(ValueError):
+        shk.run(make(1), checkpoint_every=2)
+    full = make(6)
+    ck = str(tmp_path / "ck.npz")
+    shk.run(full, checkpoint_every=3, checkpoint_path=ck)
+    with np.load(ck) as f:
+        assert int(f["t"]) == 6 and float(f["total_time"]) == 6 * 3600.0
+        assert {("lambda" if n == "lambda_" else n) for n in shk._lib.STATE_FIELDS} <= set(f.files)
+    part = make(3)
+    ck3 = str(tmp_path / "ck3.npz")
+    shk.run(part, checkpoint_every=3, checkpoint_path=ck3)
+    resumed = make(6)
+    shk.run(resumed, restart_path=ck3)
+    assert resumed.total_time == full.total_time
+    a, b = resumed.state.to_numpy(), full.state.to_numpy()
+    for f in shk._lib.STATE_FIELDS:
+        assert np.array_equal(a[f], b[f]), f
