@@ -449,7 +449,7 @@ __device__ __forceinline__ void assemble_body(Blk B, int nx, int ny, const Param
 }
 
 template <bool PARABOLIC>
-__global__ void __launch_bounds__(kThreads) k_assemble(int nx, int ny, Params P, int kfs, double dt,
+__global__ void __launch_bounds__(kThreads, 6) k_assemble(int nx, int ny, Params P, int kfs, double dt,
                                                        shk_state s, const uint8_t *__restrict__ m8,
                                                        double *__restrict__ aP, double *__restrict__ aE,
                                                        double *__restrict__ aN, double *__restrict__ rhs,
