@@ -1,8 +1,10 @@
 """Builds libshakti_b200.so (sm_100a) in-tree with nvcc.
 
 The library is plain CUDA C++ behind a C ABI (include/shakti_b200.h); it links only the CUDA
-runtime.  --fmad=false keeps every a*b+c as two rounded operations so the field kernels reproduce
-the reference's unfused Float64 arithmetic bit for bit.
+runtime.  --fmad=false keeps every a*b+c as two rounded operations so the field kernels and the
+Float64 CG reproduce the reference's unfused Float64 arithmetic bit for bit.  The multigrid
+preconditioner and the warm-start network carry no such parity requirement and are compiled with
+fused multiply-adds.
 """
 from __future__ import annotations
 
@@ -18,6 +20,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libshakti_b200.so"
 SOURCES = ["shk_api.cu", "shk_fields.cu", "shk_krylov.cu", "shk_mg.cu", "shk_ensemble.cu", "shk_nn.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FMAD = {"shk_mg.cu", "shk_nn.cu"}  # sources compiled with --fmad=true
 
 
 def nvcc() -> str:
@@ -50,7 +53,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
     objs = []
-    common = [nvcc(), *host_compiler(), *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
+    common = [nvcc(), *host_compiler(), *ARCH, "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC,-fvisibility=hidden", "-I", str(ROOT / "include"),
               "--expt-relaxed-constexpr", "--extended-lambda"]
     if verbose:
@@ -58,7 +61,8 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     common += list(extra or [])
     for src in sources():
         obj = objdir / (src.stem + ".o")
-        cmd = [*common, "-c", str(src), "-o", str(obj)]
+        fmad = "--fmad=true" if src.name in FMAD else "--fmad=false"
+        cmd = [*common, fmad, "-c", str(src), "-o", str(obj)]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stdout}\n{r.stderr}")

@@ -205,7 +205,7 @@ SHK_API int shk_create(int nx, int ny, double lx, double ly, void *stream, void 
     if (const char *v = getenv("SHK_MG_NU")) c->mg_nu = std::max(1, atoi(v));
     if (const char *v = getenv("SHK_MG_OMEGA")) c->mg_omega = (float)atof(v);
     if (const char *v = getenv("SHK_MG_OMEGA_C")) c->mg_omega_c = (float)atof(v);
-    if (const char *v = getenv("SHK_MG_FUSED")) c->mg_fused = atoi(v) != 0;
+    if (const char *v = getenv("SHK_MG_FUSED")) c->mg_fused = std::min(2, std::max(0, atoi(v)));
     // SHK_CG_GRAPHS: 0 issues each CG iteration's kernels directly, 1 replays one CUDA graph per
     // iteration in host-sized batches, 2 (default) runs the whole iteration loop as one graph with a
     // device-side WHILE node

@@ -133,7 +133,7 @@ struct Ctx {
     int mg_nu = 2;           // damped-Jacobi sweeps before and after each coarse correction
     float mg_omega = 0.8f;   // Jacobi damping
     float mg_omega_c = 1.0f; // coarse-correction scaling
-    bool mg_fused = true;    // fused two-sweep level kernels (nu = 2)
+    int mg_fused = 1;        // nu = 2 level kernels: 1 tile (default), 2 warp-marching, 0 per-sweep
     int max_blocks = 0;
     int grid_stencil = 0;    // blocks for tile-stride kernels
     int march_th = 8;        // row-marching tile height

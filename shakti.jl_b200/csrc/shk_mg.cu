@@ -403,6 +403,205 @@ __global__ void __launch_bounds__(256, 6) k_mg_up(Lv L, const TB *b, const float
 }
 
 // ---------------------------------------------------------------------------------------------
+// Warp-marching level kernels (SHK_MG_FUSED=2).  A warp owns a strip of 32 columns (lanes
+// 2..29 are its 28 output columns; lanes 0, 1, 30, 31 the halo the two sweeps need) and marches
+// down kMH rows plus two halo rows each side.  Each row is loaded once (coalesced), the two sweeps
+// are pipelined two rows apart in registers, and the x +- 1 neighbours and the west coupling come
+// from warp shuffles: no shared memory and no block barrier.  Cells outside the level load as
+// zeros (act = 0, wD = 0), so every sweep leaves them at 0, and the couplings across the level's
+// edge are zero in every operator, so no neighbour term needs a bounds test.
+// ---------------------------------------------------------------------------------------------
+constexpr int kMW = 28, kMH = 64;  // output columns and rows of a warp's strip
+
+struct RowC {  // one row's coefficients at this lane's column
+    float b, wD, dP, aE, aN;
+    int act;
+};
+
+template <typename TB>
+__device__ __forceinline__ RowC load_row(const Lv &L, const TB *b, int gx, int gy, bool inx, double *bd = nullptr) {
+    RowC r;
+    if (inx && gy >= 0 && gy < L.ny) {
+        const size_t q = (size_t)gx + (size_t)gy * L.nx;
+        const TB bq = b[q];
+        if (bd) *bd = (double)bq;
+        r.b = (float)bq;
+        r.wD = L.wD[q];
+        r.dP = L.dP[q];
+        r.aE = L.aE[q];
+        r.aN = L.aN[q];
+        r.act = L.act[q];
+    } else {
+        if (bd) *bd = 0.0;
+        r.b = r.wD = r.dP = r.aE = r.aN = 0.0f;
+        r.act = 0;
+    }
+    return r;
+}
+
+// (A x) at row c: xs, xn the column's south/north values, aNs the south row's north coupling
+__device__ __forceinline__ float ax_row(const RowC &c, float aNs, float x, float xs, float xn) {
+    const float xe = __shfl_down_sync(0xffffffffu, x, 1), xw = __shfl_up_sync(0xffffffffu, x, 1);
+    const float aW = __shfl_up_sync(0xffffffffu, c.aE, 1);
+    float y = c.dP * x;
+    y += c.aE * (x - xe);
+    y += aW * (x - xw);
+    y += c.aN * (x - xn);
+    y += aNs * (x - xs);
+    return y;
+}
+
+// Descending half: x1 = two sweeps from zero (to xo), coarse rhs bc = restriction of b - A x1.
+template <typename TB>
+__global__ void __launch_bounds__(128) k_mg_down_m(Lv L, const TB *b, float *xo, int nxc, int nyc, float *bc) {
+    if (cg_finished(L.done)) return;
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const int sxn = (L.nx + kMW - 1) / kMW, nstrips = sxn * ((L.ny + kMH - 1) / kMH);
+    for (int st = blockIdx.x * wpb + (threadIdx.x >> 5); st < nstrips; st += gridDim.x * wpb) {
+        const int x0 = (st % sxn) * kMW, y0 = (st / sxn) * kMH;
+        const int gx = x0 - 2 + lane;
+        const bool inx = gx >= 0 && gx < L.nx, out_lane = lane >= 2 && lane < 2 + kMW && gx < L.nx;
+        // pipeline registers: coefficients of rows j-1, j-2, j-3 (c1, c2, c3), x0 of rows j-1, j-2
+        // (x0a, x0b), x1 of rows j-2, j-3 (x1a, x1b); row j is loaded at the top of the loop
+        RowC c1 = load_row<TB>(L, b, gx, y0 - 3, inx), c2{}, c3{};
+        RowC cj = load_row<TB>(L, b, gx, y0 - 2, inx);
+        float x0a = cj.wD * cj.b, x0b = 0.0f, x0m = c1.wD * c1.b;  // rows y0-2, -, y0-3
+        c3 = c2;
+        c2 = c1;
+        c1 = cj;
+        x0b = x0m;
+        float x1a = 0.0f, x1b = 0.0f, part = 0.0f;
+        RowC nxt = load_row<TB>(L, b, gx, y0 - 1, inx);  // rows are fetched one iteration ahead
+        for (int j = y0 - 1; j <= y0 + kMH + 1; j++) {
+            cj = nxt;
+            if (j + 1 <= y0 + kMH + 1) nxt = load_row<TB>(L, b, gx, j + 1, inx);
+            const float x0j = cj.wD * cj.b;
+            // x1 at row j-1 (c1, x0a) from x0 at rows j-2 (x0b), j-1, j
+            const float ax0 = ax_row(c1, c2.aN, x0a, x0b, x0j);
+            const float x1n = x0a + c1.wD * (c1.b - ax0);
+            // residual at row j-2 (c2, x1a) from x1 at rows j-3 (x1b), j-2, j-1
+            if (j - 2 >= y0) {
+                const float ax1 = ax_row(c2, c3.aN, x1a, x1b, x1n);
+                const float r = c2.act ? c2.b - ax1 : 0.0f;
+                const float pr = r + __shfl_down_sync(0xffffffffu, r, 1);  // columns gx, gx + 1
+                const int gy = j - 2;
+                if ((gy & 1) == 0) {
+                    part = pr;
+                } else {
+                    const int I = gx >> 1, J = gy >> 1;
+                    if (out_lane && (lane & 1) == 0 && I < nxc && J < nyc) bc[(size_t)I + (size_t)J * nxc] = part + pr;
+                }
+            }
+            if (j - 1 >= y0 && j - 1 < y0 + kMH && j - 1 < L.ny && out_lane)
+                xo[(size_t)gx + (size_t)(j - 1) * L.nx] = x1n;
+            // shift the pipeline
+            c3 = c2;
+            c2 = c1;
+            c1 = cj;
+            x0b = x0a;
+            x0a = x0j;
+            x1b = x1a;
+            x1a = x1n;
+        }
+    }
+}
+
+// Ascending half: xt = xi + omega_c P xc, x2 = one sweep, then the second sweep; LAST (level 0)
+// writes z in Float64 and finishes the outer CG's r'z, r'r; otherwise writes the result to xo.
+template <typename TB, bool LAST>
+__global__ void __launch_bounds__(128) k_mg_up_m(Lv L, const TB *b, const float *xi, const float *xc, int nxc,
+                                                 float wc, float *xo, double *z, CgDev *cg, int init,
+                                                 double *partials, unsigned int *counter) {
+    if (cg_finished(L.done)) return;
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const int sxn = (L.nx + kMW - 1) / kMW, nstrips = sxn * ((L.ny + kMH - 1) / kMH);
+    double red[2] = {0.0, 0.0};
+    for (int st = blockIdx.x * wpb + (threadIdx.x >> 5); st < nstrips; st += gridDim.x * wpb) {
+        const int x0 = (st % sxn) * kMW, y0 = (st / sxn) * kMH;
+        const int gx = x0 - 2 + lane;
+        const bool inx = gx >= 0 && gx < L.nx, out_lane = lane >= 2 && lane < 2 + kMW && gx < L.nx;
+        // the fine iterate and the coarse value under this cell (0 outside the level)
+        auto fetch_x = [&](int gy, float &fi, float &co) {
+            fi = co = 0.0f;
+            if (!inx || gy < 0 || gy >= L.ny) return;
+            fi = xi[(size_t)gx + (size_t)gy * L.nx];
+            co = xc[(size_t)(gx >> 1) + (size_t)(gy >> 1) * nxc];
+        };
+        auto xt_of = [&](const RowC &c, float fi, float co) -> float {  // the prolonged fine iterate
+            float v = fi;
+            if (c.act) v += wc * co;
+            return v;
+        };
+        double bd = 0.0, bd1 = 0.0, bd2 = 0.0;  // Float64 rhs of rows j, j-1, j-2 (LAST)
+        float fi, co;
+        RowC c1 = load_row<TB>(L, b, gx, y0 - 3, inx, LAST ? &bd2 : nullptr), c2{}, c3{};
+        fetch_x(y0 - 3, fi, co);
+        float xtm = xt_of(c1, fi, co);
+        RowC cj = load_row<TB>(L, b, gx, y0 - 2, inx, LAST ? &bd1 : nullptr);
+        fetch_x(y0 - 2, fi, co);
+        float xta = xt_of(cj, fi, co), xtb = xtm;
+        c3 = c2;
+        c2 = c1;
+        c1 = cj;
+        float x2a = 0.0f, x2b = 0.0f;
+        double bdj1 = bd1, bdj2 = 0.0, bdn = 0.0;
+        // rows are fetched one iteration ahead
+        RowC nxt = load_row<TB>(L, b, gx, y0 - 1, inx, LAST ? &bdn : nullptr);
+        float fin, con;
+        fetch_x(y0 - 1, fin, con);
+        for (int j = y0 - 1; j <= y0 + kMH + 1; j++) {
+            cj = nxt;
+            bd = bdn;
+            fi = fin;
+            co = con;
+            if (j + 1 <= y0 + kMH + 1) {
+                nxt = load_row<TB>(L, b, gx, j + 1, inx, LAST ? &bdn : nullptr);
+                fetch_x(j + 1, fin, con);
+            }
+            const float xtj = xt_of(cj, fi, co);
+            // x2 at row j-1 from xt at rows j-2, j-1, j
+            const float axt = ax_row(c1, c2.aN, xta, xtb, xtj);
+            const float x2n = xta + c1.wD * (c1.b - axt);
+            // final sweep at row j-2 from x2 at rows j-3, j-2, j-1
+            if (j - 2 >= y0) {
+                const float ax2 = ax_row(c2, c3.aN, x2a, x2b, x2n);
+                const int gy = j - 2;
+                if (out_lane && gy < y0 + kMH && gy < L.ny) {
+                    const size_t q = (size_t)gx + (size_t)gy * L.nx;
+                    if (LAST) {
+                        const double rk = bdj2;
+                        const double zk = (double)(x2a + c2.wD * ((float)rk - ax2));
+                        z[q] = zk;
+                        red[0] += rk * zk;
+                        red[1] += rk * rk;
+                    } else {
+                        xo[q] = x2a + c2.wD * (c2.b - ax2);
+                    }
+                }
+            }
+            c3 = c2;
+            c2 = c1;
+            c1 = cj;
+            xtb = xta;
+            xta = xtj;
+            x2b = x2a;
+            x2a = x2n;
+            if (LAST) {
+                bdj2 = bdj1;
+                bdj1 = bd;
+            }
+        }
+    }
+    if (LAST) {
+        double out[2];
+        if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
+            if (init) cg_init_finish(cg, out[0], cg->rr, cg->bnorm);
+            else cg_iter_finish(cg, out[0], out[1]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Bottom of the V-cycle in one block: every level from `lb` down to the 1 x 1 coarsest level lives
 // in shared memory (29 bytes per cell: aE, aN, dP, wD, x, scratch, b and the activity flag); the
 // block runs the same pre-smoothing / restriction / exact solve / prolongation / post-smoothing
@@ -518,7 +717,15 @@ static Lv level_view(const MgLevel &m, const int *done) {
 }
 
 // The fused two-sweep level kernels serve nu = 2 (the default); other nu use the per-sweep kernels.
+// Among the fused kernels, the tile ones are the default (SHK_MG_FUSED=1); the warp-marching ones
+// (SHK_MG_FUSED=2) are the alternative (at 4096^2 one V-cycle-preconditioned CG iteration takes
+// 959 us with the tile kernels, 1044 us with the marching ones).
 static bool fused(const Ctx *c) { return c->mg_fused && c->mg_nu == 2; }
+static bool marching(const Ctx *c) { return fused(c) && c->mg_fused == 2; }
+static int march_grid(const Ctx *c, const MgLevel &m) {
+    const long long strips = (long long)((m.nx + kMW - 1) / kMW) * ((m.ny + kMH - 1) / kMH);
+    return (int)std::max(1LL, std::min((strips + 3) / 4, (long long)c->max_blocks));
+}
 static int fused_grid(const Ctx *c, const MgLevel &m) {
     const long long tiles = (long long)((m.nx + kFW - 1) / kFW) * ((m.ny + kFH - 1) / kFH);
     // one resident wave (six 256-thread blocks per SM), striding over the tiles
@@ -600,6 +807,19 @@ static int vcycle(Ctx *c, int l, const int *done, int *res) {
         return SHK_OK;
     }
     MgLevel &g = c->mg[l + 1];
+    if (marching(c)) {
+        const int gm = march_grid(c, m);
+        k_mg_down_m<float><<<gm, 128, 0, c->stream>>>(L, m.b, m.x[0], g.nx, g.ny, g.b);
+        c->launches++;
+        int gres = 0;
+        int rc = vcycle(c, l + 1, done, &gres);
+        if (rc) return rc;
+        k_mg_up_m<float, false><<<gm, 128, 0, c->stream>>>(L, m.b, m.x[0], g.x[gres], g.nx, wc, m.x[1], nullptr,
+                                                           nullptr, 0, nullptr, nullptr);
+        c->launches++;
+        *res = 1;
+        return SHK_OK;
+    }
     if (fused(c)) {
         const int gt = fused_grid(c, m);
         k_mg_down<float><<<gt, 256, 0, c->stream>>>(L, m.b, m.x[0], g.nx, g.ny, g.b);
@@ -647,6 +867,18 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
         return check_launch(c, "multigrid apply");
     }
     MgLevel &g = c->mg[1];
+    if (marching(c)) {
+        const int gm = march_grid(c, m);
+        k_mg_down_m<double><<<gm, 128, 0, c->stream>>>(L, r, m.x[0], g.nx, g.ny, g.b);
+        c->launches++;
+        int gres = 0;
+        int rc = vcycle(c, 1, &cg->done, &gres);
+        if (rc) return rc;
+        k_mg_up_m<double, true><<<gm, 128, 0, c->stream>>>(L, r, m.x[0], g.x[gres], g.nx, wc, nullptr, z, cg, init,
+                                                           c->partials, c->counter);
+        c->launches++;
+        return check_launch(c, "multigrid apply");
+    }
     if (fused(c)) {
         const int gt = fused_grid(c, m);
         k_mg_down<double><<<gt, 256, 0, c->stream>>>(L, r, m.x[0], g.nx, g.ny, g.b);

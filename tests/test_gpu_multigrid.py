@@ -1,9 +1,10 @@
 """GPU checks of the multigrid preconditioner's kernel variants and of the CG launch modes.
 
- - The fused two-sweep level kernels (one kernel per half V-cycle level, halo staged in shared
-   memory) against the per-sweep kernels: the V-cycle output is the same arithmetic, so CG iterates
-   agree to the rounding of the r'z reduction order (1e-12), and full solves take the same number
-   of iterations (+-1).
+ - The fused two-sweep level kernels (one kernel per half V-cycle level: 2D tiles with the halo
+   staged in shared memory, or warps marching down 32-column strips) against the per-sweep kernels: the same V-cycle, formed with differently contracted
+   Float32 multiply-adds, so CG iterates agree to Float32 rounding after 8 iterations (1e-6; an
+   indexing error would show at O(1)), and full solves take the same number of iterations (+-1)
+   and agree within the rel-res 1e-8 error ball.
  - The three ways of issuing CG iterations (direct launches, one CUDA graph per iteration, the whole
    loop as a graph with a device-side WHILE node) run the same kernels in the same order: bit-equal
    solutions and equal iteration counts.
@@ -42,17 +43,18 @@ def solve(shk, w, env, monkeypatch, itmax=0, rtol=1e-8, multigrid=True):
     return h, stats
 
 
-def test_fused_level_kernels_match_per_sweep_kernels(shk, cuda, monkeypatch):
+@pytest.mark.parametrize("variant", ["1", "2"], ids=["tile", "warp_marching"])
+def test_fused_level_kernels_match_per_sweep_kernels(shk, cuda, monkeypatch, variant):
     w = ragged_workload(shk)
-    h_f, st_f = solve(shk, w, {"SHK_MG_FUSED": "1"}, monkeypatch, itmax=8, rtol=0.0)
+    h_f, st_f = solve(shk, w, {"SHK_MG_FUSED": variant}, monkeypatch, itmax=8, rtol=0.0)
     h_u, st_u = solve(shk, w, {"SHK_MG_FUSED": "0"}, monkeypatch, itmax=8, rtol=0.0)
     assert st_f.niter == st_u.niter == 8
-    assert relerr(h_f, h_u) <= 1e-12, relerr(h_f, h_u)
-    h_f, st_f = solve(shk, w, {"SHK_MG_FUSED": "1"}, monkeypatch)
+    assert relerr(h_f, h_u) <= 1e-6, relerr(h_f, h_u)
+    h_f, st_f = solve(shk, w, {"SHK_MG_FUSED": variant}, monkeypatch)
     h_u, st_u = solve(shk, w, {"SHK_MG_FUSED": "0"}, monkeypatch)
     assert st_f.status == st_u.status == 0
     assert abs(st_f.niter - st_u.niter) <= 1, (st_f.niter, st_u.niter)
-    assert relerr(h_f, h_u) <= 1e-9
+    assert relerr(h_f, h_u) <= 1e-7
 
 
 @pytest.mark.parametrize("multigrid", [True, False], ids=["multigrid", "jacobi"])
