@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--ws-instances", type=int, default=96)
     ap.add_argument("--ws-steps", type=int, default=48)
     ap.add_argument("--ws-train", type=int, default=4000)
+    ap.add_argument("--nn-infer", type=int, default=0,
+                    help="profiling case: this many forward passes of the (untrained) warm-start network on a "
+                         "packed 2048^2 state, then exit")
     ap.add_argument("--profile-cg", type=int, default=0,
                     help="profiling case: initialise the workload, assemble once and run exactly this many CG "
                          "iterations of each form, then exit")
@@ -741,8 +744,26 @@ def warmstart_bench(args):
     return line
 
 
+def nn_infer(args):
+    """Small, self-ending case for ncu: forward passes of the warm-start network at 2048^2."""
+    import torch
+    shk = entry.load_package()
+    from shakti_b200 import warmstart as ws
+    net = ws.WarmStartNet(seed=0)
+    sim = ws.member_sim(shk, dict(nx=2048, seed=556, slope=0.018, melt=8e-8, C=4e4, b0=0.007))
+    X = net.pack(sim.state)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.nn_infer):
+        net.forward(X)
+    torch.cuda.synchronize()
+    print(json.dumps({"nn_infer": args.nn_infer, "ms": round((time.perf_counter() - t0) * 1e3, 3)}))
+
+
 def main():
     args = parse()
+    if args.nn_infer:
+        return nn_infer(args)
     if args.warmstart:
         line = warmstart_bench(args)
         s = json.dumps(line)
