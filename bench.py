@@ -34,9 +34,10 @@ import __graft_entry__ as entry  # noqa: E402
 METRIC = "converged timesteps/s at 4096² (rel-res 1e-8), chosen form vs plain FP64 GPU CG"
 UNIT = "timesteps/s"
 # Algorithmic bytes per cell of one CG iteration.  Jacobi (Float64): k_cg_A reads aP, aE, aN, r,
-# p_old and writes p_new, Ap; k_cg_B reads aP, p_new, Ap, x, r and writes x, r (14 words).  With a
-# separate preconditioner, k_cg_A reads z instead of r (7 words) and k_cg_B does not read aP (6).
-CG_BYTES = {"plain": 14 * 8, "fp32cg": 14 * 4, "multigrid": 13 * 8}
+# p_old and writes p_new, Ap; k_cg_B reads aP, p_new, Ap, x, r and writes x, r (14 words).  With the
+# multigrid preconditioner, k_cg_A reads z instead of r (7 words) and the x/r update is counted
+# with the V-cycle's first kernel (mg_vcycle_bytes).
+CG_BYTES = {"plain": 14 * 8, "fp32cg": 14 * 4, "multigrid": 7 * 8}
 FORMS = {"multigrid": "Float64 CG + Float32 aggregation-multigrid V-cycle preconditioner",
          "plain": "Float64 CG, Jacobi (the reference algorithm)",
          "fp32cg": "Float32 Jacobi CG with Float64 residual replacement"}
@@ -218,9 +219,10 @@ def run_steps(shk, sim, n, record=None):
 def mg_vcycle_bytes(nx, ny, fused=True):
     """Algorithmic bytes of one V-cycle (all levels, nu = 2 sweeps per side).
     Fused level kernels (the default): level 0 (Float64 residual in, Float64 z out), per fine cell,
-    descending half 30 B (r 8, activity flag 1, operator aP dP aE aN 16 in; x 4, coarse rhs 1 out)
-    and ascending half 38 B (x 4, coarse x 1, flag 1, operator 16, r 8 in; z 8 out); each coarse
-    level above the bottom, per cell, 26 + 30 B (Float32 rhs).  Per-sweep kernels: level 0
+    descending half 70 B with the CG's x/r update folded in (r, Ap, p, x 32 B, activity flag 1,
+    operator wD dP aE aN 16 in; new r 8, x 8, the level's iterate 4, coarse rhs 1 out) and
+    ascending half 38 B (iterate 4, coarse iterate 1, flag 1, operator 16, r 8 in; z 8 out); each
+    coarse level above the bottom, per cell, 26 + 30 B (Float32 rhs).  Per-sweep kernels: level 0
     17 + 33 + 26 + 34 + 37 B, coarse levels 13 + 29 + 22 + 30 + 29 B.  The levels that fit in one
     block's shared memory (29 B per cell, 200 KiB) are read once (operator 17 B + rhs 4 B per
     cell) and level lb's result written once (4 B per cell)."""
@@ -236,7 +238,7 @@ def mg_vcycle_bytes(nx, ny, fused=True):
         if rest * 29 > 200 * 1024:
             break
         lb = l
-    top, coarse = (68, 56) if fused else (147, 123)
+    top, coarse = (108, 56) if fused else (147 + 48, 123)  # per-sweep: plus k_cg_B's 48 B
     total = top * cells[0] if len(dims) > 1 else 37 * cells[0]
     for l in range(1, lb):
         total += coarse * cells[l]

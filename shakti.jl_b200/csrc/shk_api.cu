@@ -64,7 +64,7 @@ static int ctx_alloc(Ctx *c) {
     size_t o_mask8 = carve(n);
     size_t o_aP = carve(dN), o_aE = carve(dN), o_aN = carve(dN), o_rhs = carve(dN);
     size_t o_x = carve(dN), o_r = carve(dN), o_z = carve(dN), o_p0 = carve(dN), o_p1 = carve(dN), o_Ap = carve(dN);
-    size_t o_hprev = carve(dN);
+    size_t o_hprev = carve(dN), o_r2 = carve(dN);
     size_t o_cr0 = carve(dN), o_cr1 = carve(dN), o_cp0 = carve(dN), o_cp1 = carve(dN);
     size_t o_f[16];
     for (int i = 0; i < 16; i++) o_f[i] = carve(fN);
@@ -93,6 +93,7 @@ static int ctx_alloc(Ctx *c) {
     c->x = (double *)(b + o_x); c->r = (double *)(b + o_r); c->z = (double *)(b + o_z);
     c->p[0] = (double *)(b + o_p0); c->p[1] = (double *)(b + o_p1); c->Ap = (double *)(b + o_Ap);
     c->h_prev = (double *)(b + o_hprev);
+    c->r2 = (double *)(b + o_r2);
     c->cr[0] = (double *)(b + o_cr0); c->cr[1] = (double *)(b + o_cr1);
     c->cp[0] = (double *)(b + o_cp0); c->cp[1] = (double *)(b + o_cp1);
     float **fl[16] = {&c->aP32, &c->aE32, &c->aN32, &c->b32, &c->x32, &c->r32, &c->z32, &c->p32[0], &c->p32[1],

@@ -118,6 +118,7 @@ struct Ctx {
     uint8_t *mask8 = nullptr;
     double *aP = nullptr, *aE = nullptr, *aN = nullptr, *rhs = nullptr;
     double *x = nullptr, *r = nullptr, *z = nullptr, *p[2] = {nullptr, nullptr}, *Ap = nullptr;
+    double *r2 = nullptr;  // second residual buffer: the multigrid form's fused x/r update alternates
     double *h_prev = nullptr;
     double *cr[2] = {nullptr, nullptr}, *cp[2] = {nullptr, nullptr}; // Chebyshev r/p buffers
     double *r64 = nullptr;                                            // mixed: outer residual
@@ -239,5 +240,8 @@ void ens_cg_cond(cudaStream_t s, EnsInst *E, EnsCtl *ctl, int n, cudaGraphCondit
 int mg_levels_for(int nx, int ny, int *dims, int maxl);
 int mg_setup(Ctx *c);
 int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init);
+bool mg_fuses_cg_update(const Ctx *c);
+int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, const double *p, const double *Ap,
+                          double *z, CgDev *cg);
 
 } // namespace shk

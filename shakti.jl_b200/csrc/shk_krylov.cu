@@ -860,6 +860,10 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
 
     // One CG iteration: stencil + p update + p'Ap (k_cg_A), x/r update (k_cg_B), preconditioner.
     // Every kernel returns at once when the device-side stop flag is set.
+    // Multigrid (tile form): k_cg_B's x/r update runs inside the V-cycle's first kernel, which
+    // writes the new residual to the other of two buffers (r and r2 alternate with the p parity).
+    bool fuse_update = false;
+    if constexpr (std::is_same<T, double>::value) fuse_update = mg && mg_fuses_cg_update(c);
     auto enqueue_iteration = [&](int par) -> int {
         T *p_old = p[par], *p_new = p[par ^ 1];
         if (jac && lapl) {
@@ -877,6 +881,13 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
             k_cg_A<T, false><<<c->march_blocks, kMarchX, 0, c->stream>>>(nx, ny, c->march_th, aP, aE, aN, r, z, p_old,
                                                                         p_new, Ap, cgd, c->partials, c->counter,
                                                                         eps_curv);
+        }
+        if constexpr (std::is_same<T, double>::value) {
+            if (fuse_update) {
+                T *rb[2] = {r, c->r2};
+                c->launches += 1;
+                return mg_apply_fused_update(c, rb[par], rb[par ^ 1], x, p_new, Ap, z, cgd);
+            }
         }
         if (jac)
             k_cg_B<T, true><<<stream_grid(c, n, sizeof(T)), kThreads, 0, c->stream>>>(n, aP, p_new, Ap, x, r, cgd,

@@ -268,14 +268,31 @@ __device__ __forceinline__ float ax_sm(const FusedSm &S, const float (&X)[kFSH][
 // keep every lane busy; the divisions are by a compile-time constant.)
 // X0 (the first iterate over the whole region) is formed in the same pass: DOWN, the first sweep
 // from zero, wD b; UP, the fine iterate plus the prolonged coarse correction.
-template <typename TB, bool UP>
+// FB (level 0 of an iteration): the outer CG's x/r update (k_cg_B's arithmetic, unfused) is done
+// here: the staged rhs is r_new = r + (-alpha) Ap, and the tile's own cells write r_new to the
+// other r buffer (never the one neighbouring blocks read) and x += alpha p.
+struct FusedB {
+    const double *Ap, *p;
+    double *x, *r_out;
+    double alpha;
+};
+
+template <typename TB, bool UP, bool FB = false>
 __device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b, int x0, int y0, double *r64,
-                                            const float *xi, const float *xc, int nxc, float wc) {
+                                            const float *xi, const float *xc, int nxc, float wc,
+                                            const FusedB *fb = nullptr) {
     for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
         const int hx = k % kFSW, hy = k / kFSW, gx = x0 - kFR + hx, gy = y0 - kFR + hy;
         if (gx >= 0 && gx < L.nx && gy >= 0 && gy < L.ny) {
             const size_t q = (size_t)gx + (size_t)gy * L.nx;
-            const TB bq = b[q];
+            TB bq = b[q];
+            if constexpr (FB) {
+                bq = __dadd_rn(bq, __dmul_rn(-fb->alpha, fb->Ap[q]));
+                if (hx >= kFR && hx < kFR + kFW && hy >= kFR && hy < kFR + kFH) {
+                    fb->r_out[q] = bq;
+                    fb->x[q] = __dadd_rn(fb->x[q], __dmul_rn(fb->alpha, fb->p[q]));
+                }
+            }
             if (r64) r64[k] = (double)bq;
             const float bf = (float)bq, wd = L.wD[q];
             const uint8_t a = L.act[q];
@@ -317,15 +334,22 @@ __device__ __forceinline__ void sweep_sm(FusedSm &S, const float (&XI)[kFSH][kFS
 
 // Descending half of level L: x1 = two sweeps from zero (written to xo), and the coarse rhs
 // bc = restriction of b - A x1.  1D grid striding over 32 x 16 tiles.
-template <typename TB>
-__global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo, int nxc, int nyc, float *bc) {
-    if (cg_finished(L.done)) return;
+template <typename TB, bool FB = false>
+__global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo, int nxc, int nyc, float *bc,
+                                                    FusedB fbv = FusedB{}, const CgDev *cg = nullptr) {
+    if constexpr (FB) {
+        const CgView cv = block_cg_view(cg);
+        if (cv.done) return;
+        fbv.alpha = cv.alpha;
+    } else {
+        if (cg_finished(L.done)) return;
+    }
     __shared__ FusedSm S;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // output rows: 32 x 8 threads
     const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
-        stage_level<TB, false>(S, L, b, x0, y0, nullptr, nullptr, nullptr, 0, 0.0f);
+        stage_level<TB, false, FB>(S, L, b, x0, y0, nullptr, nullptr, nullptr, 0, 0.0f, &fbv);
         __syncthreads();
         sweep_sm(S, S.x0, S.x1);
         __syncthreads();
@@ -915,6 +939,29 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
                                                          c->counter);
         c->launches += c->mg_nu;
     }
+    return check_launch(c, "multigrid apply");
+}
+
+// One iteration's x/r update fused into the V-cycle's first level-0 kernel (tile form, nu = 2):
+// r_new = r_in - alpha Ap into r_out, x += alpha p, then z = M^-1 r_new and the CG's r'z, r'r.
+bool mg_fuses_cg_update(const Ctx *c) { return marching(c) ? false : fused(c) && c->mg_levels > 1; }
+
+int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, const double *p, const double *Ap,
+                          double *z, CgDev *cg) {
+    MgLevel &m = c->mg[0];
+    const Lv L = level_view(m, &cg->done);
+    MgLevel &g = c->mg[1];
+    const float wc = c->mg_omega_c;
+    const int gt = fused_grid(c, m);
+    k_mg_down<double, true><<<gt, 256, 0, c->stream>>>(L, r_in, m.x[0], g.nx, g.ny, g.b,
+                                                        FusedB{Ap, p, x, r_out, 0.0}, cg);
+    c->launches++;
+    int gres = 0;
+    int rc = vcycle(c, 1, &cg->done, &gres);
+    if (rc) return rc;
+    k_mg_up<double, true><<<gt, 256, 0, c->stream>>>(L, r_out, m.x[0], g.x[gres], g.nx, wc, nullptr, z, cg, 0,
+                                                     c->partials, c->counter);
+    c->launches++;
     return check_launch(c, "multigrid apply");
 }
 
