@@ -207,6 +207,7 @@ SHK_API int shk_create(int nx, int ny, double lx, double ly, void *stream, void 
     if (const char *v = getenv("SHK_MG_OMEGA")) c->mg_omega = (float)atof(v);
     if (const char *v = getenv("SHK_MG_OMEGA_C")) c->mg_omega_c = (float)atof(v);
     if (const char *v = getenv("SHK_MG_FUSED")) c->mg_fused = std::min(2, std::max(0, atoi(v)));
+    if (const char *v = getenv("SHK_MG_TMA")) c->mg_tma = atoi(v) != 0;
     // SHK_CG_GRAPHS: 0 issues each CG iteration's kernels directly, 1 replays one CUDA graph per
     // iteration in host-sized batches, 2 (default) runs the whole iteration loop as one graph with a
     // device-side WHILE node
@@ -235,6 +236,7 @@ SHK_API int shk_destroy(void *ctx) {
     for (auto &g : c->graphs) cudaGraphExecDestroy(g.exec);
     c->graphs.clear();
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+    mg_release(c);
     if (c->arena) cudaFree(c->arena);
     if (c->host_dev) cudaFreeHost(c->host_dev);
     delete c;

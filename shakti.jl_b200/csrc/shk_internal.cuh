@@ -49,6 +49,7 @@ struct CgDev {
     int done, status, first, stop_rule;
     int cont;        // init continues the previous search direction instead of restarting
     unsigned int trips;  // trips of the device-side iteration loop (bounded)
+    int fault;           // set by a kernel whose bounded wait for a tile copy ran out
 };
 
 struct ChebDev {
@@ -135,6 +136,8 @@ struct Ctx {
     float mg_omega = 0.8f;   // Jacobi damping
     float mg_omega_c = 1.0f; // coarse-correction scaling
     int mg_fused = 1;        // nu = 2 level kernels: 1 tile (default), 2 warp-marching, 0 per-sweep
+    int mg_tma = 1;          // tile kernels stage through TMA copies where the level's pitch allows
+    struct MgTma *mg_maps = nullptr;  // the levels' tensor maps (built on first use)
     int max_blocks = 0;
     int grid_stencil = 0;    // blocks for tile-stride kernels
     int march_th = 8;        // row-marching tile height
@@ -239,6 +242,7 @@ void ens_cg_cond(cudaStream_t s, EnsInst *E, EnsCtl *ctl, int n, cudaGraphCondit
 // shk_mg.cu
 int mg_levels_for(int nx, int ny, int *dims, int maxl);
 int mg_setup(Ctx *c);
+void mg_release(Ctx *c);
 int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init);
 bool mg_fuses_cg_update(const Ctx *c);
 int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, const double *p, const double *Ap,

@@ -1083,6 +1083,7 @@ int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
         if ((rc = check_launch(c, "cg finish"))) return rc;
         if ((rc = read_scalars(c))) return rc;
         const CgDev &g = c->host_dev->cg;
+        if (g.fault) return fail(c, SHK_CUDA_ERROR, "multigrid: a tile copy did not complete (bounded wait ran out)");
         s.niter = (long)g.iter;
         s.status = g.status;
         s.rnorm0 = g.rnorm0;

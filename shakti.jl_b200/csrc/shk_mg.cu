@@ -14,6 +14,7 @@
 // sweeps before and after the coarse correction; exact solve on the 1x1 coarsest level), so it is
 // a valid CG preconditioner.  Per level: nu damped-Jacobi sweeps (omega) before and after, coarse
 // correction scaled by omega_c; the levels that fit in one block's shared memory run as one kernel.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <float.h>
 #include <string.h>
@@ -427,6 +428,292 @@ __global__ void __launch_bounds__(256, 6) k_mg_up(Lv L, const TB *b, const float
 }
 
 // ---------------------------------------------------------------------------------------------
+// TMA-staged tile kernels (the default where every array of the level has a 16-byte-multiple
+// row pitch).  Same tiles, sweeps and expressions as the kernels above -- the same V-cycle bit
+// for bit -- but a block's staged region arrives by 2D tensor copies (cp.async.bulk.tensor) into
+// one of two shared-memory stages, completing on that stage's mbarrier: while the block smooths
+// tile t, the copies of its next tile t + gridDim.x are in flight, so each SM keeps several tiles'
+// bytes moving instead of stalling on every staging load.  Cells outside the level arrive as
+// zeros (the copies' out-of-bounds fill), as the staging loops above write them.
+// Box origins keep the innermost coordinate x 16-byte aligned: Float64 boxes start 2 columns
+// left of the tile (36 wide), Float32 boxes 4 (40 wide), the uint8 activity box 16 (64 wide); the
+// coarse iterate box covers the tile's aggregates from 4 coarse columns left (24 x 10).
+// ---------------------------------------------------------------------------------------------
+constexpr int kTFW = kFSW + 4, kTOff = 2;     // Float32 boxes: 40 wide, staged hx = 0 at column 2
+constexpr int kTAW = 64, kTAOff = 14;         // activity box: 64 wide, staged hx = 0 at column 14
+constexpr int kTCW = 24, kTCH = 10;           // coarse iterate box
+constexpr long kTmaSpin = 1L << 22;           // try_wait polls before a wait gives up
+
+struct TmaArgs {  // the launch's tensor maps (kernel parameters, one 128-byte descriptor each)
+    CUtensorMap b, ap, wD, dP, aE, aN, act, xi, xc;
+};
+
+__device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void tma_bar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tma_expect(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(su32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(su32(bar))
+        : "memory");
+}
+
+// Bounded wait for the stage's phase `parity`; false when the polls ran out.
+__device__ __forceinline__ bool tma_wait(uint64_t *bar, uint32_t parity) {
+    for (long i = 0; i < kTmaSpin; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(su32(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// Shared-memory layout of one launch: two stages of boxes, then the Float32 rhs and the two
+// iterates over the staged region, then the stages' mbarriers.  Box offsets are 128-byte aligned.
+template <typename TB, bool UP, bool FB>
+struct TLayout {
+    static constexpr unsigned rnd(unsigned v) { return (v + 127u) & ~127u; }
+    static constexpr int bW = sizeof(TB) == 8 ? kFSW : kTFW, bOff = sizeof(TB) == 8 ? 0 : kTOff;
+    static constexpr unsigned bB = bW * kFSH * sizeof(TB), apB = FB ? kFSW * kFSH * 8 : 0;
+    static constexpr unsigned fB = kTFW * kFSH * 4, actB = kTAW * kFSH;
+    static constexpr unsigned xiB = UP ? fB : 0, xcB = UP ? kTCW * kTCH * 4 : 0;
+    static constexpr unsigned o_b = 0, o_ap = rnd(o_b + bB), o_wD = rnd(o_ap + apB), o_dP = rnd(o_wD + fB),
+                              o_aE = rnd(o_dP + fB), o_aN = rnd(o_aE + fB), o_act = rnd(o_aN + fB),
+                              o_xi = rnd(o_act + actB), o_xc = rnd(o_xi + xiB), stage = rnd(o_xc + xcB);
+    static constexpr unsigned tx = bB + apB + 4 * fB + actB + xiB + xcB;  // bytes per stage fill
+    static constexpr unsigned o_bf = 2 * stage, o_x0 = o_bf + kFCells * 4, o_x1 = o_x0 + kFCells * 4,
+                              o_bar = rnd(o_x1 + kFCells * 4), bytes = o_bar + 16;
+};
+
+// One stage's copies for the tile at (x0, y0) (issued by one thread).
+template <typename Y, bool UP, bool FB>
+__device__ __forceinline__ void tma_issue(const TmaArgs &M, unsigned char *st, uint64_t *bar, int x0, int y0) {
+    tma_expect(bar, Y::tx);
+    tma_load(st + Y::o_b, &M.b, bar, x0 - kFR - Y::bOff, y0 - kFR);
+    if (FB) tma_load(st + Y::o_ap, &M.ap, bar, x0 - kFR, y0 - kFR);
+    tma_load(st + Y::o_wD, &M.wD, bar, x0 - kFR - kTOff, y0 - kFR);
+    tma_load(st + Y::o_dP, &M.dP, bar, x0 - kFR - kTOff, y0 - kFR);
+    tma_load(st + Y::o_aE, &M.aE, bar, x0 - kFR - kTOff, y0 - kFR);
+    tma_load(st + Y::o_aN, &M.aN, bar, x0 - kFR - kTOff, y0 - kFR);
+    tma_load(st + Y::o_act, &M.act, bar, x0 - kFR - kTAOff, y0 - kFR);
+    if (UP) {
+        tma_load(st + Y::o_xi, &M.xi, bar, x0 - kFR - kTOff, y0 - kFR);
+        tma_load(st + Y::o_xc, &M.xc, bar, x0 / 2 - 4, y0 / 2 - 1);
+    }
+}
+
+// The staged operator of one stage (Float32 boxes pre-offset so that [hy * kTFW + hx] is staged
+// position (hx, hy), as is [hy * kTAW + hx] of the activity box).
+struct TOp {
+    const float *wD, *dP, *aE, *aN;
+    const uint8_t *act;
+};
+
+template <typename Y>
+__device__ __forceinline__ TOp stage_op(const unsigned char *st) {
+    return TOp{reinterpret_cast<const float *>(st + Y::o_wD) + kTOff,
+               reinterpret_cast<const float *>(st + Y::o_dP) + kTOff,
+               reinterpret_cast<const float *>(st + Y::o_aE) + kTOff,
+               reinterpret_cast<const float *>(st + Y::o_aN) + kTOff,
+               reinterpret_cast<const uint8_t *>(st + Y::o_act) + kTAOff};
+}
+
+// ax_sm's expression on the staged boxes.
+__device__ __forceinline__ float ax_t(const TOp &O, const float (*X)[kFSW], int hx, int hy) {
+    const int o = hy * kTFW + hx;
+    const float xc = X[hy][hx];
+    float y = O.dP[o] * xc;
+    y += O.aE[o] * (xc - X[hy][hx + 1]);
+    y += O.aE[o - 1] * (xc - X[hy][hx - 1]);
+    y += O.aN[o] * (xc - X[hy + 1][hx]);
+    y += O.aN[o - kTFW] * (xc - X[hy - 1][hx]);
+    return y;
+}
+
+__device__ __forceinline__ void sweep_t(const TOp &O, const float (*B)[kFSW], const float (*XI)[kFSW],
+                                        float (*XO)[kFSW]) {
+    constexpr int wdt = kFW + 2, hgt = kFH + 2;
+    for (int k = threadIdx.x; k < wdt * hgt; k += blockDim.x) {
+        const int hx = kFR - 1 + k % wdt, hy = kFR - 1 + k / wdt;
+        XO[hy][hx] = XI[hy][hx] + O.wD[hy * kTFW + hx] * (B[hy][hx] - ax_t(O, XI, hx, hy));
+    }
+}
+
+// Records a failed wait (the solve stops and reports it) after waiting, bounded, for the copies
+// still in flight into the other stage.
+__device__ __forceinline__ void tma_give_up(CgDev *cg, uint64_t *other, uint32_t parity, bool pending) {
+    if (threadIdx.x == 0) {
+        if (pending) tma_wait(other, parity);
+        cg->fault = 1;
+        atomicExch(&cg->done, 1);
+    }
+}
+
+// Common frame of the two kernels: barrier set-up, the first tile's copies, and per tile the next
+// tile's copies, the wait, and BODY(stage, tile origin).
+template <typename Y, bool UP, bool FB, typename Body>
+__device__ __forceinline__ void tma_tiles(const TmaArgs &M, const Lv &L, unsigned char *sm, CgDev *cg, Body body) {
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Y::o_bar);
+    const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
+    if (su32(sm) & 127u) {  // the boxes' 128-byte alignment is not met: no copy is issued
+        tma_give_up(cg, &bar[0], 0, false);
+        return;
+    }
+    if (threadIdx.x == 0) {
+        tma_bar_init(&bar[0]);
+        tma_bar_init(&bar[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if ((int)blockIdx.x < ntiles)
+            tma_issue<Y, UP, FB>(M, sm, &bar[0], ((int)blockIdx.x % tiles_x) * kFW, ((int)blockIdx.x / tiles_x) * kFH);
+    }
+    __syncthreads();
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+        const int s = it & 1, tn = t + gridDim.x;
+        if (threadIdx.x == 0 && tn < ntiles) {
+            // the other stage was last read before the previous tile's closing barrier
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tma_issue<Y, UP, FB>(M, sm + (s ^ 1) * Y::stage, &bar[s ^ 1], (tn % tiles_x) * kFW, (tn / tiles_x) * kFH);
+        }
+        const bool ok = tma_wait(&bar[s], (it >> 1) & 1);
+        if (__syncthreads_or(!ok)) {
+            tma_give_up(cg, &bar[s ^ 1], ((it + 1) >> 1) & 1, tn < ntiles);
+            return;
+        }
+        body(sm + s * Y::stage, (t % tiles_x) * kFW, (t / tiles_x) * kFH);
+        __syncthreads();  // the stage and the staged arrays are reused
+    }
+}
+
+// k_mg_down on TMA-staged tiles.
+template <typename TB, bool FB>
+__global__ void __launch_bounds__(256, 3) k_mg_down_t(const __grid_constant__ TmaArgs M, Lv L, float *xo, int nxc,
+                                                      int nyc, float *bc, FusedB fbv, CgDev *cg) {
+    if constexpr (FB) {
+        const CgView cv = block_cg_view(cg);
+        if (cv.done) return;
+        fbv.alpha = cv.alpha;
+    } else {
+        if (cg_finished(L.done)) return;
+    }
+    using Y = TLayout<TB, false, FB>;
+    extern __shared__ __align__(128) unsigned char sm[];
+    float(*BF)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_bf);
+    float(*X0)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_x0);
+    float(*X1)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_x1);
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    tma_tiles<Y, false, FB>(M, L, sm, cg, [&](unsigned char *st, int x0, int y0) {
+        const TB *SB = reinterpret_cast<const TB *>(st + Y::o_b) + Y::bOff;
+        const TOp O = stage_op<Y>(st);
+        for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
+            const int hx = k % kFSW, hy = k / kFSW;
+            TB bq = SB[hy * Y::bW + hx];
+            if constexpr (FB) {
+                const double *AP = reinterpret_cast<const double *>(st + Y::o_ap);
+                bq = __dadd_rn(bq, __dmul_rn(-fbv.alpha, AP[k]));
+                const int gx = x0 - kFR + hx, gy = y0 - kFR + hy;
+                if (hx >= kFR && hx < kFR + kFW && hy >= kFR && hy < kFR + kFH && gx < L.nx && gy < L.ny) {
+                    const size_t q = (size_t)gx + (size_t)gy * L.nx;
+                    fbv.r_out[q] = bq;
+                    fbv.x[q] = __dadd_rn(fbv.x[q], __dmul_rn(fbv.alpha, fbv.p[q]));
+                }
+            }
+            const float bf = (float)bq;
+            BF[hy][hx] = bf;
+            X0[hy][hx] = O.wD[hy * kTFW + hx] * bf;
+        }
+        __syncthreads();
+        sweep_t(O, BF, X0, X1);
+        __syncthreads();
+        for (int r = ty; r < kFH; r += 8) {
+            const int gx = x0 + tx, gy = y0 + r, hx = tx + kFR, hy = r + kFR;
+            if (gx < L.nx && gy < L.ny) xo[(size_t)gx + (size_t)gy * L.nx] = X1[hy][hx];
+            X0[hy][hx] = O.act[hy * kTAW + hx] ? BF[hy][hx] - ax_t(O, X1, hx, hy) : 0.0f;
+        }
+        __syncthreads();
+        if (threadIdx.x < (kFW / 2) * (kFH / 2)) {
+            const int ai = threadIdx.x % (kFW / 2), aj = threadIdx.x / (kFW / 2);
+            const int I = x0 / 2 + ai, J = y0 / 2 + aj;
+            if (I < nxc && J < nyc) {
+                const int hx = 2 * ai + kFR, hy = 2 * aj + kFR;
+                float sres = 0.0f;
+                sres += X0[hy][hx];
+                sres += X0[hy][hx + 1];
+                sres += X0[hy + 1][hx];
+                sres += X0[hy + 1][hx + 1];
+                bc[(size_t)I + (size_t)J * nxc] = sres;
+            }
+        }
+    });
+}
+
+// k_mg_up on TMA-staged tiles.
+template <typename TB, bool LAST>
+__global__ void __launch_bounds__(256, 3) k_mg_up_t(const __grid_constant__ TmaArgs M, Lv L, float wc, float *xo,
+                                                    double *z, CgDev *cg, int init, double *partials,
+                                                    unsigned int *counter) {
+    if (cg_finished(L.done)) return;
+    using Y = TLayout<TB, true, false>;
+    extern __shared__ __align__(128) unsigned char sm[];
+    float(*BF)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_bf);
+    float(*X0)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_x0);
+    float(*X1)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_x1);
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double red[2] = {0.0, 0.0};
+    tma_tiles<Y, true, false>(M, L, sm, cg, [&](unsigned char *st, int x0, int y0) {
+        const TB *SB = reinterpret_cast<const TB *>(st + Y::o_b) + Y::bOff;
+        const TOp O = stage_op<Y>(st);
+        const float *XI = reinterpret_cast<const float *>(st + Y::o_xi) + kTOff;
+        const float *XC = reinterpret_cast<const float *>(st + Y::o_xc);
+        for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
+            const int hx = k % kFSW, hy = k / kFSW;
+            BF[hy][hx] = (float)SB[hy * Y::bW + hx];
+            float v = XI[hy * kTFW + hx];
+            if (O.act[hy * kTAW + hx]) v += wc * XC[(1 + ((hy - kFR) >> 1)) * kTCW + 4 + ((hx - kFR) >> 1)];
+            X0[hy][hx] = v;
+        }
+        __syncthreads();
+        sweep_t(O, BF, X0, X1);
+        __syncthreads();
+        for (int r = ty; r < kFH; r += 8) {
+            const int gx = x0 + tx, gy = y0 + r;
+            if (gx >= L.nx || gy >= L.ny) continue;
+            const int hx = tx + kFR, hy = r + kFR;
+            const float ax = ax_t(O, X1, hx, hy);
+            const size_t q = (size_t)gx + (size_t)gy * L.nx;
+            const float wd = O.wD[hy * kTFW + hx];
+            if (LAST) {
+                const double rk = (double)SB[hy * Y::bW + hx];
+                const double zk = (double)(X1[hy][hx] + wd * ((float)rk - ax));
+                z[q] = zk;
+                red[0] += rk * zk;
+                red[1] += rk * rk;
+            } else {
+                xo[q] = X1[hy][hx] + wd * (BF[hy][hx] - ax);
+            }
+        }
+    });
+    if (LAST) {
+        double out[2];
+        if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
+            if (init) cg_init_finish(cg, out[0], cg->rr, cg->bnorm);
+            else cg_iter_finish(cg, out[0], out[1]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Warp-marching level kernels (SHK_MG_FUSED=2).  A warp owns a strip of 32 columns (lanes
 // 2..29 are its 28 output columns; lanes 0, 1, 30, 31 the halo the two sweeps need) and marches
 // down kMH rows plus two halo rows each side.  Each row is loaded once (coalesced), the two sweeps
@@ -781,6 +1068,9 @@ static size_t bottom_plan(const Ctx *c, int lb, BottomPlan *P) {
     return (size_t)off * kBottomBytesPerCell;
 }
 
+struct MgTma;
+static MgTma *tma_maps(Ctx *c, int *rc);
+
 // Rebuilds every level's operator from the assembled Float64 system (after k_to_float_lapl).
 int mg_setup(Ctx *c) {
     if (c->mg_levels < 1) return fail(c, SHK_CUDA_ERROR, "multigrid hierarchy not allocated");
@@ -812,13 +1102,153 @@ int mg_setup(Ctx *c) {
             if (e != cudaSuccess) return check_cuda(c, e, "multigrid bottom shared memory");
             attr_set[c->device] = true;
         }
+        if (fused(c) && !marching(c)) {  // tensor maps and kernel attributes, outside any capture
+            int rc = SHK_OK;
+            tma_maps(c, &rc);
+            if (rc) return rc;
+        }
     }
     return check_launch(c, "multigrid setup");
 }
 
+// Tensor maps of the TMA-staged tile kernels, built once per context at the first multigrid set-up
+// (outside any stream capture; the arrays live in the context's arena for its lifetime).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+struct MgTma {
+    bool ok[kMgMaxLevels] = {};  // level l's tile kernels stage through TMA
+    CUtensorMap wD[kMgMaxLevels], dP[kMgMaxLevels], aE[kMgMaxLevels], aN[kMgMaxLevels], act[kMgMaxLevels];
+    CUtensorMap b[kMgMaxLevels], xi[kMgMaxLevels];
+    CUtensorMap xc[kMgMaxLevels][2];  // level l's two iterates as coarse boxes (read by level l - 1)
+    CUtensorMap r, r2, Ap;            // level 0's Float64 vectors
+    int grid[5] = {};                 // per kernel: blocks of one resident wave
+};
+
+enum { TK_DOWN0, TK_DOWN0_FB, TK_DOWN, TK_UP0, TK_UP };
+
+static bool encode(EncodeTiledFn fn, CUtensorMap *m, CUtensorMapDataType dt, size_t esz, const void *base, int nx,
+                   int ny, int bw, int bh) {
+    if (!base || (uintptr_t)base % 16 || ((size_t)nx * esz) % 16) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)ny};
+    const cuuint64_t strides[1] = {(cuuint64_t)nx * esz};
+    const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh}, es[2] = {1, 1};
+    return fn(m, dt, 2, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename K>
+static int tma_kernel_bps(Ctx *c, K kernel, unsigned smem, int *blocks_per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return check_cuda(c, e, "multigrid TMA kernel shared memory");
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, 256, smem);
+    if (e != cudaSuccess) return check_cuda(c, e, "multigrid TMA kernel occupancy");
+    return SHK_OK;
+}
+
+void mg_release(Ctx *c) {
+    delete c->mg_maps;
+    c->mg_maps = nullptr;
+}
+
+// The maps, or nullptr when the TMA kernels are off or no level qualifies.
+static MgTma *tma_maps(Ctx *c, int *rc) {
+    *rc = SHK_OK;
+    if (!c->mg_tma || c->mg_levels < 2) return nullptr;
+    if (c->mg_maps) return c->mg_maps;
+    void *fp = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fp, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fp) {
+        cudaGetLastError();
+        c->mg_tma = 0;  // no driver entry point: the LDG-staged tile kernels serve every level
+        return nullptr;
+    }
+    const EncodeTiledFn fn = (EncodeTiledFn)fp;
+    MgTma *T = new MgTma();
+    const CUtensorMapDataType F32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32, F64 = CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                              U8 = CU_TENSOR_MAP_DATA_TYPE_UINT8;
+    const int lb = bottom_level(c);
+    bool any = false;
+    for (int l = 0; l < lb; l++) {
+        const MgLevel &m = c->mg[l], &g = c->mg[l + 1];
+        if (m.nx % 16 || g.nx % 4) continue;
+        bool ok = encode(fn, &T->wD[l], F32, 4, m.wD, m.nx, m.ny, kTFW, kFSH) &&
+                  encode(fn, &T->dP[l], F32, 4, m.dP, m.nx, m.ny, kTFW, kFSH) &&
+                  encode(fn, &T->aE[l], F32, 4, m.aE, m.nx, m.ny, kTFW, kFSH) &&
+                  encode(fn, &T->aN[l], F32, 4, m.aN, m.nx, m.ny, kTFW, kFSH) &&
+                  encode(fn, &T->act[l], U8, 1, m.act, m.nx, m.ny, kTAW, kFSH) &&
+                  encode(fn, &T->xi[l], F32, 4, m.x[0], m.nx, m.ny, kTFW, kFSH) &&
+                  encode(fn, &T->xc[l + 1][0], F32, 4, g.x[0], g.nx, g.ny, kTCW, kTCH) &&
+                  encode(fn, &T->xc[l + 1][1], F32, 4, g.x[1], g.nx, g.ny, kTCW, kTCH);
+        if (l == 0)
+            ok = ok && encode(fn, &T->r, F64, 8, c->r, m.nx, m.ny, kFSW, kFSH) &&
+                 encode(fn, &T->r2, F64, 8, c->r2, m.nx, m.ny, kFSW, kFSH) &&
+                 encode(fn, &T->Ap, F64, 8, c->Ap, m.nx, m.ny, kFSW, kFSH);
+        else
+            ok = ok && encode(fn, &T->b[l], F32, 4, m.b, m.nx, m.ny, kTFW, kFSH);
+        T->ok[l] = ok;
+        any = any || ok;
+    }
+    if (!any) {
+        delete T;
+        c->mg_tma = 0;
+        return nullptr;
+    }
+    int bps[5] = {};
+    int e = tma_kernel_bps(c, k_mg_down_t<double, false>, TLayout<double, false, false>::bytes, &bps[TK_DOWN0]);
+    if (!e) e = tma_kernel_bps(c, k_mg_down_t<double, true>, TLayout<double, false, true>::bytes, &bps[TK_DOWN0_FB]);
+    if (!e) e = tma_kernel_bps(c, k_mg_down_t<float, false>, TLayout<float, false, false>::bytes, &bps[TK_DOWN]);
+    if (!e) e = tma_kernel_bps(c, k_mg_up_t<double, true>, TLayout<double, true, false>::bytes, &bps[TK_UP0]);
+    if (!e) e = tma_kernel_bps(c, k_mg_up_t<float, false>, TLayout<float, true, false>::bytes, &bps[TK_UP]);
+    if (e) {
+        delete T;
+        *rc = e;
+        return nullptr;
+    }
+    for (int k = 0; k < 5; k++) {
+        if (bps[k] < 1) {
+            delete T;
+            *rc = fail(c, SHK_CUDA_ERROR, "multigrid TMA kernel does not fit on an SM");
+            return nullptr;
+        }
+        T->grid[k] = c->num_sms * bps[k];
+    }
+    c->mg_maps = T;
+    return T;
+}
+
+static int tma_grid(const Ctx *c, const MgTma *T, int kind, const MgLevel &m) {
+    const long long tiles = (long long)((m.nx + kFW - 1) / kFW) * ((m.ny + kFH - 1) / kFH);
+    return (int)std::max(1LL, std::min({tiles, (long long)c->max_blocks, (long long)T->grid[kind]}));
+}
+
+static TmaArgs tma_args(const MgTma *T, int l, const CUtensorMap &b, const CUtensorMap *ap, const CUtensorMap *xc) {
+    TmaArgs a;
+    memset(&a, 0, sizeof(a));
+    a.b = b;
+    if (ap) a.ap = *ap;
+    a.wD = T->wD[l];
+    a.dP = T->dP[l];
+    a.aE = T->aE[l];
+    a.aN = T->aN[l];
+    a.act = T->act[l];
+    a.xi = T->xi[l];
+    if (xc) a.xc = *xc;
+    return a;
+}
+
+// Level 0's residual map for a CG residual buffer (nullptr: not one of the context's buffers).
+static const CUtensorMap *r_map(const Ctx *c, const MgTma *T, const double *r) {
+    return r == c->r ? &T->r : r == c->r2 ? &T->r2 : nullptr;
+}
+
 // Recursive V-cycle on level l >= 1 with rhs lv[l].b; the solution ends in lv[l].x[*res].
-static int vcycle(Ctx *c, int l, const int *done, int *res) {
+static int vcycle(Ctx *c, int l, CgDev *cg, int *res) {
     MgLevel &m = c->mg[l];
+    const int *done = &cg->done;
     const Lv L = level_view(m, done);
     const float wc = c->mg_omega_c;
     if (l == bottom_level(c)) {
@@ -836,10 +1266,27 @@ static int vcycle(Ctx *c, int l, const int *done, int *res) {
         k_mg_down_m<float><<<gm, 128, 0, c->stream>>>(L, m.b, m.x[0], g.nx, g.ny, g.b);
         c->launches++;
         int gres = 0;
-        int rc = vcycle(c, l + 1, done, &gres);
+        int rc = vcycle(c, l + 1, cg, &gres);
         if (rc) return rc;
         k_mg_up_m<float, false><<<gm, 128, 0, c->stream>>>(L, m.b, m.x[0], g.x[gres], g.nx, wc, m.x[1], nullptr,
                                                            nullptr, 0, nullptr, nullptr);
+        c->launches++;
+        *res = 1;
+        return SHK_OK;
+    }
+    int trc = SHK_OK;
+    const MgTma *T = fused(c) ? tma_maps(c, &trc) : nullptr;
+    if (trc) return trc;
+    if (T && T->ok[l]) {
+        const int gd = tma_grid(c, T, TK_DOWN, m), gu = tma_grid(c, T, TK_UP, m);
+        k_mg_down_t<float, false><<<gd, 256, TLayout<float, false, false>::bytes, c->stream>>>(
+            tma_args(T, l, T->b[l], nullptr, nullptr), L, m.x[0], g.nx, g.ny, g.b, FusedB{}, cg);
+        c->launches++;
+        int gres = 0;
+        int rc = vcycle(c, l + 1, cg, &gres);
+        if (rc) return rc;
+        k_mg_up_t<float, false><<<gu, 256, TLayout<float, true, false>::bytes, c->stream>>>(
+            tma_args(T, l, T->b[l], nullptr, &T->xc[l + 1][gres]), L, wc, m.x[1], nullptr, cg, 0, nullptr, nullptr);
         c->launches++;
         *res = 1;
         return SHK_OK;
@@ -849,7 +1296,7 @@ static int vcycle(Ctx *c, int l, const int *done, int *res) {
         k_mg_down<float><<<gt, 256, 0, c->stream>>>(L, m.b, m.x[0], g.nx, g.ny, g.b);
         c->launches++;
         int gres = 0;
-        int rc = vcycle(c, l + 1, done, &gres);
+        int rc = vcycle(c, l + 1, cg, &gres);
         if (rc) return rc;
         k_mg_up<float, false><<<gt, 256, 0, c->stream>>>(L, m.b, m.x[0], g.x[gres], g.nx, wc, m.x[1], nullptr,
                                                          nullptr, 0, nullptr, nullptr);
@@ -865,7 +1312,7 @@ static int vcycle(Ctx *c, int l, const int *done, int *res) {
     k_mg_restrict<float><<<gc, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], g.nx, g.ny, g.b);
     c->launches += 1 + c->mg_nu;
     int gres = 0;
-    int rc = vcycle(c, l + 1, done, &gres);
+    int rc = vcycle(c, l + 1, cg, &gres);
     if (rc) return rc;
     k_mg_prolong_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], g.x[gres], g.nx, wc,
                                                               m.x[cur ^ 1]);
@@ -896,10 +1343,27 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
         k_mg_down_m<double><<<gm, 128, 0, c->stream>>>(L, r, m.x[0], g.nx, g.ny, g.b);
         c->launches++;
         int gres = 0;
-        int rc = vcycle(c, 1, &cg->done, &gres);
+        int rc = vcycle(c, 1, cg, &gres);
         if (rc) return rc;
         k_mg_up_m<double, true><<<gm, 128, 0, c->stream>>>(L, r, m.x[0], g.x[gres], g.nx, wc, nullptr, z, cg, init,
                                                            c->partials, c->counter);
+        c->launches++;
+        return check_launch(c, "multigrid apply");
+    }
+    int trc = SHK_OK;
+    const MgTma *T = fused(c) ? tma_maps(c, &trc) : nullptr;
+    if (trc) return trc;
+    if (T && T->ok[0] && r_map(c, T, r)) {
+        const int gd = tma_grid(c, T, TK_DOWN0, m), gu = tma_grid(c, T, TK_UP0, m);
+        k_mg_down_t<double, false><<<gd, 256, TLayout<double, false, false>::bytes, c->stream>>>(
+            tma_args(T, 0, *r_map(c, T, r), nullptr, nullptr), L, m.x[0], g.nx, g.ny, g.b, FusedB{}, cg);
+        c->launches++;
+        int gres = 0;
+        int rc = vcycle(c, 1, cg, &gres);
+        if (rc) return rc;
+        k_mg_up_t<double, true><<<gu, 256, TLayout<double, true, false>::bytes, c->stream>>>(
+            tma_args(T, 0, *r_map(c, T, r), nullptr, &T->xc[1][gres]), L, wc, nullptr, z, cg, init, c->partials,
+            c->counter);
         c->launches++;
         return check_launch(c, "multigrid apply");
     }
@@ -908,7 +1372,7 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
         k_mg_down<double><<<gt, 256, 0, c->stream>>>(L, r, m.x[0], g.nx, g.ny, g.b);
         c->launches++;
         int gres = 0;
-        int rc = vcycle(c, 1, &cg->done, &gres);
+        int rc = vcycle(c, 1, cg, &gres);
         if (rc) return rc;
         k_mg_up<double, true><<<gt, 256, 0, c->stream>>>(L, r, m.x[0], g.x[gres], g.nx, wc, nullptr, z, cg, init,
                                                          c->partials, c->counter);
@@ -923,7 +1387,7 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
     k_mg_restrict<double><<<gc, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], g.nx, g.ny, g.b);
     c->launches += 1 + c->mg_nu;
     int gres = 0;
-    int rc = vcycle(c, 1, &cg->done, &gres);
+    int rc = vcycle(c, 1, cg, &gres);
     if (rc) return rc;
     if (c->mg_nu == 1) {
         k_mg_last<true><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[cur], g.x[gres], g.nx, wc, z, cg, init,
@@ -952,12 +1416,30 @@ int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, 
     const Lv L = level_view(m, &cg->done);
     MgLevel &g = c->mg[1];
     const float wc = c->mg_omega_c;
+    int trc = SHK_OK;
+    const MgTma *T = tma_maps(c, &trc);
+    if (trc) return trc;
+    if (T && T->ok[0] && r_map(c, T, r_in) && r_map(c, T, r_out) && Ap == c->Ap) {
+        const int gd = tma_grid(c, T, TK_DOWN0_FB, m), gu = tma_grid(c, T, TK_UP0, m);
+        k_mg_down_t<double, true><<<gd, 256, TLayout<double, false, true>::bytes, c->stream>>>(
+            tma_args(T, 0, *r_map(c, T, r_in), &T->Ap, nullptr), L, m.x[0], g.nx, g.ny, g.b,
+            FusedB{Ap, p, x, r_out, 0.0}, cg);
+        c->launches++;
+        int gres = 0;
+        int rc = vcycle(c, 1, cg, &gres);
+        if (rc) return rc;
+        k_mg_up_t<double, true><<<gu, 256, TLayout<double, true, false>::bytes, c->stream>>>(
+            tma_args(T, 0, *r_map(c, T, r_out), nullptr, &T->xc[1][gres]), L, wc, nullptr, z, cg, 0, c->partials,
+            c->counter);
+        c->launches++;
+        return check_launch(c, "multigrid apply");
+    }
     const int gt = fused_grid(c, m);
     k_mg_down<double, true><<<gt, 256, 0, c->stream>>>(L, r_in, m.x[0], g.nx, g.ny, g.b,
                                                         FusedB{Ap, p, x, r_out, 0.0}, cg);
     c->launches++;
     int gres = 0;
-    int rc = vcycle(c, 1, &cg->done, &gres);
+    int rc = vcycle(c, 1, cg, &gres);
     if (rc) return rc;
     k_mg_up<double, true><<<gt, 256, 0, c->stream>>>(L, r_out, m.x[0], g.x[gres], g.nx, wc, nullptr, z, cg, 0,
                                                      c->partials, c->counter);

@@ -5,6 +5,10 @@
    Float32 multiply-adds, so CG iterates agree to Float32 rounding after 8 iterations (1e-6; an
    indexing error would show at O(1)), and full solves take the same number of iterations (+-1)
    and agree within the rel-res 1e-8 error ball.
+ - The TMA-staged tile kernels (levels whose rows have a 16-byte-multiple pitch) against the
+   LDG-staged ones: the same V-cycle arithmetic; only the outer CG's dot products are summed over a
+   different block count, so iterates agree to Float64 rounding (1e-9 after 8 iterations; a
+   staging error would show at O(1)).
  - The three ways of issuing CG iterations (direct launches, one CUDA graph per iteration, the whole
    loop as a graph with a device-side WHILE node) run the same kernels in the same order: bit-equal
    solutions and equal iteration counts.
@@ -24,6 +28,14 @@ def ragged_workload(shk):
     # 301 x 301: odd sizes on every level, tiles cut by the domain edge, LAND/OTHER_BASIN blobs
     # (identity rows) and moulins; several levels above the one-block bottom of the V-cycle
     return shk.configs.seasonal(301, 15e3, seed=4242, C=0.25)
+
+
+def tma_workload(shk, nx, ny):
+    # nx a multiple of 16: level 0 (and, for 512, levels 1-2) stage through TMA; ny = 360 leaves
+    # ragged tile rows on every level, nx = 400 ragged tile columns; LAND/OTHER_BASIN blobs
+    w = shk.configs.plain(nx, 20e3, seed=777, ny=ny, ly=20e3 * (ny - 1) / (nx - 1), C=0.25)
+    shk.configs._paint_blobs(w.inputs["mask"], np.random.default_rng(778), 0.1, 2, 6)
+    return w
 
 
 def solve(shk, w, env, monkeypatch, itmax=0, rtol=1e-8, multigrid=True):
@@ -61,6 +73,29 @@ def test_fused_level_kernels_match_per_sweep_kernels(shk, cuda, monkeypatch, var
 def test_cg_launch_modes_are_bit_identical(shk, cuda, monkeypatch, multigrid):
     w = ragged_workload(shk)
     out = [solve(shk, w, {"SHK_CG_GRAPHS": m}, monkeypatch, multigrid=multigrid) for m in ("0", "1", "2")]
+    (h0, s0), (h1, s1), (h2, s2) = out
+    assert s0.status == s1.status == s2.status == 0
+    assert s0.niter == s1.niter == s2.niter
+    assert np.array_equal(h0, h1) and np.array_equal(h0, h2)
+
+
+@pytest.mark.parametrize("nx", [512, 400])
+def test_tma_tile_kernels_match_ldg_tile_kernels(shk, cuda, monkeypatch, nx):
+    w = tma_workload(shk, nx, 360)
+    h_t, st_t = solve(shk, w, {"SHK_MG_TMA": "1"}, monkeypatch, itmax=8, rtol=0.0)
+    h_l, st_l = solve(shk, w, {"SHK_MG_TMA": "0"}, monkeypatch, itmax=8, rtol=0.0)
+    assert st_t.niter == st_l.niter == 8
+    assert relerr(h_t, h_l) <= 1e-9, relerr(h_t, h_l)
+    h_t, st_t = solve(shk, w, {"SHK_MG_TMA": "1"}, monkeypatch)
+    h_l, st_l = solve(shk, w, {"SHK_MG_TMA": "0"}, monkeypatch)
+    assert st_t.status == st_l.status == 0
+    assert abs(st_t.niter - st_l.niter) <= 1, (st_t.niter, st_l.niter)
+    assert relerr(h_t, h_l) <= 1e-7
+
+
+def test_cg_launch_modes_are_bit_identical_tma(shk, cuda, monkeypatch):
+    w = tma_workload(shk, 512, 360)
+    out = [solve(shk, w, {"SHK_CG_GRAPHS": m}, monkeypatch) for m in ("0", "1", "2")]
     (h0, s0), (h1, s1), (h2, s2) = out
     assert s0.status == s1.status == s2.status == 0
     assert s0.niter == s1.niter == s2.niter
