@@ -254,13 +254,16 @@ struct FusedSm {
 // couplings across the level's edge are zero in every assembled and coarsened operator (the
 // east/north entries of the last column/row, and the staged zeros outside the level), so those
 // terms add 0 * (finite) = 0.
+// The tile kernels spell out every rounding (one multiply, then one fused multiply-add per
+// coupling), so that their two staging forms -- these LDG ones and the TMA ones below, which work
+// on packed pairs -- compute the same V-cycle bit for bit.
 __device__ __forceinline__ float ax_sm(const FusedSm &S, const float (&X)[kFSH][kFSW], int hx, int hy) {
     const float xc = X[hy][hx];
-    float y = S.dP[hy][hx] * xc;
-    y += S.aE[hy][hx] * (xc - X[hy][hx + 1]);
-    y += S.aE[hy][hx - 1] * (xc - X[hy][hx - 1]);
-    y += S.aN[hy][hx] * (xc - X[hy + 1][hx]);
-    y += S.aN[hy - 1][hx] * (xc - X[hy - 1][hx]);
+    float y = __fmul_rn(S.dP[hy][hx], xc);
+    y = __fmaf_rn(S.aE[hy][hx], __fsub_rn(xc, X[hy][hx + 1]), y);
+    y = __fmaf_rn(S.aE[hy][hx - 1], __fsub_rn(xc, X[hy][hx - 1]), y);
+    y = __fmaf_rn(S.aN[hy][hx], __fsub_rn(xc, X[hy + 1][hx]), y);
+    y = __fmaf_rn(S.aN[hy - 1][hx], __fsub_rn(xc, X[hy - 1][hx]), y);
     return y;
 }
 
@@ -305,10 +308,10 @@ __device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b
             S.act[hy][hx] = a;
             if (UP) {
                 float v = xi[q];
-                if (a) v += wc * xc[(size_t)(gx >> 1) + (size_t)(gy >> 1) * nxc];
+                if (a) v = __fmaf_rn(wc, xc[(size_t)(gx >> 1) + (size_t)(gy >> 1) * nxc], v);
                 S.x0[hy][hx] = v;
             } else {
-                S.x0[hy][hx] = wd * bf;
+                S.x0[hy][hx] = __fmul_rn(wd, bf);
             }
         } else {
             if (r64) r64[k] = 0.0;
@@ -329,7 +332,7 @@ __device__ __forceinline__ void sweep_sm(FusedSm &S, const float (&XI)[kFSH][kFS
     constexpr int wdt = kFW + 2, hgt = kFH + 2;
     for (int k = threadIdx.x; k < wdt * hgt; k += blockDim.x) {
         const int hx = kFR - 1 + k % wdt, hy = kFR - 1 + k / wdt;
-        XO[hy][hx] = XI[hy][hx] + S.wD[hy][hx] * (S.b[hy][hx] - ax_sm(S, XI, hx, hy));
+        XO[hy][hx] = __fmaf_rn(S.wD[hy][hx], __fsub_rn(S.b[hy][hx], ax_sm(S, XI, hx, hy)), XI[hy][hx]);
     }
 }
 
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo
         for (int r = ty; r < kFH; r += 8) {
             const int gx = x0 + tx, gy = y0 + r, hx = tx + kFR, hy = r + kFR;
             if (gx < L.nx && gy < L.ny) xo[(size_t)gx + (size_t)gy * L.nx] = S.x1[hy][hx];
-            S.x0[hy][hx] = S.act[hy][hx] ? S.b[hy][hx] - ax_sm(S, S.x1, hx, hy) : 0.0f;
+            S.x0[hy][hx] = S.act[hy][hx] ? __fsub_rn(S.b[hy][hx], ax_sm(S, S.x1, hx, hy)) : 0.0f;
         }
         __syncthreads();
         // restriction: one thread per aggregate of the tile (16 x 8 aggregates, 128 threads), in the
@@ -408,12 +411,12 @@ __global__ void __launch_bounds__(256, 6) k_mg_up(Lv L, const TB *b, const float
             const size_t q = (size_t)gx + (size_t)gy * L.nx;
             if (LAST) {
                 const double rk = r64[hy * kFSW + hx];
-                const double zk = (double)(S.x1[hy][hx] + S.wD[hy][hx] * ((float)rk - ax));
+                const double zk = (double)__fmaf_rn(S.wD[hy][hx], __fsub_rn((float)rk, ax), S.x1[hy][hx]);
                 z[q] = zk;
                 red[0] += rk * zk;
                 red[1] += rk * rk;
             } else {
-                xo[q] = S.x1[hy][hx] + S.wD[hy][hx] * (S.b[hy][hx] - ax);
+                xo[q] = __fmaf_rn(S.wD[hy][hx], __fsub_rn(S.b[hy][hx], ax), S.x1[hy][hx]);
             }
         }
         __syncthreads();
@@ -479,8 +482,8 @@ __device__ __forceinline__ bool tma_wait(uint64_t *bar, uint32_t parity) {
     return false;
 }
 
-// Shared-memory layout of one launch: two stages of boxes, then the Float32 rhs and the two
-// iterates over the staged region, then the stages' mbarriers.  Box offsets are 128-byte aligned.
+// Shared-memory layout of one launch: two stages of boxes, then the two iterates over the staged
+// region, then the stages' mbarriers.  Box offsets are 128-byte aligned.
 template <typename TB, bool UP, bool FB>
 struct TLayout {
     static constexpr unsigned rnd(unsigned v) { return (v + 127u) & ~127u; }
@@ -492,8 +495,8 @@ struct TLayout {
                               o_aE = rnd(o_dP + fB), o_aN = rnd(o_aE + fB), o_act = rnd(o_aN + fB),
                               o_xi = rnd(o_act + actB), o_xc = rnd(o_xi + xiB), stage = rnd(o_xc + xcB);
     static constexpr unsigned tx = bB + apB + 4 * fB + actB + xiB + xcB;  // bytes per stage fill
-    static constexpr unsigned o_bf = 2 * stage, o_x0 = o_bf + kFCells * 4, o_x1 = o_x0 + kFCells * 4,
-                              o_bar = rnd(o_x1 + kFCells * 4), bytes = o_bar + 16;
+    static constexpr unsigned o_x0 = 2 * stage, o_x1 = o_x0 + kFCells * 4, o_bar = rnd(o_x1 + kFCells * 4),
+                              bytes = o_bar + 16;
 };
 
 // One stage's copies for the tile at (x0, y0) (issued by one thread).
@@ -529,25 +532,71 @@ __device__ __forceinline__ TOp stage_op(const unsigned char *st) {
                reinterpret_cast<const uint8_t *>(st + Y::o_act) + kTAOff};
 }
 
-// ax_sm's expression on the staged boxes.
-__device__ __forceinline__ float ax_t(const TOp &O, const float (*X)[kFSW], int hx, int hy) {
-    const int o = hy * kTFW + hx;
-    const float xc = X[hy][hx];
-    float y = O.dP[o] * xc;
-    y += O.aE[o] * (xc - X[hy][hx + 1]);
-    y += O.aE[o - 1] * (xc - X[hy][hx - 1]);
-    y += O.aN[o] * (xc - X[hy + 1][hx]);
-    y += O.aN[o - kTFW] * (xc - X[hy - 1][hx]);
+// Work split of the TMA kernels: each thread owns horizontal pairs of staged cells (hx even) and
+// keeps their operator and rhs in registers across the prolongation, both sweeps and the residual;
+// only the iterates go through shared memory, as 64-bit words.  The arithmetic runs on packed
+// Float32 pairs (Blackwell's two-wide FMUL/FADD/FFMA), element for element the roundings of
+// ax_sm and sweep_sm.  Slot 0 of thread t is tile pair t (row 2 + t / 16, pair 1 + t % 16: a warp
+// holds one row of aggregates, so the restriction is a shuffle); slot 1 of threads t < 104 is one
+// of the 104 pairs of the two-cell ring around the tile.
+struct Pair {
+    int k, fo, ao;   // staged index of the first cell (row pitch kFSW), its Float32 and activity box index
+    bool sweep;      // in the sweeps' rows (1 .. kFH + 2); pairs at hx = 0 and 34 also compute their
+                     // outer cell, whose result nothing reads
+    float2 B, W, D, E, Ew, N, Ns;
+    bool a0, a1;     // activity of the two cells
+};
+
+__device__ __forceinline__ void pair_at(Pair &P, int row, int pr) {
+    P.k = row * kFSW + 2 * pr;
+    P.fo = row * kTFW + 2 * pr;
+    P.ao = row * kTAW + 2 * pr;
+    P.sweep = row >= kFR - 1 && row <= kFR + kFH;
+}
+
+// Slot 1: ring pair i (0 <= i < 104): rows 0, 1, 18, 19 (18 pairs each), then the first and last
+// pair of rows 2 .. 17.
+__device__ __forceinline__ void ring_pair_at(Pair &P, int i) {
+    constexpr int np = kFSW / 2;
+    if (i < 4 * np) {
+        const int r = i / np;
+        pair_at(P, r < 2 ? r : kFSH - 4 + r, i % np);
+    } else {
+        const int j = i - 4 * np;
+        pair_at(P, kFR + j / 2, (j % 2) * (np - 1));
+    }
+}
+constexpr int kRingPairs = 4 * (kFSW / 2) + 2 * kFH;  // 104
+
+__device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+
+__device__ __forceinline__ void pair_load(Pair &P, const TOp &O) {
+    P.W = ld2(O.wD + P.fo);
+    P.D = ld2(O.dP + P.fo);
+    P.E = ld2(O.aE + P.fo);
+    P.Ew = make_float2(O.aE[P.fo - 1], P.E.x);
+    P.N = ld2(O.aN + P.fo);
+    P.Ns = P.sweep ? ld2(O.aN + P.fo - kTFW) : make_float2(0.0f, 0.0f);
+    const uchar2 a = *reinterpret_cast<const uchar2 *>(O.act + P.ao);
+    P.a0 = a.x != 0;
+    P.a1 = a.y != 0;
+}
+
+// A X at the pair (ax_sm's roundings, elementwise).
+__device__ __forceinline__ float2 pair_ax(const Pair &P, const float *X) {
+    const float2 xc = ld2(X + P.k);
+    float2 y = __fmul2_rn(P.D, xc);
+    y = __ffma2_rn(P.E, sub2(xc, make_float2(xc.y, X[P.k + 2])), y);
+    y = __ffma2_rn(P.Ew, sub2(xc, make_float2(X[P.k - 1], xc.x)), y);
+    y = __ffma2_rn(P.N, sub2(xc, ld2(X + P.k + kFSW)), y);
+    y = __ffma2_rn(P.Ns, sub2(xc, ld2(X + P.k - kFSW)), y);
     return y;
 }
 
-__device__ __forceinline__ void sweep_t(const TOp &O, const float (*B)[kFSW], const float (*XI)[kFSW],
-                                        float (*XO)[kFSW]) {
-    constexpr int wdt = kFW + 2, hgt = kFH + 2;
-    for (int k = threadIdx.x; k < wdt * hgt; k += blockDim.x) {
-        const int hx = kFR - 1 + k % wdt, hy = kFR - 1 + k / wdt;
-        XO[hy][hx] = XI[hy][hx] + O.wD[hy * kTFW + hx] * (B[hy][hx] - ax_t(O, XI, hx, hy));
-    }
+__device__ __forceinline__ void pair_sweep(const Pair &P, const float *XI, float *XO) {
+    st2(XO + P.k, __ffma2_rn(P.W, sub2(P.B, pair_ax(P, XI)), ld2(XI + P.k)));
 }
 
 // Records a failed wait (the solve stops and reports it) after waiting, bounded, for the copies
@@ -561,9 +610,11 @@ __device__ __forceinline__ void tma_give_up(CgDev *cg, uint64_t *other, uint32_t
 }
 
 // Common frame of the two kernels: barrier set-up, the first tile's copies, and per tile the next
-// tile's copies, the wait, and BODY(stage, tile origin).
-template <typename Y, bool UP, bool FB, typename Body>
-__device__ __forceinline__ void tma_tiles(const TmaArgs &M, const Lv &L, unsigned char *sm, CgDev *cg, Body body) {
+// tile's copies, PRE(tile origin) (work that needs no staged data), the wait, and BODY(stage, tile
+// origin).
+template <typename Y, bool UP, bool FB, typename Pre, typename Body>
+__device__ __forceinline__ void tma_tiles(const TmaArgs &M, const Lv &L, unsigned char *sm, CgDev *cg, Pre pre,
+                                          Body body) {
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Y::o_bar);
     const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
     if (su32(sm) & 127u) {  // the boxes' 128-byte alignment is not met: no copy is issued
@@ -586,17 +637,30 @@ __device__ __forceinline__ void tma_tiles(const TmaArgs &M, const Lv &L, unsigne
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             tma_issue<Y, UP, FB>(M, sm + (s ^ 1) * Y::stage, &bar[s ^ 1], (tn % tiles_x) * kFW, (tn / tiles_x) * kFH);
         }
+        const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
+        pre(x0, y0);
         const bool ok = tma_wait(&bar[s], (it >> 1) & 1);
         if (__syncthreads_or(!ok)) {
             tma_give_up(cg, &bar[s ^ 1], ((it + 1) >> 1) & 1, tn < ntiles);
             return;
         }
-        body(sm + s * Y::stage, (t % tiles_x) * kFW, (t / tiles_x) * kFH);
+        body(sm + s * Y::stage, x0, y0);
         __syncthreads();  // the stage and the staged arrays are reused
     }
 }
 
-// k_mg_down on TMA-staged tiles.
+// The rhs pair at staged index k (Float64 boxes: pitch kFSW; Float32: kTFW, pre-offset).
+template <typename Y>
+__device__ __forceinline__ double2 rhs_pair(const double *SB, const Pair &P) {
+    return *reinterpret_cast<const double2 *>(SB + P.k);
+}
+template <typename Y>
+__device__ __forceinline__ double2 rhs_pair(const float *SB, const Pair &P) {
+    const float2 v = ld2(SB + P.fo);
+    return make_double2((double)v.x, (double)v.y);
+}
+
+// k_mg_down on TMA-staged tiles.  FB: x and p of the tile pair are read before the wait.
 template <typename TB, bool FB>
 __global__ void __launch_bounds__(256, 3) k_mg_down_t(const __grid_constant__ TmaArgs M, Lv L, float *xo, int nxc,
                                                       int nyc, float *bc, FusedB fbv, CgDev *cg) {
@@ -609,101 +673,138 @@ __global__ void __launch_bounds__(256, 3) k_mg_down_t(const __grid_constant__ Tm
     }
     using Y = TLayout<TB, false, FB>;
     extern __shared__ __align__(128) unsigned char sm[];
-    float(*BF)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_bf);
-    float(*X0)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_x0);
-    float(*X1)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_x1);
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    tma_tiles<Y, false, FB>(M, L, sm, cg, [&](unsigned char *st, int x0, int y0) {
-        const TB *SB = reinterpret_cast<const TB *>(st + Y::o_b) + Y::bOff;
-        const TOp O = stage_op<Y>(st);
-        for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
-            const int hx = k % kFSW, hy = k / kFSW;
-            TB bq = SB[hy * Y::bW + hx];
+    float *X0 = reinterpret_cast<float *>(sm + Y::o_x0);
+    float *X1 = reinterpret_cast<float *>(sm + Y::o_x1);
+    const int tid = threadIdx.x;
+    Pair P0, P1;
+    pair_at(P0, kFR + (tid >> 4), 1 + (tid & 15));
+    const bool has1 = tid < kRingPairs;
+    ring_pair_at(P1, has1 ? tid : 0);
+    const int gx0 = -kFR + 2 * (1 + (tid & 15)), gy0 = (tid >> 4);  // tile pair's offset from (x0, y0)
+    double2 xq = make_double2(0.0, 0.0), pq = xq;
+    bool inside = false;
+    size_t q = 0;
+    tma_tiles<Y, false, FB>(
+        M, L, sm, cg,
+        [&](int x0, int y0) {
+            const int gx = x0 + gx0, gy = y0 + gy0;
+            inside = gx < L.nx && gy < L.ny;  // nx is even: both cells of the pair, or neither
+            q = (size_t)gx + (size_t)gy * L.nx;
             if constexpr (FB) {
-                const double *AP = reinterpret_cast<const double *>(st + Y::o_ap);
-                bq = __dadd_rn(bq, __dmul_rn(-fbv.alpha, AP[k]));
-                const int gx = x0 - kFR + hx, gy = y0 - kFR + hy;
-                if (hx >= kFR && hx < kFR + kFW && hy >= kFR && hy < kFR + kFH && gx < L.nx && gy < L.ny) {
-                    const size_t q = (size_t)gx + (size_t)gy * L.nx;
-                    fbv.r_out[q] = bq;
-                    fbv.x[q] = __dadd_rn(fbv.x[q], __dmul_rn(fbv.alpha, fbv.p[q]));
+                if (inside) {
+                    xq = *reinterpret_cast<const double2 *>(fbv.x + q);
+                    pq = *reinterpret_cast<const double2 *>(fbv.p + q);
                 }
             }
-            const float bf = (float)bq;
-            BF[hy][hx] = bf;
-            X0[hy][hx] = O.wD[hy * kTFW + hx] * bf;
-        }
-        __syncthreads();
-        sweep_t(O, BF, X0, X1);
-        __syncthreads();
-        for (int r = ty; r < kFH; r += 8) {
-            const int gx = x0 + tx, gy = y0 + r, hx = tx + kFR, hy = r + kFR;
-            if (gx < L.nx && gy < L.ny) xo[(size_t)gx + (size_t)gy * L.nx] = X1[hy][hx];
-            X0[hy][hx] = O.act[hy * kTAW + hx] ? BF[hy][hx] - ax_t(O, X1, hx, hy) : 0.0f;
-        }
-        __syncthreads();
-        if (threadIdx.x < (kFW / 2) * (kFH / 2)) {
-            const int ai = threadIdx.x % (kFW / 2), aj = threadIdx.x / (kFW / 2);
-            const int I = x0 / 2 + ai, J = y0 / 2 + aj;
-            if (I < nxc && J < nyc) {
-                const int hx = 2 * ai + kFR, hy = 2 * aj + kFR;
-                float sres = 0.0f;
-                sres += X0[hy][hx];
-                sres += X0[hy][hx + 1];
-                sres += X0[hy + 1][hx];
-                sres += X0[hy + 1][hx + 1];
-                bc[(size_t)I + (size_t)J * nxc] = sres;
+        },
+        [&](unsigned char *st, int x0, int y0) {
+            const TB *SB = reinterpret_cast<const TB *>(st + Y::o_b) + Y::bOff;
+            const TOp O = stage_op<Y>(st);
+            auto prep = [&](Pair &P, bool tile) {
+                double2 bq = rhs_pair<Y>(SB, P);
+                if constexpr (FB) {
+                    const double2 ap = *reinterpret_cast<const double2 *>(
+                        reinterpret_cast<const double *>(st + Y::o_ap) + P.k);
+                    bq.x = __dadd_rn(bq.x, __dmul_rn(-fbv.alpha, ap.x));
+                    bq.y = __dadd_rn(bq.y, __dmul_rn(-fbv.alpha, ap.y));
+                    if (tile && inside) {
+                        *reinterpret_cast<double2 *>(fbv.r_out + q) = bq;
+                        *reinterpret_cast<double2 *>(fbv.x + q) =
+                            make_double2(__dadd_rn(xq.x, __dmul_rn(fbv.alpha, pq.x)),
+                                         __dadd_rn(xq.y, __dmul_rn(fbv.alpha, pq.y)));
+                    }
+                }
+                pair_load(P, O);
+                P.B = make_float2((float)bq.x, (float)bq.y);
+                st2(X0 + P.k, __fmul2_rn(P.W, P.B));
+            };
+            prep(P0, true);
+            if (has1) prep(P1, false);
+            __syncthreads();
+            pair_sweep(P0, X0, X1);
+            if (has1 && P1.sweep) pair_sweep(P1, X0, X1);
+            __syncthreads();
+            // residual of the tile pair (0 on inactive cells), x1 out, restriction by shuffle
+            const float2 ax = pair_ax(P0, X1);
+            const float2 x1 = ld2(X1 + P0.k);
+            if (inside) *reinterpret_cast<float2 *>(xo + q) = x1;
+            const float r0 = P0.a0 ? __fsub_rn(P0.B.x, ax.x) : 0.0f, r1 = P0.a1 ? __fsub_rn(P0.B.y, ax.y) : 0.0f;
+            const float u0 = __shfl_down_sync(0xffffffffu, r0, 16), u1 = __shfl_down_sync(0xffffffffu, r1, 16);
+            if ((tid & 16) == 0) {
+                const int I = x0 / 2 + (tid & 15), J = y0 / 2 + (tid >> 5);
+                if (I < nxc && J < nyc) {
+                    float sres = 0.0f;
+                    sres += r0;
+                    sres += r1;
+                    sres += u0;
+                    sres += u1;
+                    bc[(size_t)I + (size_t)J * nxc] = sres;
+                }
             }
-        }
-    });
+        });
 }
 
 // k_mg_up on TMA-staged tiles.
 template <typename TB, bool LAST>
-__global__ void __launch_bounds__(256, 3) k_mg_up_t(const __grid_constant__ TmaArgs M, Lv L, float wc, float *xo,
+__global__ void __launch_bounds__(256, 4) k_mg_up_t(const __grid_constant__ TmaArgs M, Lv L, float wc, float *xo,
                                                     double *z, CgDev *cg, int init, double *partials,
                                                     unsigned int *counter) {
     if (cg_finished(L.done)) return;
     using Y = TLayout<TB, true, false>;
     extern __shared__ __align__(128) unsigned char sm[];
-    float(*BF)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_bf);
-    float(*X0)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_x0);
-    float(*X1)[kFSW] = reinterpret_cast<float(*)[kFSW]>(sm + Y::o_x1);
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    float *X0 = reinterpret_cast<float *>(sm + Y::o_x0);
+    float *X1 = reinterpret_cast<float *>(sm + Y::o_x1);
+    const int tid = threadIdx.x;
+    Pair P0, P1;
+    pair_at(P0, kFR + (tid >> 4), 1 + (tid & 15));
+    const bool has1 = tid < kRingPairs;
+    ring_pair_at(P1, has1 ? tid : 0);
+    const int gx0 = -kFR + 2 * (1 + (tid & 15)), gy0 = (tid >> 4);
     double red[2] = {0.0, 0.0};
-    tma_tiles<Y, true, false>(M, L, sm, cg, [&](unsigned char *st, int x0, int y0) {
-        const TB *SB = reinterpret_cast<const TB *>(st + Y::o_b) + Y::bOff;
-        const TOp O = stage_op<Y>(st);
-        const float *XI = reinterpret_cast<const float *>(st + Y::o_xi) + kTOff;
-        const float *XC = reinterpret_cast<const float *>(st + Y::o_xc);
-        for (int k = threadIdx.x; k < kFCells; k += blockDim.x) {
-            const int hx = k % kFSW, hy = k / kFSW;
-            BF[hy][hx] = (float)SB[hy * Y::bW + hx];
-            float v = XI[hy * kTFW + hx];
-            if (O.act[hy * kTAW + hx]) v += wc * XC[(1 + ((hy - kFR) >> 1)) * kTCW + 4 + ((hx - kFR) >> 1)];
-            X0[hy][hx] = v;
-        }
-        __syncthreads();
-        sweep_t(O, BF, X0, X1);
-        __syncthreads();
-        for (int r = ty; r < kFH; r += 8) {
-            const int gx = x0 + tx, gy = y0 + r;
-            if (gx >= L.nx || gy >= L.ny) continue;
-            const int hx = tx + kFR, hy = r + kFR;
-            const float ax = ax_t(O, X1, hx, hy);
-            const size_t q = (size_t)gx + (size_t)gy * L.nx;
-            const float wd = O.wD[hy * kTFW + hx];
-            if (LAST) {
-                const double rk = (double)SB[hy * Y::bW + hx];
-                const double zk = (double)(X1[hy][hx] + wd * ((float)rk - ax));
-                z[q] = zk;
-                red[0] += rk * zk;
-                red[1] += rk * rk;
-            } else {
-                xo[q] = X1[hy][hx] + wd * (BF[hy][hx] - ax);
+    tma_tiles<Y, true, false>(
+        M, L, sm, cg, [&](int, int) {},
+        [&](unsigned char *st, int x0, int y0) {
+            const TB *SB = reinterpret_cast<const TB *>(st + Y::o_b) + Y::bOff;
+            const TOp O = stage_op<Y>(st);
+            const float *XI = reinterpret_cast<const float *>(st + Y::o_xi) + kTOff;
+            const float *XC = reinterpret_cast<const float *>(st + Y::o_xc);
+            auto prep = [&](Pair &P) {
+                const double2 bq = rhs_pair<Y>(SB, P);
+                pair_load(P, O);
+                P.B = make_float2((float)bq.x, (float)bq.y);
+                float2 v = ld2(XI + P.fo);
+                // both cells of a pair prolong from the same coarse cell
+                const int hx = P.k % kFSW, hy = P.k / kFSW;
+                const float c = XC[(1 + ((hy - kFR) >> 1)) * kTCW + 4 + ((hx - kFR) >> 1)];
+                if (P.a0) v.x = __fmaf_rn(wc, c, v.x);
+                if (P.a1) v.y = __fmaf_rn(wc, c, v.y);
+                st2(X0 + P.k, v);
+            };
+            prep(P0);
+            if (has1) prep(P1);
+            __syncthreads();
+            pair_sweep(P0, X0, X1);
+            if (has1 && P1.sweep) pair_sweep(P1, X0, X1);
+            __syncthreads();
+            const int gx = x0 + gx0, gy = y0 + gy0;
+            if (gx < L.nx && gy < L.ny) {
+                const float2 ax = pair_ax(P0, X1);
+                const float2 x1 = ld2(X1 + P0.k);
+                const size_t q = (size_t)gx + (size_t)gy * L.nx;
+                if (LAST) {
+                    const double2 rk = rhs_pair<Y>(SB, P0);
+                    const double z0 = (double)__fmaf_rn(P0.W.x, __fsub_rn((float)rk.x, ax.x), x1.x);
+                    const double z1 = (double)__fmaf_rn(P0.W.y, __fsub_rn((float)rk.y, ax.y), x1.y);
+                    *reinterpret_cast<double2 *>(z + q) = make_double2(z0, z1);
+                    red[0] += rk.x * z0;
+                    red[0] += rk.y * z1;
+                    red[1] += rk.x * rk.x;
+                    red[1] += rk.y * rk.y;
+                } else {
+                    *reinterpret_cast<float2 *>(xo + q) = __ffma2_rn(P0.W, sub2(P0.B, ax), x1);
+                }
             }
-        }
-    });
+        });
     if (LAST) {
         double out[2];
         if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {

@@ -6,9 +6,11 @@
    indexing error would show at O(1)), and full solves take the same number of iterations (+-1)
    and agree within the rel-res 1e-8 error ball.
  - The TMA-staged tile kernels (levels whose rows have a 16-byte-multiple pitch) against the
-   LDG-staged ones: the same V-cycle arithmetic; only the outer CG's dot products are summed over a
-   different block count, so iterates agree to Float64 rounding (1e-9 after 8 iterations; a
-   staging error would show at O(1)).
+   LDG-staged ones: the same V-cycle arithmetic, but the outer CG's dot products are summed over a
+   different block count.  After one iteration (h0 + alpha p0, p0 the V-cycle of the same r0) the
+   heads agree to Float64 rounding (1e-12); from the second iteration on, last-bit differences of
+   r flip Float32 roundings of the V-cycle's input, so after 8 iterations they agree to Float32
+   rounding (1e-6).  A staging error would show at O(1).
  - The three ways of issuing CG iterations (direct launches, one CUDA graph per iteration, the whole
    loop as a graph with a device-side WHILE node) run the same kernels in the same order: bit-equal
    solutions and equal iteration counts.
@@ -82,10 +84,14 @@ def test_cg_launch_modes_are_bit_identical(shk, cuda, monkeypatch, multigrid):
 @pytest.mark.parametrize("nx", [512, 400])
 def test_tma_tile_kernels_match_ldg_tile_kernels(shk, cuda, monkeypatch, nx):
     w = tma_workload(shk, nx, 360)
+    h_t, st_t = solve(shk, w, {"SHK_MG_TMA": "1"}, monkeypatch, itmax=1, rtol=0.0)
+    h_l, st_l = solve(shk, w, {"SHK_MG_TMA": "0"}, monkeypatch, itmax=1, rtol=0.0)
+    assert st_t.niter == st_l.niter == 1
+    assert relerr(h_t, h_l) <= 1e-12, relerr(h_t, h_l)
     h_t, st_t = solve(shk, w, {"SHK_MG_TMA": "1"}, monkeypatch, itmax=8, rtol=0.0)
     h_l, st_l = solve(shk, w, {"SHK_MG_TMA": "0"}, monkeypatch, itmax=8, rtol=0.0)
     assert st_t.niter == st_l.niter == 8
-    assert relerr(h_t, h_l) <= 1e-9, relerr(h_t, h_l)
+    assert relerr(h_t, h_l) <= 1e-6, relerr(h_t, h_l)
     h_t, st_t = solve(shk, w, {"SHK_MG_TMA": "1"}, monkeypatch)
     h_l, st_l = solve(shk, w, {"SHK_MG_TMA": "0"}, monkeypatch)
     assert st_t.status == st_l.status == 0
