@@ -245,6 +245,8 @@ int mg_setup(Ctx *c);
 void mg_release(Ctx *c);
 int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init);
 bool mg_fuses_cg_update(const Ctx *c);
+int mg_cg_matvec(Ctx *c, int par, const double *aP, const double *aE, const double *aN, const double *z,
+                 const double *p_old, double *p_new, double *Ap, CgDev *cg, double eps_curv, bool *launched);
 int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, const double *p, const double *Ap,
                           double *z, CgDev *cg);
 

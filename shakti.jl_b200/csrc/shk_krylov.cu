@@ -866,6 +866,18 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
     if constexpr (std::is_same<T, double>::value) fuse_update = mg && mg_fuses_cg_update(c);
     auto enqueue_iteration = [&](int par) -> int {
         T *p_old = p[par], *p_new = p[par ^ 1];
+        if constexpr (std::is_same<T, double>::value) {
+            if (fuse_update && !jac && !lapl) {
+                bool launched = false;
+                int rc = mg_cg_matvec(c, par, aP, aE, aN, z, p_old, p_new, Ap, cgd, eps_curv, &launched);
+                if (rc) return rc;
+                if (launched) {
+                    T *rb[2] = {r, c->r2};
+                    c->launches += 1;
+                    return mg_apply_fused_update(c, rb[par], rb[par ^ 1], x, p_new, Ap, z, cgd);
+                }
+            }
+        }
         if (jac && lapl) {
             k_cg_A<T, true, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(
                 nx, ny, c->march_th, aP, aE, aN, r, nullptr, p_old, p_new, Ap, cgd, c->partials, c->counter, eps_curv,

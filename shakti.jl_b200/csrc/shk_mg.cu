@@ -612,11 +612,10 @@ __device__ __forceinline__ void tma_give_up(CgDev *cg, uint64_t *other, uint32_t
 // Common frame of the two kernels: barrier set-up, the first tile's copies, and per tile the next
 // tile's copies, PRE(tile origin) (work that needs no staged data), the wait, and BODY(stage, tile
 // origin).
-template <typename Y, bool UP, bool FB, typename Pre, typename Body>
-__device__ __forceinline__ void tma_tiles(const TmaArgs &M, const Lv &L, unsigned char *sm, CgDev *cg, Pre pre,
-                                          Body body) {
+template <typename Y, typename Iss, typename Pre, typename Body>
+__device__ __forceinline__ void tma_tiles(int nx, int ny, unsigned char *sm, CgDev *cg, Iss iss, Pre pre, Body body) {
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Y::o_bar);
-    const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
+    const int tiles_x = (nx + kFW - 1) / kFW, ntiles = tiles_x * ((ny + kFH - 1) / kFH);
     if (su32(sm) & 127u) {  // the boxes' 128-byte alignment is not met: no copy is issued
         tma_give_up(cg, &bar[0], 0, false);
         return;
@@ -626,7 +625,7 @@ __device__ __forceinline__ void tma_tiles(const TmaArgs &M, const Lv &L, unsigne
         tma_bar_init(&bar[1]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         if ((int)blockIdx.x < ntiles)
-            tma_issue<Y, UP, FB>(M, sm, &bar[0], ((int)blockIdx.x % tiles_x) * kFW, ((int)blockIdx.x / tiles_x) * kFH);
+            iss(sm, &bar[0], ((int)blockIdx.x % tiles_x) * kFW, ((int)blockIdx.x / tiles_x) * kFH);
     }
     __syncthreads();
     int it = 0;
@@ -635,7 +634,7 @@ __device__ __forceinline__ void tma_tiles(const TmaArgs &M, const Lv &L, unsigne
         if (threadIdx.x == 0 && tn < ntiles) {
             // the other stage was last read before the previous tile's closing barrier
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            tma_issue<Y, UP, FB>(M, sm + (s ^ 1) * Y::stage, &bar[s ^ 1], (tn % tiles_x) * kFW, (tn / tiles_x) * kFH);
+            iss(sm + (s ^ 1) * Y::stage, &bar[s ^ 1], (tn % tiles_x) * kFW, (tn / tiles_x) * kFH);
         }
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
         pre(x0, y0);
@@ -684,8 +683,9 @@ __global__ void __launch_bounds__(256, 3) k_mg_down_t(const __grid_constant__ Tm
     double2 xq = make_double2(0.0, 0.0), pq = xq;
     bool inside = false;
     size_t q = 0;
-    tma_tiles<Y, false, FB>(
-        M, L, sm, cg,
+    tma_tiles<Y>(
+        L.nx, L.ny, sm, cg,
+        [&](unsigned char *st, uint64_t *b, int x0, int y0) { tma_issue<Y, false, FB>(M, st, b, x0, y0); },
         [&](int x0, int y0) {
             const int gx = x0 + gx0, gy = y0 + gy0;
             inside = gx < L.nx && gy < L.ny;  // nx is even: both cells of the pair, or neither
@@ -761,8 +761,10 @@ __global__ void __launch_bounds__(256, 4) k_mg_up_t(const __grid_constant__ TmaA
     ring_pair_at(P1, has1 ? tid : 0);
     const int gx0 = -kFR + 2 * (1 + (tid & 15)), gy0 = (tid >> 4);
     double red[2] = {0.0, 0.0};
-    tma_tiles<Y, true, false>(
-        M, L, sm, cg, [&](int, int) {},
+    tma_tiles<Y>(
+        L.nx, L.ny, sm, cg,
+        [&](unsigned char *st, uint64_t *b, int x0, int y0) { tma_issue<Y, true, false>(M, st, b, x0, y0); },
+        [&](int, int) {},
         [&](unsigned char *st, int x0, int y0) {
             const TB *SB = reinterpret_cast<const TB *>(st + Y::o_b) + Y::bOff;
             const TOp O = stage_op<Y>(st);
@@ -810,6 +812,112 @@ __global__ void __launch_bounds__(256, 4) k_mg_up_t(const __grid_constant__ TmaA
         if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
             if (init) cg_init_finish(cg, out[0], cg->rr, cg->bnorm);
             else cg_iter_finish(cg, out[0], out[1]);
+        }
+    }
+}
+
+// The outer CG's search-direction update and matvec of the multigrid form on TMA-staged tiles:
+// p_new = z + beta p_old over the tile and a one-cell ring, then Ap = A p_new on the tile and
+// p_new'Ap, with the Float64 roundings of k_cg_A (no fused multiply-adds: every product and sum is
+// rounded, in k_cg_A's order, so the two kernels agree bit for bit up to the order of the grid
+// sum).  Boxes: z and p_old over rows y0-1 .. y0+16 and columns x0-2 .. x0+33 (36 x 18), aP on
+// the tile, aE from column x0-2 (34 x 16), aN from row y0-1 (32 x 17).
+constexpr int kMvW = kFW + 4, kMvH = kFH + 2;  // staged p region (36 x 18)
+
+struct MvArgs {
+    CUtensorMap z, po, aP, aE, aN;
+};
+
+constexpr unsigned rnd128(unsigned v) { return (v + 127u) & ~127u; }
+
+struct MvLayout {
+    static constexpr unsigned pB = kMvW * kMvH * 8, apB = kFW * kFH * 8, aeB = (kFW + 2) * kFH * 8,
+                              anB = kFW * (kFH + 1) * 8;
+    static constexpr unsigned o_z = 0, o_po = rnd128(pB), o_aP = rnd128(o_po + pB), o_aE = rnd128(o_aP + apB),
+                              o_aN = rnd128(o_aE + aeB), stage = rnd128(o_aN + anB);
+    static constexpr unsigned o_p = 2 * stage, o_bar = rnd128(o_p + pB), bytes = o_bar + 16;
+};
+
+__global__ void __launch_bounds__(256, 4) k_cg_matvec_t(const __grid_constant__ MvArgs M, int nx, int ny,
+                                                        double *p_new, double *Ap, CgDev *cg, double *partials,
+                                                        unsigned int *counter, double eps_curv) {
+    const CgView cv = block_cg_view(cg);
+    if (cv.done) return;
+    using Y = MvLayout;
+    extern __shared__ __align__(128) unsigned char sm[];
+    double *P = reinterpret_cast<double *>(sm + Y::o_p);
+    const bool first = cv.first != 0;
+    const double beta = cv.beta;
+    const int tid = threadIdx.x;
+    const unsigned tx = Y::pB * (first ? 1 : 2) + Y::apB + Y::aeB + Y::anB;
+    // p pairs: slot 0 = pair tid of the 324, slot 1 = pair 256 + tid (tid < 68)
+    constexpr int np = kMvW / 2, npairs = np * kMvH;
+    const int k0 = (tid / np) * kMvW + 2 * (tid % np), k1 = ((tid + 256) / np) * kMvW + 2 * ((tid + 256) % np);
+    const bool has1 = tid + 256 < npairs;
+    const int r = tid >> 4, pc = 2 * (tid & 15);  // the thread's output pair: tile row r, columns pc, pc + 1
+    double acc = 0.0;
+    tma_tiles<Y>(
+        nx, ny, sm, cg,
+        [&](unsigned char *st, uint64_t *b, int x0, int y0) {
+            tma_expect(b, tx);
+            tma_load(st + Y::o_z, &M.z, b, x0 - 2, y0 - 1);
+            if (!first) tma_load(st + Y::o_po, &M.po, b, x0 - 2, y0 - 1);
+            tma_load(st + Y::o_aP, &M.aP, b, x0, y0);
+            tma_load(st + Y::o_aE, &M.aE, b, x0 - 2, y0);
+            tma_load(st + Y::o_aN, &M.aN, b, x0, y0 - 1);
+        },
+        [&](int, int) {},
+        [&](unsigned char *st, int x0, int y0) {
+            const double *Z = reinterpret_cast<const double *>(st + Y::o_z);
+            const double *PO = reinterpret_cast<const double *>(st + Y::o_po);
+            auto form = [&](int k) {
+                const double2 z = *reinterpret_cast<const double2 *>(Z + k);
+                double2 v = z;
+                if (!first) {
+                    const double2 po = *reinterpret_cast<const double2 *>(PO + k);
+                    v = make_double2(__dadd_rn(z.x, __dmul_rn(beta, po.x)), __dadd_rn(z.y, __dmul_rn(beta, po.y)));
+                }
+                *reinterpret_cast<double2 *>(P + k) = v;
+            };
+            form(k0);
+            if (has1) form(k1);
+            __syncthreads();
+            const double *AP = reinterpret_cast<const double *>(st + Y::o_aP);
+            const double *AE = reinterpret_cast<const double *>(st + Y::o_aE);
+            const double *AN = reinterpret_cast<const double *>(st + Y::o_aN);
+            const int gy = y0 + r, gx = x0 + pc;
+            if (gy < ny && gx < nx) {  // nx is even: both cells of the pair, or neither
+                const int kp = (r + 1) * kMvW + pc + 2;  // staged index of the pair's first cell
+                double y[2], pv[2];
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int k = kp + e, ix = gx + e;
+                    const double pk = P[k];
+                    double v = __dmul_rn(AP[r * kFW + pc + e], pk);
+                    if (ix < nx - 1) v = __dsub_rn(v, __dmul_rn(AE[r * (kFW + 2) + pc + e + 2], P[k + 1]));
+                    if (ix > 0) v = __dsub_rn(v, __dmul_rn(AE[r * (kFW + 2) + pc + e + 1], P[k - 1]));
+                    if (gy + 1 < ny) v = __dsub_rn(v, __dmul_rn(AN[(r + 1) * kFW + pc + e], P[k + kMvW]));
+                    if (gy > 0) v = __dsub_rn(v, __dmul_rn(AN[r * kFW + pc + e], P[k - kMvW]));
+                    y[e] = v;
+                    pv[e] = pk;
+                }
+                const size_t q = (size_t)gx + (size_t)gy * nx;
+                *reinterpret_cast<double2 *>(p_new + q) = make_double2(pv[0], pv[1]);
+                *reinterpret_cast<double2 *>(Ap + q) = make_double2(y[0], y[1]);
+                acc = __dadd_rn(acc, __dmul_rn(pv[0], y[0]));
+                acc = __dadd_rn(acc, __dmul_rn(pv[1], y[1]));
+            }
+        });
+    double red[1] = {acc}, out[1];
+    if (grid_reduce<1, false>(red, partials, counter, out) && threadIdx.x == 0) {
+        const double pAp = out[0];
+        cg->pAp = pAp;
+        const double lim = eps_curv * cg->pNorm2;
+        if ((pAp <= lim && fabs(pAp) <= lim) || isnan(pAp)) {
+            cg->done = 1;
+            cg->status = SHK_BREAKDOWN;
+        } else {
+            cg->alpha = __ddiv_rn(cg->gamma, pAp);
         }
     }
 }
@@ -1224,10 +1332,12 @@ struct MgTma {
     CUtensorMap b[kMgMaxLevels], xi[kMgMaxLevels];
     CUtensorMap xc[kMgMaxLevels][2];  // level l's two iterates as coarse boxes (read by level l - 1)
     CUtensorMap r, r2, Ap;            // level 0's Float64 vectors
-    int grid[5] = {};                 // per kernel: blocks of one resident wave
+    bool mv_ok = false;               // the outer CG's matvec stages through TMA
+    CUtensorMap mv_z, mv_p[2], mv_aP, mv_aE, mv_aN;
+    int grid[6] = {};                 // per kernel: blocks of one resident wave
 };
 
-enum { TK_DOWN0, TK_DOWN0_FB, TK_DOWN, TK_UP0, TK_UP };
+enum { TK_DOWN0, TK_DOWN0_FB, TK_DOWN, TK_UP0, TK_UP, TK_MV };
 
 static bool encode(EncodeTiledFn fn, CUtensorMap *m, CUtensorMapDataType dt, size_t esz, const void *base, int nx,
                    int ny, int bw, int bh) {
@@ -1298,18 +1408,28 @@ static MgTma *tma_maps(Ctx *c, int *rc) {
         c->mg_tma = 0;
         return nullptr;
     }
-    int bps[5] = {};
+    if (T->ok[0]) {
+        const MgLevel &m = c->mg[0];
+        T->mv_ok = encode(fn, &T->mv_z, F64, 8, c->z, m.nx, m.ny, kMvW, kMvH) &&
+                   encode(fn, &T->mv_p[0], F64, 8, c->p[0], m.nx, m.ny, kMvW, kMvH) &&
+                   encode(fn, &T->mv_p[1], F64, 8, c->p[1], m.nx, m.ny, kMvW, kMvH) &&
+                   encode(fn, &T->mv_aP, F64, 8, c->aP, m.nx, m.ny, kFW, kFH) &&
+                   encode(fn, &T->mv_aE, F64, 8, c->aE, m.nx, m.ny, kFW + 2, kFH) &&
+                   encode(fn, &T->mv_aN, F64, 8, c->aN, m.nx, m.ny, kFW, kFH + 1);
+    }
+    int bps[6] = {};
     int e = tma_kernel_bps(c, k_mg_down_t<double, false>, TLayout<double, false, false>::bytes, &bps[TK_DOWN0]);
     if (!e) e = tma_kernel_bps(c, k_mg_down_t<double, true>, TLayout<double, false, true>::bytes, &bps[TK_DOWN0_FB]);
     if (!e) e = tma_kernel_bps(c, k_mg_down_t<float, false>, TLayout<float, false, false>::bytes, &bps[TK_DOWN]);
     if (!e) e = tma_kernel_bps(c, k_mg_up_t<double, true>, TLayout<double, true, false>::bytes, &bps[TK_UP0]);
     if (!e) e = tma_kernel_bps(c, k_mg_up_t<float, false>, TLayout<float, true, false>::bytes, &bps[TK_UP]);
+    if (!e) e = tma_kernel_bps(c, k_cg_matvec_t, MvLayout::bytes, &bps[TK_MV]);
     if (e) {
         delete T;
         *rc = e;
         return nullptr;
     }
-    for (int k = 0; k < 5; k++) {
+    for (int k = 0; k < 6; k++) {
         if (bps[k] < 1) {
             delete T;
             *rc = fail(c, SHK_CUDA_ERROR, "multigrid TMA kernel does not fit on an SM");
@@ -1505,6 +1625,23 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
         c->launches += c->mg_nu;
     }
     return check_launch(c, "multigrid apply");
+}
+
+// The outer CG's p update and matvec on TMA-staged tiles, where the context's maps cover these
+// buffers; *launched says whether it ran (otherwise k_cg_A serves).
+int mg_cg_matvec(Ctx *c, int par, const double *aP, const double *aE, const double *aN, const double *z,
+                 const double *p_old, double *p_new, double *Ap, CgDev *cg, double eps_curv, bool *launched) {
+    *launched = false;
+    const MgTma *T = c->mg_maps;
+    if (!T || !T->mv_ok || aP != c->aP || aE != c->aE || aN != c->aN || z != c->z || p_old != c->p[par] ||
+        p_new != c->p[par ^ 1] || Ap != c->Ap)
+        return SHK_OK;
+    const MgLevel &m = c->mg[0];
+    const MvArgs a{T->mv_z, T->mv_p[par], T->mv_aP, T->mv_aE, T->mv_aN};
+    k_cg_matvec_t<<<tma_grid(c, T, TK_MV, m), 256, MvLayout::bytes, c->stream>>>(
+        a, m.nx, m.ny, p_new, Ap, cg, c->partials, c->counter, eps_curv);
+    *launched = true;
+    return check_launch(c, "cg matvec");
 }
 
 // One iteration's x/r update fused into the V-cycle's first level-0 kernel (tile form, nu = 2):
