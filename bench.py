@@ -256,8 +256,8 @@ def iteration_bytes(form, nx, ny):
 
 
 def measure_cg_iteration(shk, sim, form, short=20, long=220):
-    """Average duration of one CG iteration of `form` (k_cg_A + k_cg_B, plus the V-cycle for the
-    multigrid form) on the current assembled system: CUDA events around a solve of exactly `long`
+    """Average duration of one CG iteration of `form` (its matvec, update and, for the multigrid
+    form, V-cycle kernels) on the current assembled system: CUDA events around a solve of exactly `long`
     iterations minus one of `short` iterations (rtol = 0), so set-up and initial residual cancel."""
     import ctypes as C
     import torch
@@ -297,8 +297,9 @@ def roofline_for(shk, sim, form, w, peaks):
     achieved = nbytes / (it_ms / 1e3) / 1e9
     kernel = {"plain": "k_cg_A + k_cg_B (one Jacobi-PCG iteration, Float64)",
               "fp32cg": "k_cg_A + k_cg_B (one Jacobi-PCG iteration, Float32 Laplacian form)",
-              "multigrid": "one multigrid-preconditioned CG iteration: k_cg_A + k_cg_B (Float64) + the Float32 "
-                           "V-cycle (fused level kernels k_mg_down/k_mg_up + the one-block k_mg_bottom)"}[form]
+              "multigrid": "one multigrid-preconditioned CG iteration: the TMA-staged Float64 p update and "
+                           "matvec (k_cg_matvec_t), the Float32 V-cycle on TMA-staged tiles (k_mg_down_t, its "
+                           "level-0 launch with the CG's x/r update, k_mg_up_t) and the one-block k_mg_bottom"}[form]
     r = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
          "frac": round(achieved / peak, 4), "traffic": None, "kernel": kernel,
          "algorithmic_bytes_per_launch": nbytes, "us_per_iteration": round(it_ms * 1e3, 2),
