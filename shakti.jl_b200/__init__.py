@@ -21,7 +21,8 @@ from .simulation import (AbstractHeadScheme, EllipticHeadScheme, ParabolicHeadSc
                          ExplicitGapScheme, ImplicitGapScheme, AbstractSensibleHeatScheme, WithSensibleHeat,
                          NoSensibleHeat, AbstractOpenBySlidingScheme, WithOpenBySliding, NoOpenBySliding,
                          AbstractObserver, NoObserver, LiveObserver, Simulation, run, step, step_h, step_b,
-                         update_ieb, picard_status, set_initial_conditions, save_checkpoint, load_checkpoint)
+                         update_ieb, picard_status, set_initial_conditions, save_checkpoint, load_checkpoint,
+                         HostIO)
 from .ensemble import Ensemble
 from . import configs
 

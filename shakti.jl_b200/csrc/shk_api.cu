@@ -122,8 +122,12 @@ static int ctx_alloc(Ctx *c) {
     c->dev = (DevScalars *)(b + o_dev);
     e = cudaMemsetAsync(c->arena, 0, off, c->stream);
     if (e != cudaSuccess) return check_cuda(c, e, "cudaMemset(workspace)");
-    e = cudaMallocHost(&c->host_dev, sizeof(DevScalars));
-    if (e != cudaSuccess) return check_cuda(c, e, "cudaMallocHost");
+    e = cudaHostAlloc(&c->host_dev, sizeof(DevScalars), cudaHostAllocMapped);
+    if (e != cudaSuccess) return check_cuda(c, e, "cudaHostAlloc");
+    if (cudaHostGetDevicePointer((void **)&c->host_dev_d, c->host_dev, 0) != cudaSuccess) {
+        cudaGetLastError();
+        c->host_dev_d = nullptr;  // control scalars then move by cudaMemcpyAsync
+    }
     memset(c->host_dev, 0, sizeof(DevScalars));
     // ChebyshevPreconditioner placeholder bounds (1, 1) (src/preconditioner.jl:179-186)
     c->host_dev->cheb.lam_min = 1.0;

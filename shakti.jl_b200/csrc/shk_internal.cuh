@@ -130,6 +130,7 @@ struct Ctx {
     unsigned int *counter = nullptr;
     DevScalars *dev = nullptr;
     DevScalars *host_dev = nullptr;  // pinned mirror for read-back
+    DevScalars *host_dev_d = nullptr;  // its device alias (mapped pinned memory), or null
     MgLevel mg[kMgMaxLevels];
     int mg_levels = 0;
     int mg_nu = 2;           // damped-Jacobi sweeps before and after each coarse correction
@@ -224,6 +225,7 @@ int cheb_set_bounds(Ctx *c, double lmin, double lmax);
 int launch_chebyshev_apply_standalone(Ctx *c, int degree, const double *x, double *y);
 int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st);
 int read_scalars(Ctx *c);
+int move_scalars(Ctx *c, void *dst, const void *src, size_t bytes, bool to_host);
 int residual_norms(Ctx *c, const double *x, double *rnorm, double *bnorm);
 int jacobi_smooth(Ctx *c, double *x, double *tmp, int sweeps, double omega);
 

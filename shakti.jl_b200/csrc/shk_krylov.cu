@@ -715,15 +715,39 @@ int residual_norms(Ctx *c, const double *x, double *rnorm, double *bnorm) {
     return SHK_OK;
 }
 
+// Control scalars move between the device scalar block and its pinned host mirror through a
+// one-block kernel that reads or writes the mapped host memory, not through a copy engine: a large
+// transfer the caller has queued on a copy engine (a field on its way to the host while the solve
+// runs) would otherwise hold every small control copy -- and the host loop waiting on it -- behind
+// it.  Falls back to cudaMemcpyAsync for host memory outside the mirror.
+__global__ void k_words(const unsigned long long *src, unsigned long long *dst, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+int move_scalars(Ctx *c, void *dst, const void *src, size_t bytes, bool to_host) {
+    const char *h0 = (const char *)c->host_dev, *hp = (const char *)(to_host ? dst : src);
+    const bool mirrored = c->host_dev_d && hp >= h0 && hp + bytes <= h0 + sizeof(DevScalars) && bytes % 8 == 0 &&
+                          ((uintptr_t)dst % 8) == 0 && ((uintptr_t)src % 8) == 0;
+    if (mirrored) {
+        void *alias = (char *)c->host_dev_d + (hp - h0);
+        const void *s = to_host ? src : alias;
+        void *d = to_host ? alias : dst;
+        k_words<<<1, 64, 0, c->stream>>>((const unsigned long long *)s, (unsigned long long *)d, (int)(bytes / 8));
+        c->launches++;
+        return check_launch(c, "control scalars");
+    }
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, to_host ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice,
+                                    c->stream);
+    return e == cudaSuccess ? SHK_OK : check_cuda(c, e, "control scalars");
+}
+
 int read_scalars(Ctx *c) {
-    cudaError_t e = cudaMemcpyAsync(c->host_dev, c->dev, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream);
-    if (e != cudaSuccess) return check_cuda(c, e, "read scalars");
+    if (int rc = move_scalars(c, c->host_dev, c->dev, sizeof(DevScalars), true)) return rc;
     return check_cuda(c, cudaStreamSynchronize(c->stream), "stream sync");
 }
 
 static int read_cg_flags(Ctx *c, CgDev *dst, const CgDev *src) {
-    cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(CgDev), cudaMemcpyDeviceToHost, c->stream);
-    if (e != cudaSuccess) return check_cuda(c, e, "read cg scalars");
+    if (int rc = move_scalars(c, dst, src, sizeof(CgDev), true)) return rc;
     return check_cuda(c, cudaStreamSynchronize(c->stream), "stream sync");
 }
 
@@ -842,8 +866,8 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
     };
     const double eps_curv = sizeof(T) == 8 ? DBL_EPSILON : (double)FLT_EPSILON;
     cgh->trips = 0;
-    cudaError_t e = cudaMemcpyAsync(cgd, cgh, sizeof(CgDev), cudaMemcpyHostToDevice, c->stream);
-    if (e != cudaSuccess) return check_cuda(c, e, "cg scalars upload");
+    if (int rc0 = move_scalars(c, cgd, cgh, sizeof(CgDev), false)) return rc0;
+    cudaError_t e = cudaSuccess;
     if (jac) {
         k_cg_init<T, true><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, aP, aE, aN, x0, b, r, x, cgd, c->partials,
                                                                        c->counter);

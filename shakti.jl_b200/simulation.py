@@ -277,6 +277,94 @@ def run(sim: Simulation, checkpoint_every: int | None = None, checkpoint_path: s
 
 
 # ---------------------------------------------------------------------------------------------
+# Host-fed runs: per-step inputs from and outputs to host memory, the transfers overlapped with the
+# computation (no reference counterpart: the reference's run! keeps every field on its device and
+# its observers copy to the host between steps).
+# ---------------------------------------------------------------------------------------------
+class HostIO:
+    """Runs `sim` with per-step input from and output to host memory, overlapping the transfers
+    with the computation.  The device staging buffers (the basal input twice, h and b twice each:
+    about 6 fields) and the two copy streams are allocated here, once; `run` may be called any
+    number of times."""
+
+    def __init__(self, sim: Simulation):
+        import torch
+        self.sim = sim
+        st = sim.state
+        self.h2d, self.d2h = torch.cuda.Stream(), torch.cuda.Stream()
+        self.stage = [torch.empty_like(st.ieb) for _ in range(2)]
+        self.snap_h = [torch.empty_like(st.h) for _ in range(2)]
+        self.snap_b = [torch.empty_like(st.b) for _ in range(2)]
+
+    def run(self, ieb_host, h_host=None, b_host=None) -> None:
+        """Advance the simulation by len(ieb_host) timesteps (step! as in `run`, without observers
+        and with the basal input taken from the host instead of sim.mi): step k uses ieb from the
+        pinned host tensor ieb_host[k] and returns its head and gap height into h_host / b_host
+        (one pinned tensor each, overwritten every step, or a sequence with one tensor per step).
+        Host tensors are shaped (ny, nx), row-major: the fields' memory order.
+
+        Step k+1's input is copied host -> device on one copy stream while step k computes, and
+        step k's h and b, snapshotted on the device right after the step, are copied device -> host
+        on the other while step k+1 computes, so the host link's time hides behind the solve.
+        Returns with every copy ordered before the current stream's next work
+        (torch.cuda.synchronize() waits for them)."""
+        import torch
+        sim, st = self.sim, self.sim.state
+        steps = len(ieb_host)
+        if steps == 0:
+            return
+        comp, h2d, d2h = torch.cuda.current_stream(), self.h2d, self.d2h
+        stage, snap_h, snap_b = self.stage, self.snap_h, self.snap_b
+        want_out = h_host is not None or b_host is not None
+        ev = torch.cuda.Event
+        in_ready, in_free, snap_ready, out_done = [ev(), ev()], [ev(), ev()], [ev(), ev()], [ev(), ev()]
+        start = ev()
+        start.record(comp)
+        h2d.wait_event(start)
+        d2h.wait_event(start)
+
+        def pick(x, k):
+            return x if isinstance(x, torch.Tensor) else x[k]
+
+        def issue_in(k):
+            s = k % 2
+            with torch.cuda.stream(h2d):
+                if k >= 2:
+                    h2d.wait_event(in_free[s])
+                stage[s].t().copy_(ieb_host[k], non_blocking=True)
+                in_ready[s].record(h2d)
+
+        issue_in(0)
+        if steps > 1:
+            issue_in(1)
+        for k in range(steps):
+            s = k % 2
+            comp.wait_event(in_ready[s])
+            st.ieb.copy_(stage[s])
+            in_free[s].record(comp)
+            if k + 2 < steps:
+                issue_in(k + 2)
+            step_h(sim)
+            step_b(sim)
+            sim.total_time += sim.dt
+            if want_out:
+                if k >= 2:
+                    comp.wait_event(out_done[s])
+                snap_h[s].copy_(st.h)
+                snap_b[s].copy_(st.b)
+                snap_ready[s].record(comp)
+                with torch.cuda.stream(d2h):
+                    d2h.wait_event(snap_ready[s])
+                    if h_host is not None:
+                        pick(h_host, k).copy_(snap_h[s].t(), non_blocking=True)
+                    if b_host is not None:
+                        pick(b_host, k).copy_(snap_b[s].t(), non_blocking=True)
+                    out_done[s].record(d2h)
+        comp.wait_stream(h2d)
+        comp.wait_stream(d2h)
+
+
+# ---------------------------------------------------------------------------------------------
 # set_initial_conditions! (src/initial_conditions.jl:14-125)
 # ---------------------------------------------------------------------------------------------
 def _copy_in(dst, arr):
