@@ -156,8 +156,12 @@ class ClockSampler:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # the timed region starts once the sampler is producing samples (it takes a moment to start)
+            t_end = time.time() + 3.0
+            while time.time() < t_end and Path(self.path).stat().st_size == 0:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
