@@ -134,7 +134,7 @@ static int ens_layout(Ens *e) {
         // flat_grid in shk_krylov.cu)
         int nb[EF_N];
         nb[EF_STENCIL] = c->grid_stencil;
-        nb[EF_TAIL] = std::max(1, std::min(tiles_of(I.nx, I.ny), c->num_sms * 4));
+        nb[EF_TAIL] = std::max(1, std::min(tiles_of(I.nx, I.ny), c->num_sms * kTailBlocksPerSm));
         nb[EF_MARCH] = march_blocks_of(I.nx, I.ny, I.march_th);
         nb[EF_STREAM] = (int)std::max(1LL, std::min((long long)c->num_sms * 8, (n + 1023) / 1024));
         nb[EF_FLAT] = (int)std::max(1LL, std::min((long long)c->grid_stencil, (n + kThreads - 1) / kThreads));

@@ -363,7 +363,7 @@ __device__ __forceinline__ void tail_body(Blk B, int nx, int ny, const Params &P
 }
 
 template <bool FROM_H, bool CHECK>
-__global__ void __launch_bounds__(kTailThreads, 4) k_tail(int nx, int ny, Params P, Sliding L, shk_state s,
+__global__ void __launch_bounds__(kTailThreads, kTailBlocksPerSm) k_tail(int nx, int ny, Params P, Sliding L, shk_state s,
                                                       const uint8_t *__restrict__ m8,
                                                       const double *__restrict__ h_prev, double *partials,
                                                       unsigned int *counter, PicDev *pic) {
@@ -551,10 +551,10 @@ int build_mask8(Ctx *c) {
     return check_launch(c, "k_mask8");
 }
 
-// One resident wave of the tail (four blocks per SM), striding over the tiles.
+// One resident wave of the tail (kTailBlocksPerSm blocks per SM), striding over the tiles.
 static int tail_grid(const Ctx *c) {
     const long long tiles = (long long)((c->nx + kTailW - 1) / kTailW) * ((c->ny + kTailH - 1) / kTailH);
-    return (int)std::max(1LL, std::min(tiles, (long long)c->num_sms * 4));
+    return (int)std::max(1LL, std::min(tiles, (long long)c->num_sms * kTailBlocksPerSm));
 }
 
 int launch_initial_conditions(Ctx *c) {
@@ -658,7 +658,7 @@ __global__ void __launch_bounds__(kThreads) k_ens_assemble(EnsInst *E, const int
     assemble_body<false>(B, I.nx, I.ny, I.P, I.kfs, 0.0, I.st, I.mask8, I.aP, I.aE, I.aN, I.rhs, I.h_prev);
 }
 
-__global__ void __launch_bounds__(kTailThreads, 3) k_ens_tail(EnsInst *E, const int *b2i) {
+__global__ void __launch_bounds__(kTailThreads, kTailBlocksPerSm) k_ens_tail(EnsInst *E, const int *b2i) {
     __shared__ EnsInst I;
     const Blk B = ens_stage(I, E, b2i, EF_TAIL);
     if (!I.pic_active) return;

@@ -33,6 +33,10 @@ constexpr int kTX = 32;             // tile width (cells along x, one warp)
 constexpr int kTY = 8;              // tile height
 constexpr int kThreads = kTX * kTY; // 256 threads per block
 constexpr int kMaxRedValues = 4;
+// Resident blocks per SM of the fused field tail (288 threads).  Five (40 registers, a few spills)
+// measured fastest at 4096^2: 1310 us per call against 1376 with four, 1485 with six and 1616 with
+// three (no spills): the tail needs warps in flight more than registers.
+constexpr int kTailBlocksPerSm = 5;
 constexpr int kMarchX = 128;        // columns per block of the row-marching stencil kernels
 constexpr int kUnrollB = 2;         // 16-byte vectors in flight per thread in streaming kernels
 constexpr int kRingRows = 6;        // shared-memory ring depth of the row-marching kernels
