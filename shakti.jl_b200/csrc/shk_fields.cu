@@ -449,7 +449,7 @@ __device__ __forceinline__ void assemble_body(Blk B, int nx, int ny, const Param
 }
 
 template <bool PARABOLIC>
-__global__ void __launch_bounds__(kThreads, 6) k_assemble(int nx, int ny, Params P, int kfs, double dt,
+__global__ void __launch_bounds__(kThreads, kAsmBlocksPerSm) k_assemble(int nx, int ny, Params P, int kfs, double dt,
                                                        shk_state s, const uint8_t *__restrict__ m8,
                                                        double *__restrict__ aP, double *__restrict__ aE,
                                                        double *__restrict__ aN, double *__restrict__ rhs,
@@ -583,11 +583,13 @@ int launch_initial_conditions(Ctx *c) {
 
 int launch_assemble(Ctx *c, int parabolic, double dt, bool copy_h_prev) {
     double *hp = copy_h_prev ? c->h_prev : nullptr;
+    const long long tiles = (long long)((c->nx + kTX - 1) / kTX) * ((c->ny + kTY - 1) / kTY);
+    const int grid = (int)std::max(1LL, std::min(tiles, (long long)c->num_sms * kAsmBlocksPerSm));
     if (parabolic)
-        k_assemble<true><<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->kfs, dt, c->st, c->mask8,
+        k_assemble<true><<<grid, kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->kfs, dt, c->st, c->mask8,
                                                                       c->aP, c->aE, c->aN, c->rhs, hp);
     else
-        k_assemble<false><<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->kfs, dt, c->st, c->mask8,
+        k_assemble<false><<<grid, kThreads, 0, c->stream>>>(c->nx, c->ny, c->P, c->kfs, dt, c->st, c->mask8,
                                                                        c->aP, c->aE, c->aN, c->rhs, hp);
     c->launches++;
     return check_launch(c, "k_assemble");
