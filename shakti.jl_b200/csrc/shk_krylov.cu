@@ -1086,10 +1086,13 @@ int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
     if (o->precond != SHK_PRECOND_JACOBI && o->precond != SHK_PRECOND_CHEBYSHEV && o->precond != SHK_PRECOND_MULTIGRID)
         return fail(c, SHK_BAD_ARG, "unknown preconditioner");
     if (o->precond == SHK_PRECOND_MULTIGRID) {
-        // Float32 Laplacian-form operator of level 0, then the coarse levels
-        k_to_float_lapl<<<flat_grid(c, n), kThreads, 0, c->stream>>>(nx, ny, c->aP, c->aE, c->aN, c->aP32, c->aE32,
-                                                                     c->aN32, c->dP32);
-        c->launches++;
+        // the Float32 Laplacian-form operator of level 0 and the coarse levels (a hierarchy of two
+        // or more levels builds level 0 inside its first coarsening pass)
+        if (c->mg_levels <= 1) {
+            k_to_float_lapl<<<flat_grid(c, n), kThreads, 0, c->stream>>>(nx, ny, c->aP, c->aE, c->aN, c->aP32,
+                                                                         c->aE32, c->aN32, c->dP32);
+            c->launches++;
+        }
         int rc = mg_setup(c);
         if (rc) return rc;
     }

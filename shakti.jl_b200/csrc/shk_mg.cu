@@ -90,6 +90,68 @@ __global__ void k_mg_coarsen(int nxf, int nyf, int nxc, int nyc, const double *a
     }
 }
 
+// Level 0 of a hierarchy of two or more levels in one pass: per fine cell the Float32 Laplacian-form
+// operator (aE, aN, dP = aP - the four couplings) and the smoother's activity flag and damped
+// inverse diagonal (the arrays k_to_float_lapl and k_mg_act0 write), and per 2x2 aggregate the
+// level-1 Float64 operator (k_mg_coarsen's sums, in its order).  One thread per aggregate on a 2D
+// grid, so a warp reads 64 consecutive fine cells of each of its two rows.
+__global__ void __launch_bounds__(256) k_mg_level0(int nx, int ny, int nxc, int nyc, const uint8_t *m8,
+                                                   const double *aP, const double *aE, const double *aN,
+                                                   double omega, float *fE, float *fN, float *fD, float *fW,
+                                                   uint8_t *act0, double *aEc, double *aNc, double *dPc,
+                                                   uint8_t *actc) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= nxc || J >= nyc) return;
+    auto active = [&](size_t c) { return m8[c] == M_GROUNDED || m8[c] == M_UNKNOWN; };
+    double dp[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    bool a[2][2] = {{false, false}, {false, false}};
+    for (int dj = 0; dj < 2; dj++)
+        for (int di = 0; di < 2; di++) {
+            const int i = 2 * I + di, j = 2 * J + dj;
+            if (i >= nx || j >= ny) continue;
+            const size_t c = (size_t)i + (size_t)j * nx;
+            const double e = aE[c], w = i > 0 ? aE[c - 1] : 0.0, no = aN[c], so = j > 0 ? aN[c - nx] : 0.0;
+            const double p = aP[c], d = p - (e + w + no + so);
+            const bool ac = active(c);
+            fE[c] = (float)e;
+            fN[c] = (float)no;
+            fD[c] = (float)d;
+            fW[c] = (float)((ac ? omega : 1.0) / p);
+            act0[c] = ac ? 1 : 0;
+            dp[dj][di] = d;
+            a[dj][di] = ac;
+        }
+    double d = 0.0, e = 0.0, no = 0.0;
+    int act = 0;
+    for (int dj = 0; dj < 2; dj++)
+        for (int di = 0; di < 2; di++) {
+            if (!a[dj][di]) continue;  // out-of-range cells are inactive
+            act = 1;
+            d += dp[dj][di];
+        }
+    const int ie = 2 * I + 1;  // fine column on the west side of the east aggregate boundary
+    if (ie + 1 < nx)
+        for (int dj = 0; dj < 2; dj++) {
+            const int j = 2 * J + dj;
+            if (j >= ny) continue;
+            const size_t c = (size_t)ie + (size_t)j * nx;
+            if (a[dj][1] && active(c + 1)) e += aE[c];
+        }
+    const int jn = 2 * J + 1;
+    if (jn + 1 < ny)
+        for (int di = 0; di < 2; di++) {
+            const int i = 2 * I + di;
+            if (i >= nx) continue;
+            const size_t c = (size_t)i + (size_t)jn * nx;
+            if (a[1][di] && active(c + nx)) no += aN[c];
+        }
+    const size_t k = (size_t)I + (size_t)J * nxc;
+    aEc[k] = act ? e : 0.0;
+    aNc[k] = act ? no : 0.0;
+    dPc[k] = act ? d : 1.0;
+    actc[k] = (uint8_t)act;
+}
+
 // Float32 copies and the smoother's damped inverse diagonal wD = omega/aP with the Jacobi diagonal
 // aP = dP + the four couplings (identity rows: aP = 1, wD = 1).
 __global__ void k_mg_finish_level(int nx, int ny, const double *aE, const double *aN, const double *dP,
@@ -1286,16 +1348,21 @@ int mg_setup(Ctx *c) {
     if (grid2d(c->nx, c->ny).y > 65535u) return fail(c, SHK_BAD_ARG, "multigrid needs ny <= 524280");
     MgLevel *lv = c->mg;
     const int n0 = c->nx * c->ny;
-    k_mg_act0<<<mg_grid(c, n0), kThreads, 0, c->stream>>>(n0, c->mask8, c->aP, (double)c->mg_omega, lv[0].act,
-                                                           lv[0].wD);
-    c->launches++;
+    if (c->mg_levels == 1) {  // level 0 alone (k_to_float_lapl has written its Float32 operator)
+        k_mg_act0<<<mg_grid(c, n0), kThreads, 0, c->stream>>>(n0, c->mask8, c->aP, (double)c->mg_omega,
+                                                               lv[0].act, lv[0].wD);
+        c->launches++;
+    }
     for (int l = 0; l + 1 < c->mg_levels; l++) {
         const MgLevel &f = lv[l];
         MgLevel &g = lv[l + 1];
-        const double *aEf = l == 0 ? c->aE : f.aE64, *aNf = l == 0 ? c->aN : f.aN64;
-        const double *dPf = l == 0 ? nullptr : f.dP64;
-        k_mg_coarsen<<<mg_grid(c, (long long)g.nx * g.ny), kThreads, 0, c->stream>>>(
-            f.nx, f.ny, g.nx, g.ny, aEf, aNf, dPf, c->aP, f.act, g.aE64, g.aN64, g.dP64, g.act);
+        if (l == 0)
+            k_mg_level0<<<grid2d(g.nx, g.ny), kBlock2d, 0, c->stream>>>(
+                f.nx, f.ny, g.nx, g.ny, c->mask8, c->aP, c->aE, c->aN, (double)c->mg_omega, (float *)f.aE,
+                (float *)f.aN, (float *)f.dP, (float *)f.wD, f.act, g.aE64, g.aN64, g.dP64, g.act);
+        else
+            k_mg_coarsen<<<mg_grid(c, (long long)g.nx * g.ny), kThreads, 0, c->stream>>>(
+                f.nx, f.ny, g.nx, g.ny, f.aE64, f.aN64, f.dP64, nullptr, f.act, g.aE64, g.aN64, g.dP64, g.act);
         k_mg_finish_level<<<mg_grid(c, (long long)g.nx * g.ny), kThreads, 0, c->stream>>>(
             g.nx, g.ny, g.aE64, g.aN64, g.dP64, g.act, (double)c->mg_omega, (float *)g.aE, (float *)g.aN,
             (float *)g.dP, (float *)g.wD);
