@@ -152,6 +152,68 @@ __global__ void __launch_bounds__(256) k_mg_level0(int nx, int ny, int nxc, int 
     actc[k] = (uint8_t)act;
 }
 
+// k_mg_coarsen and k_mg_finish_level of coarse level l+1 (fine level l >= 1) in one pass.  The
+// finish needs the coarse west and south couplings of the neighbouring aggregates; each thread
+// recomputes them from the fine boundary they sum (same terms, same order), so the values are the
+// ones k_mg_coarsen would have stored.
+__global__ void k_mg_coarsen_finish(int nxf, int nyf, int nxc, int nyc, const double *aEf, const double *aNf,
+                                    const double *dPf, const uint8_t *actf, double omega, double *aEc,
+                                    double *aNc, double *dPc, uint8_t *actc, float *fE, float *fN, float *fD,
+                                    float *fW) {
+    GSTRIDE(k, nxc * nyc) {
+        const int I = k % nxc, J = k / nxc;
+        auto af = [&](int i, int j) { return i >= 0 && j >= 0 && i < nxf && j < nyf && actf[(size_t)i + (size_t)j * nxf]; };
+        double d = 0.0, e = 0.0, no = 0.0;
+        int act = 0;
+        for (int dj = 0; dj < 2; dj++)
+            for (int di = 0; di < 2; di++) {
+                const int i = 2 * I + di, j = 2 * J + dj;
+                if (!af(i, j)) continue;
+                act = 1;
+                d += dPf[(size_t)i + (size_t)j * nxf];
+            }
+        // east / north boundary sums of aggregate (A, B)
+        auto east = [&](int A, int B) {
+            double v = 0.0;
+            const int ie = 2 * A + 1;
+            if (ie + 1 < nxf)
+                for (int dj = 0; dj < 2; dj++) {
+                    const int j = 2 * B + dj;
+                    if (j >= nyf) continue;
+                    if (af(ie, j) && af(ie + 1, j)) v += aEf[(size_t)ie + (size_t)j * nxf];
+                }
+            return v;
+        };
+        auto north = [&](int A, int B) {
+            double v = 0.0;
+            const int jn = 2 * B + 1;
+            if (jn + 1 < nyf)
+                for (int di = 0; di < 2; di++) {
+                    const int i = 2 * A + di;
+                    if (i >= nxf) continue;
+                    if (af(i, jn) && af(i, jn + 1)) v += aNf[(size_t)i + (size_t)jn * nxf];
+                }
+            return v;
+        };
+        auto any_active = [&](int A, int B) {
+            return af(2 * A, 2 * B) || af(2 * A + 1, 2 * B) || af(2 * A, 2 * B + 1) || af(2 * A + 1, 2 * B + 1);
+        };
+        e = east(I, J);
+        no = north(I, J);
+        const double ae = act ? e : 0.0, an = act ? no : 0.0, dd = act ? d : 1.0;
+        aEc[k] = ae;
+        aNc[k] = an;
+        dPc[k] = dd;
+        actc[k] = (uint8_t)act;
+        const double w = (I > 0 && any_active(I - 1, J)) ? east(I - 1, J) : 0.0;
+        const double so = (J > 0 && any_active(I, J - 1)) ? north(I, J - 1) : 0.0;
+        fE[k] = (float)ae;
+        fN[k] = (float)an;
+        fD[k] = (float)dd;
+        fW[k] = act ? (float)(omega / (dd + (ae + w + an + so))) : 1.0f;
+    }
+}
+
 // Float32 copies and the smoother's damped inverse diagonal wD = omega/aP with the Jacobi diagonal
 // aP = dP + the four couplings (identity rows: aP = 1, wD = 1).
 __global__ void k_mg_finish_level(int nx, int ny, const double *aE, const double *aN, const double *dP,
@@ -1356,13 +1418,16 @@ int mg_setup(Ctx *c) {
     for (int l = 0; l + 1 < c->mg_levels; l++) {
         const MgLevel &f = lv[l];
         MgLevel &g = lv[l + 1];
-        if (l == 0)
-            k_mg_level0<<<grid2d(g.nx, g.ny), kBlock2d, 0, c->stream>>>(
-                f.nx, f.ny, g.nx, g.ny, c->mask8, c->aP, c->aE, c->aN, (double)c->mg_omega, (float *)f.aE,
-                (float *)f.aN, (float *)f.dP, (float *)f.wD, f.act, g.aE64, g.aN64, g.dP64, g.act);
-        else
-            k_mg_coarsen<<<mg_grid(c, (long long)g.nx * g.ny), kThreads, 0, c->stream>>>(
-                f.nx, f.ny, g.nx, g.ny, f.aE64, f.aN64, f.dP64, nullptr, f.act, g.aE64, g.aN64, g.dP64, g.act);
+        if (l > 0) {  // coarsening and the coarse level's Float32 copies in one pass
+            k_mg_coarsen_finish<<<mg_grid(c, (long long)g.nx * g.ny), kThreads, 0, c->stream>>>(
+                f.nx, f.ny, g.nx, g.ny, f.aE64, f.aN64, f.dP64, f.act, (double)c->mg_omega, g.aE64, g.aN64, g.dP64,
+                g.act, (float *)g.aE, (float *)g.aN, (float *)g.dP, (float *)g.wD);
+            c->launches++;
+            continue;
+        }
+        k_mg_level0<<<grid2d(g.nx, g.ny), kBlock2d, 0, c->stream>>>(
+            f.nx, f.ny, g.nx, g.ny, c->mask8, c->aP, c->aE, c->aN, (double)c->mg_omega, (float *)f.aE,
+            (float *)f.aN, (float *)f.dP, (float *)f.wD, f.act, g.aE64, g.aN64, g.dP64, g.act);
         k_mg_finish_level<<<mg_grid(c, (long long)g.nx * g.ny), kThreads, 0, c->stream>>>(
             g.nx, g.ny, g.aE64, g.aN64, g.dP64, g.act, (double)c->mg_omega, (float *)g.aE, (float *)g.aN,
             (float *)g.dP, (float *)g.wD);
