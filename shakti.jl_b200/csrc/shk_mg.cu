@@ -42,59 +42,15 @@ __global__ void k_mg_act0(int n, const uint8_t *m8, const double *aP, double ome
     }
 }
 
-// Fine excess dP = aP - (aE + aW + aN + aS) at level 0 (Float64 operator, 3-array storage).
-__device__ __forceinline__ double dP0(const double *aP, const double *aE, const double *aN, int nx, int ix, int iy,
-                                      size_t c) {
-    const double w = ix > 0 ? aE[c - 1] : 0.0, s = iy > 0 ? aN[c - nx] : 0.0;
-    return aP[c] - (aE[c] + w + aN[c] + s);
-}
-
-// Coarse operator of level l+1 from level l.  Fine inputs in Float64: aE, aN and either dP (fine
-// level >= 1) or aP (fine level 0, dP computed on the fly).
-__global__ void k_mg_coarsen(int nxf, int nyf, int nxc, int nyc, const double *aEf, const double *aNf,
-                             const double *dPf, const double *aPf, const uint8_t *actf, double *aEc, double *aNc,
-                             double *dPc, uint8_t *actc) {
-    GSTRIDE(k, nxc * nyc) {
-        const int I = k % nxc, J = k / nxc;
-        double d = 0.0, e = 0.0, no = 0.0;
-        int act = 0;
-        for (int dj = 0; dj < 2; dj++)
-            for (int di = 0; di < 2; di++) {
-                const int i = 2 * I + di, j = 2 * J + dj;
-                if (i >= nxf || j >= nyf) continue;
-                const size_t c = (size_t)i + (size_t)j * nxf;
-                if (!actf[c]) continue;
-                act = 1;
-                d += dPf ? dPf[c] : dP0(aPf, aEf, aNf, nxf, i, j, c);
-            }
-        const int ie = 2 * I + 1;  // fine column on the west side of the east aggregate boundary
-        if (ie + 1 < nxf)
-            for (int dj = 0; dj < 2; dj++) {
-                const int j = 2 * J + dj;
-                if (j >= nyf) continue;
-                const size_t c = (size_t)ie + (size_t)j * nxf;
-                if (actf[c] && actf[c + 1]) e += aEf[c];
-            }
-        const int jn = 2 * J + 1;
-        if (jn + 1 < nyf)
-            for (int di = 0; di < 2; di++) {
-                const int i = 2 * I + di;
-                if (i >= nxf) continue;
-                const size_t c = (size_t)i + (size_t)jn * nxf;
-                if (actf[c] && actf[c + nxf]) no += aNf[c];
-            }
-        aEc[k] = act ? e : 0.0;
-        aNc[k] = act ? no : 0.0;
-        dPc[k] = act ? d : 1.0;
-        actc[k] = (uint8_t)act;
-    }
-}
-
+// Coarse operator of level l+1 from level l (Galerkin sums over 2x2 aggregates, Float64): the
+// coarse excess dP is the sum of the active fine cells' excesses (dj outer, di inner); the coarse
+// east (north) coupling the sum of the fine aE (aN) across the aggregate's east (north) boundary
+// where both fine cells are active; inactive aggregates get dP = 1 and no couplings.
 // Level 0 of a hierarchy of two or more levels in one pass: per fine cell the Float32 Laplacian-form
 // operator (aE, aN, dP = aP - the four couplings) and the smoother's activity flag and damped
 // inverse diagonal (the arrays k_to_float_lapl and k_mg_act0 write), and per 2x2 aggregate the
-// level-1 Float64 operator (k_mg_coarsen's sums, in its order).  One thread per aggregate on a 2D
-// grid, so a warp reads 64 consecutive fine cells of each of its two rows.
+// level-1 Float64 operator (the sums above, dP computed from aP on the fly).  One thread per
+// aggregate on a 2D grid, so a warp reads 64 consecutive fine cells of each of its two rows.
 __global__ void __launch_bounds__(256) k_mg_level0(int nx, int ny, int nxc, int nyc, const uint8_t *m8,
                                                    const double *aP, const double *aE, const double *aN,
                                                    double omega, float *fE, float *fN, float *fD, float *fW,
@@ -152,10 +108,10 @@ __global__ void __launch_bounds__(256) k_mg_level0(int nx, int ny, int nxc, int 
     actc[k] = (uint8_t)act;
 }
 
-// k_mg_coarsen and k_mg_finish_level of coarse level l+1 (fine level l >= 1) in one pass.  The
-// finish needs the coarse west and south couplings of the neighbouring aggregates; each thread
-// recomputes them from the fine boundary they sum (same terms, same order), so the values are the
-// ones k_mg_coarsen would have stored.
+// The sums above and k_mg_finish_level's Float32 copies of coarse level l+1 (fine level l >= 1) in
+// one pass.  The damped diagonal needs the coarse west and south couplings of the neighbouring
+// aggregates; each thread recomputes them from the fine boundary they sum (same terms, same
+// order), so they equal the values those aggregates store.
 __global__ void k_mg_coarsen_finish(int nxf, int nyf, int nxc, int nyc, const double *aEf, const double *aNf,
                                     const double *dPf, const uint8_t *actf, double omega, double *aEc,
                                     double *aNc, double *dPc, uint8_t *actc, float *fE, float *fN, float *fD,
