@@ -1,6 +1,6 @@
 """CPU restatement (numpy) of the learned-warm-start network's forward and backward passes.
 
-TEST INFRASTRUCTURE ONLY: the checker of the GPU training kernels (shakti.jl_b200/csrc/shk_nn.cu,
+TEST INFRASTRUCTURE ONLY: the test oracle of the GPU training kernels (shakti.jl_b200/csrc/shk_nn.cu,
 driven by shakti.jl_b200/warmstart.py).  Nothing in the product imports it.
 
 It follows the GPU pass exactly, operation by operation, including where the GPU rounds to BF16

@@ -1,6 +1,6 @@
 """ctypes binding of the CPU restatement in oracle/shakti_oracle.c.
 
-TEST INFRASTRUCTURE ONLY: the checker for the CUDA library and the reported CPU baseline.  Only
+TEST INFRASTRUCTURE ONLY: the test oracle of the CUDA library and the reported CPU baseline.  Only
 tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module; the product
 path never does.
 

@@ -1,6 +1,6 @@
 /*
  * shakti_oracle.c -- CPU restatement (FP64, OpenMP) of Shakti.jl's per-timestep head solve and
- * field updates.  TEST INFRASTRUCTURE: the checker and the reported CPU baseline, never the product.
+ * field updates.  TEST INFRASTRUCTURE: the test oracle and the reported CPU baseline, never the product.
  *
  * Every function restates one reference kernel or driver, cited by file:line.  Each kernel is its
  * own loop (no fusion) and every arithmetic expression keeps the reference's evaluation order

@@ -1,8 +1,8 @@
 /*
  * shakti_oracle.h -- CPU restatement of Shakti.jl's per-timestep head solve and field updates.
  *
- * TEST INFRASTRUCTURE ONLY.  This header and oracle/shakti_oracle.c are the checker for the
- * CUDA library: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may link or
+ * TEST INFRASTRUCTURE ONLY.  This header and oracle/shakti_oracle.c are the test oracle of
+ * the CUDA library: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may link or
  * call them.  The product path (libshakti_b200.so) never does.
  *
  * Parity pinning: the reference (Julia) cannot run in this environment, and the reference holds no

@@ -1,7 +1,7 @@
 """Test configuration: registers the `gpu` marker and exposes the package and the oracle.
 
 `shakti_b200` is the package directory shakti.jl_b200/; `shakti_oracle` is oracle/oracle.py (the
-CPU restatement used as the checker)."""
+CPU restatement used as the test oracle)."""
 import sys
 from pathlib import Path
 
