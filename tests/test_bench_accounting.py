@@ -1,0 +1,28 @@
+"""bench.py's algorithmic byte counts (the roofline numerator), on CPU: per-cell figures of one CG
+iteration for each form, and the multigrid V-cycle's sum over the levels of a 4096^2 hierarchy
+(levels 1-5 on tile kernels, levels 6-12 in the one-block bottom kernel)."""
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT))
+
+import bench  # noqa: E402
+
+
+def test_plain_iteration_bytes():
+    n = 4096 * 4096
+    assert bench.iteration_bytes("plain", 4096, 4096) == 112 * n   # 14 Float64 words per cell
+    assert bench.iteration_bytes("fp32cg", 4096, 4096) == 56 * n    # the same words in Float32
+
+
+def test_multigrid_iteration_bytes(monkeypatch):
+    monkeypatch.delenv("SHK_MG_FUSED", raising=False)
+    n0 = 4096 * 4096
+    # matvec 56 B + level 0 (108 B: descending half with the CG update 70 B, ascending half 38 B)
+    # + levels 1-5 at 56 B per level cell + the bottom (25 B at level 6, 17 B below)
+    coarse = sum((4096 >> l) ** 2 for l in range(1, 6))
+    bottom = 25 * 64 * 64 + 17 * sum((64 >> k) ** 2 for k in range(1, 7))
+    expect = 56 * n0 + 108 * n0 + 56 * coarse + bottom
+    assert bench.iteration_bytes("multigrid", 4096, 4096) == expect
+    assert abs(expect / n0 - 182.66) < 0.01
