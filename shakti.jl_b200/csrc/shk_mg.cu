@@ -1253,20 +1253,29 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b
         if (iy > 0) y += sN[o + i - nx] * (xc - X[o + i - nx]);
         return y;
     };
-    // one damped-Jacobi sweep on level l: Y = X + wD (B - A X), then X = Y (sP holds wD)
-    auto sweep = [&](int l) {
+    // A level's iterate alternates between the two buffers, one damped-Jacobi sweep
+    // XO = XI + wD (B - A XI) per swap (sP holds wD): the level's iterate is in Xb[cur].  The
+    // descending half (the first sweep from zero into sX, nu - 1 more) leaves it in
+    // Xb[(nu - 1) & 1]; the ascending half (nu sweeps from there) in Xb[(2 nu - 1) & 1] = sY;
+    // the coarsest level's exact solve in sX.
+    float *Xb[2] = {sX, sY};
+    auto sweep = [&](int l, int cur) {
         const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
-        for (int i = tid; i < n; i += nt) sY[o + i] = sX[o + i] + sP[o + i] * (sB[o + i] - Ax(l, sX, i));
+        const float *XI = Xb[cur];
+        float *XO = Xb[cur ^ 1];
+        for (int i = tid; i < n; i += nt) XO[o + i] = XI[o + i] + sP[o + i] * (sB[o + i] - Ax(l, XI, i));
         __syncthreads();
-        for (int i = tid; i < n; i += nt) sX[o + i] = sY[o + i];
-        __syncthreads();
+        return cur ^ 1;
     };
     const int L = P.nlev;
+    const int cur_down = (nu - 1) & 1, cur_up = 1;
     for (int l = 0; l < L - 1; l++) {  // descend
         const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
         for (int i = tid; i < n; i += nt) sX[o + i] = sP[o + i] * sB[o + i];
         __syncthreads();
-        for (int s = 1; s < nu; s++) sweep(l);
+        int cur = 0;
+        for (int s = 1; s < nu; s++) cur = sweep(l, cur);
+        const float *XC = Xb[cur];
         const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, nxc = P.lv[l + 1].nx, nyc = P.lv[l + 1].ny, oc = P.lv[l + 1].off;
         for (int c = tid; c < nxc * nyc; c += nt) {
             const int I = c % nxc, J = c / nxc;
@@ -1277,7 +1286,7 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b
                     if (i >= nxf || j >= nyf) continue;
                     const int f = i + j * nxf;
                     if (!sA[o + f]) continue;
-                    sres += sB[o + f] - Ax(l, sX, f);
+                    sres += sB[o + f] - Ax(l, XC, f);
                 }
             sB[oc + c] = sres;
         }
@@ -1290,14 +1299,18 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b
     }
     for (int l = L - 2; l >= 0; l--) {  // ascend
         const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, o = P.lv[l].off, nxc = P.lv[l + 1].nx, oc = P.lv[l + 1].off;
+        float *XF = Xb[cur_down];
+        const float *XC = Xb[l + 1 == L - 1 ? 0 : cur_up];
         for (int f = tid; f < nxf * nyf; f += nt) {
             const int i = f % nxf, j = f / nxf;
-            if (sA[o + f]) sX[o + f] += wc * sX[oc + (i >> 1) + (j >> 1) * nxc];
+            if (sA[o + f]) XF[o + f] += wc * XC[oc + (i >> 1) + (j >> 1) * nxc];
         }
         __syncthreads();
-        for (int s = 0; s < nu; s++) sweep(l);
+        int cur = cur_down;
+        for (int s = 0; s < nu; s++) cur = sweep(l, cur);
     }
-    for (int i = tid; i < P.lv[0].nx * P.lv[0].ny; i += nt) x_top[i] = sX[i];
+    const float *X0 = Xb[L == 1 ? 0 : cur_up];
+    for (int i = tid; i < P.lv[0].nx * P.lv[0].ny; i += nt) x_top[i] = X0[i];
 }
 
 // ---------------------------------------------------------------------------------------------
