@@ -260,6 +260,35 @@ def iteration_bytes(form, nx, ny):
     return b
 
 
+# Whole-timestep algorithmic bytes per cell (Float64 words of the reference's data layout): a Picard
+# iteration's assembly, field tail and convergence check read 17 and write 24 fields (five
+# coefficient arrays, rhs, pw, N, the face gradients, fluxes, Reynolds numbers and stresses, the
+# melt terms, K) and write and read back h_prev: 43 words; a gap step reads 7 fields and writes 4.
+PICARD_BYTES, GAP_BYTES = 43 * 8, 11 * 8
+
+
+def step_bytes(form, nx, ny, counts):
+    """Algorithmic bytes of the timed window per timestep: every Picard iteration's field work,
+    every CG iteration of `form`, every gap step."""
+    cells = nx * ny
+    total = (counts["picard_iters"] * PICARD_BYTES * cells + counts["cg_iters"] * iteration_bytes(form, nx, ny)
+             + counts["steps"] * GAP_BYTES * cells)
+    return total / max(counts["steps"], 1)
+
+
+def step_roofline(form, w, counts, ms_per_step, peaks):
+    b = step_bytes(form, w.nx, w.ny, counts)
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = b / (ms_per_step / 1e3) / 1e9
+    return {"bound": "hbm", "bytes_per_step": int(b), "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "accounting": (f"per timestep: {counts['picard_iters']}/{counts['steps']} Picard iterations x "
+                           f"{PICARD_BYTES} B/cell (assembly, tail, check) + {counts['cg_iters']}/{counts['steps']} "
+                           f"CG iterations x {iteration_bytes(form, w.nx, w.ny) / (w.nx * w.ny):.1f} B/cell + "
+                           f"{GAP_BYTES} B/cell (gap step)"),
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s (of fallback)"}
+
+
 def measure_cg_iteration(shk, sim, form, short=20, long=220):
     """Average duration of one CG iteration of `form` (its matvec, update and, for the multigrid
     form, V-cycle kernels) on the current assembled system: CUDA events around a solve of exactly `long`
@@ -452,6 +481,7 @@ def ours(args, world, rank, local, pg):
                    "l2": "inputs larger than L2 (about 8 GB resident per GPU)",
                    "parallelism": f"replicas x{world} (independent instances, no data-path collective)"},
         "roofline": roofline,
+        "step_roofline": step_roofline(args.form, w, counts_of(main["rec"]), main["ms_max"] / args.steps, peaks),
         "plain_fp64_gpu": plain,
         "cpu_baseline": cpu,
         "e2e": e2e,

@@ -26,3 +26,17 @@ def test_multigrid_iteration_bytes(monkeypatch):
     expect = 56 * n0 + 108 * n0 + 56 * coarse + bottom
     assert bench.iteration_bytes("multigrid", 4096, 4096) == expect
     assert abs(expect / n0 - 182.66) < 0.01
+
+
+def test_step_bytes():
+    n = 4096 * 4096
+    counts = {"picard_iters": 46, "cg_iters": 160, "steps": 16}
+    expect = (46 * 43 * 8 * n + 160 * bench.iteration_bytes("multigrid", 4096, 4096) + 16 * 11 * 8 * n) / 16
+    assert bench.step_bytes("multigrid", 4096, 4096, counts) == expect
+
+    class W:
+        nx = ny = 4096
+
+    r = bench.step_roofline("multigrid", W, counts, 14.56, {"hbm_gbs": 6539.0})
+    assert r["peak"] == 6539.0 and abs(r["achieved"] - expect / 14.56e-3 / 1e9) < 0.1
+    assert r["peak_source"].endswith("(of measured)")
