@@ -92,7 +92,10 @@ typedef struct {
  * (src/linear_solver.jl:832-843) plus the Krylov.jl cg! keywords the reference leaves at their
  * defaults.
  *   stop_rule SHK_STOP_KRYLOV: sqrt(r'z) <= atol + rtol*sqrt(r0'z0) (Krylov.jl default rule)
- *   stop_rule SHK_STOP_RELRES: ||b - A x||_2 <= rtol*||b||_2 (the recursive residual)
+ *   stop_rule SHK_STOP_RELRES: ||b - A x||_2 <= rtol*||b_G||_2, the recursive residual over every
+ *     row against the GROUNDED rows of b (b_G).  The OCEAN/LAND/OTHER_BASIN rows are identity
+ *     rows holding a fixed head (~1e3 m), decoupled from the free heads; their residual is zero
+ *     once h holds the fixed value, and counted in ||b|| they would dominate it.
  *   precision SHK_FP64: every vector and coefficient in Float64
  *   precision SHK_MIXED: Float32 stencil and CG inside Float64 iterative refinement; the outer
  *     residual, the refinement update and the stopping test stay Float64 (rel-res rule only).
@@ -321,11 +324,12 @@ SHK_API int shk_nn_pack_state(const shk_state *st, int nx, int ny, int Hp, int W
 /* out = h + dh_scale * Yf[channel 0] on GROUNDED cells (mask 0), h elsewhere */
 SHK_API int shk_nn_apply_increment(const float *Yf, int C, int nx, int ny, int Wp, double dh_scale,
                                    const double *h, const double *mask, double *out, void *stream);
-/* ||rhs - A h||_2 and ||rhs||_2 of the elliptic system assembled at the context's current h (the
- * initial residual a Picard iteration would start from); assembles into the context's workspace. */
+/* ||rhs - A h||_2 (every row) and ||rhs||_2 (GROUNDED rows) of the elliptic system assembled at the
+ * context's current h (the initial residual a Picard iteration would start from); assembles into
+ * the context's workspace. */
 SHK_API int shk_initial_residual(void *ctx, double *rnorm, double *bnorm);
-/* ||rhs - A x||_2 (and ||rhs||_2) of the system last assembled in the context, for a device vector x
- * of nx*ny doubles. */
+/* ||rhs - A x||_2 (every row; and ||rhs||_2 over the GROUNDED rows) of the system last assembled in
+ * the context, for a device vector x of nx*ny doubles. */
 SHK_API int shk_residual_of(void *ctx, const double *x, double *rnorm, double *bnorm);
 /* `sweeps` damped Jacobi sweeps x <- x + omega (rhs - A x) / aP on the system last assembled in the
  * context (x and tmp: nx*ny doubles, device): removes the rough part of an initial guess's error. */
@@ -345,7 +349,8 @@ SHK_API int shk_set_cg_warm_start(void *ctx, const double *x0);
  * operator in this library's matrix-free form: aP, aE, aN (nx*ny doubles each; the west/south
  * couplings are the neighbours' east/north entries, exactly what shk_export_mfls writes), rhs,
  * and x (warm start in, solution out).  Only o->precond = SHK_PRECOND_JACOBI, o->precision =
- * SHK_FP64 are accepted.  stream may be NULL.
+ * SHK_FP64 are accepted.  stream may be NULL.  The operator carries no mask, so with
+ * SHK_STOP_RELRES ||rhs|| counts every row.
  *
  * Scratch (Krylov vectors, reduction partials, scalars) lives in one file-scope device array of
  * about 2.8 MB that every GPU loading the library holds until the process exits; nothing is

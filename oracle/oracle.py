@@ -77,7 +77,15 @@ class _PicardStats(C.Structure):
 class _Melt(C.Structure):
     _fields_ = [("kind", C.c_int)] + [(n, C.c_double) for n in
                                       ("t_start", "period", "omega", "amplitude", "offset", "i_min",
-                                       "seconds_per_year")]
+                                       "seconds_per_year")] + [("base", DP)]
+
+
+class _Progress(C.Structure):
+    _fields_ = [("steps_done", C.c_int), ("picard_iters", C.c_long), ("cg_iters", C.c_long),
+                ("cg_breakdowns", C.c_int), ("pic_iter_now", C.c_int), ("cg_iter_now", C.c_long),
+                ("elapsed", C.c_double), ("completed_s", C.c_double), ("step_s_now", C.c_double),
+                ("last_step_s", C.c_double), ("last_picard", C.c_int), ("last_cg", C.c_long),
+                ("last_converged", C.c_int), ("all_converged", C.c_int), ("total_time", C.c_double)]
 
 
 class _Sim(C.Structure):
@@ -117,6 +125,9 @@ def lib():
         L.orc_cg.argtypes = [C.c_int, C.c_int] + [DP] * 7 + [C.POINTER(_CgOpts), C.POINTER(_ChebState),
                                                               C.POINTER(_CgStats)]
         L.orc_cg.restype = C.c_int
+        L.orc_cg_masked.argtypes = [C.c_int, C.c_int] + [DP] * 8 + [C.POINTER(_CgOpts), C.POINTER(_ChebState),
+                                                                     C.POINTER(_CgStats)]
+        L.orc_cg_masked.restype = C.c_int
         L.orc_picard_tail.argtypes = [S, C.POINTER(_Params), C.POINTER(_Sliding)]
         L.orc_picard_iteration.argtypes = [S, C.POINTER(_Params), C.POINTER(_Sliding), C.c_int, C.POINTER(_CgOpts),
                                            C.POINTER(_ChebState), C.c_double, DP, C.POINTER(_CgStats)]
@@ -131,6 +142,13 @@ def lib():
                               C.POINTER(_CgOpts), C.POINTER(_ChebState), C.POINTER(_PicardOpts), C.c_int,
                               DP, C.POINTER(_PicardStats)]
         L.orc_run.restype = C.c_int
+        L.orc_session_create.argtypes = [S, C.POINTER(_Params), C.POINTER(_Sliding), C.POINTER(_Melt),
+                                         C.POINTER(_Sim), C.POINTER(_CgOpts), C.POINTER(_ChebState),
+                                         C.POINTER(_PicardOpts), C.c_double]
+        L.orc_session_create.restype = C.c_void_p
+        L.orc_session_advance.argtypes = [C.c_void_p, C.c_double, C.c_int, C.POINTER(_Progress)]
+        L.orc_session_advance.restype = C.c_int
+        L.orc_session_destroy.argtypes = [C.c_void_p]
         for name in ("orc_compute_face_masks", "orc_apply_mask_to_sliding", "orc_compute_H", "orc_compute_abs_ub",
                      "orc_compute_N", "orc_compute_dhdxy", "orc_compute_dpwdxy", "orc_compute_Re",
                      "orc_compute_b_xy"):
@@ -293,14 +311,19 @@ def chebyshev_apply(A: dict, degree: int, cheb: _ChebState, x: np.ndarray) -> np
     return y
 
 
-def cg(A: dict, x0: np.ndarray, spec: CgSpec, cheb: _ChebState | None = None):
-    """Krylov.jl cg! with warm start x0 on the assembled system; returns (x, stats dict)."""
+def cg(A: dict, x0: np.ndarray, spec: CgSpec, cheb: _ChebState | None = None, mask: np.ndarray | None = None):
+    """Krylov.jl cg! with warm start x0 on the assembled system; returns (x, stats dict).  With
+    `mask` (State.mask), the relative-residual rule divides by the GROUNDED rows' ||rhs|| only."""
     nx, ny = A["aP"].shape
     x = np.array(x0, dtype=np.float64, order="F", copy=True)
     cheb = cheb if cheb is not None else _ChebState(1.0, 1.0, 0)
     st = _CgStats()
-    lib().orc_cg(nx, ny, *[_ptr(A[k]) for k in ("aP", "aE", "aW", "aN", "aS", "rhs")], _ptr(x), C.byref(_cg(spec)),
-                 C.byref(cheb), C.byref(st))
+    ptrs = [_ptr(A[k]) for k in ("aP", "aE", "aW", "aN", "aS", "rhs")]
+    if mask is None:
+        lib().orc_cg(nx, ny, *ptrs, _ptr(x), C.byref(_cg(spec)), C.byref(cheb), C.byref(st))
+    else:
+        m = np.asfortranarray(mask, dtype=np.float64)
+        lib().orc_cg_masked(nx, ny, *ptrs, _ptr(m), _ptr(x), C.byref(_cg(spec)), C.byref(cheb), C.byref(st))
     return x, dict(niter=st.niter, status=st.status, rnorm0=st.rnorm0, rnorm=st.rnorm)
 
 
@@ -350,11 +373,34 @@ def step_b(st: OracleState, p: dict | None, gap_scheme: int, dt: float) -> None:
     lib().orc_step_b(C.byref(s), C.byref(params_struct(p)), int(gap_scheme), float(dt))
 
 
-def melt_struct(mi: dict | None) -> _Melt:
+def melt_struct(mi: dict | None, keep: list | None = None) -> _Melt:
+    """kind 0 constant, 1 seasonal (uniform), 2 seasonal plus mi['base'] (an (nx, ny) field)."""
     if not mi or mi.get("kind", 0) == 0:
-        return _Melt(0, 0, 0, 0, 0, 0, 0, 1)
-    return _Melt(1, mi["t_start"], mi["period"], mi["omega"], mi["amplitude"], mi["offset"], mi["i_min"],
-                 mi["seconds_per_year"])
+        return _Melt(0, 0, 0, 0, 0, 0, 0, 1, None)
+    base = None
+    if mi.get("base") is not None:
+        b = np.asfortranarray(mi["base"], dtype=np.float64)
+        if keep is not None:
+            keep.append(b)
+        base = _ptr(b)
+    return _Melt(2 if base is not None else 1, mi["t_start"], mi["period"], mi["omega"], mi["amplitude"],
+                 mi["offset"], mi["i_min"], mi["seconds_per_year"], base)
+
+
+def seasonal_melt(w_melt: dict) -> dict:
+    """The oracle melt spec of a workload's seasonal melt (t_start, t_end, amplitude, offset, i_min,
+    seconds_per_year and optional base), with period and omega derived as SeasonalMeltInput does
+    (src/melt_input.jl:49-66)."""
+    period = w_melt["t_end"] - w_melt["t_start"]
+    return dict(kind=1, t_start=w_melt["t_start"], period=period, omega=2 * math.pi / period,
+                amplitude=w_melt["amplitude"], offset=w_melt["offset"], i_min=w_melt["i_min"],
+                seconds_per_year=w_melt["seconds_per_year"], base=w_melt.get("base"))
+
+
+def update_ieb(st: OracleState, mi: dict | None, t: float) -> None:
+    keep = []
+    s = st.struct()
+    lib().orc_update_ieb(C.byref(s), C.byref(melt_struct(mi, keep)), float(t))
 
 
 def run(st: OracleState, p: dict | None, sl: SlidingSpec, tsteps: int, dt: float, *, kfs: int = 0,
@@ -371,7 +417,7 @@ def run(st: OracleState, p: dict | None, sl: SlidingSpec, tsteps: int, dt: float
     per = (_PicardStats * max(tsteps, 1))()
     tt = C.c_double(total_time)
     rc = lib().orc_run(C.byref(s), C.byref(params_struct(p)), C.byref(sliding_struct(sl, keep)),
-                       C.byref(melt_struct(melt)), C.byref(_Sim(head_scheme, gap_scheme, kfs, dt)),
+                       C.byref(melt_struct(melt, keep)), C.byref(_Sim(head_scheme, gap_scheme, kfs, dt)),
                        C.byref(_cg(cgspec or CgSpec())), C.byref(st.cheb),
                        C.byref(_PicardOpts(picard_iters, check_every, picard_tol, alpha)), int(tsteps),
                        C.byref(tt), per)
@@ -403,3 +449,43 @@ def direct_solve(A: dict) -> np.ndarray:
     M = sparse_matrix(A).tocsc()
     x = spla.spsolve(M, A["rhs"].ravel(order="F"))
     return x.reshape(A["aP"].shape, order="F")
+
+
+class RunSession:
+    """The run! loop (src/run.jl:37-43) as a resumable session: advance(seconds) spends about that
+    much wall time on it and stops between two CG iterations; nothing is recomputed on the next
+    call.  Same arguments and arithmetic as run()."""
+
+    def __init__(self, st: OracleState, p: dict | None, sl: SlidingSpec, dt: float, *, kfs: int = 0,
+                 gap_scheme: int = 1, head_scheme: int | None = None, cgspec: CgSpec | None = None,
+                 melt: dict | None = None, picard_iters: int = 500, picard_tol: float = 1e-6,
+                 alpha: float = float("nan"), check_every: int = 1, total_time: float = 0.0):
+        pp = dict(DEFAULT_PARAMS)
+        pp.update(p or {})
+        if head_scheme is None:
+            head_scheme = 0 if pp["e_v"] == 0.0 else 1
+        self._keep = [st]
+        self._s = st.struct()
+        self._h = lib().orc_session_create(
+            C.byref(self._s), C.byref(params_struct(p)), C.byref(sliding_struct(sl, self._keep)),
+            C.byref(melt_struct(melt, self._keep)), C.byref(_Sim(head_scheme, gap_scheme, kfs, dt)),
+            C.byref(_cg(cgspec or CgSpec())), C.byref(st.cheb),
+            C.byref(_PicardOpts(picard_iters, check_every, picard_tol, alpha)), float(total_time))
+
+    def advance(self, seconds: float, max_steps: int = 0) -> dict:
+        pr = _Progress()
+        more = lib().orc_session_advance(self._h, float(seconds), int(max_steps), C.byref(pr))
+        d = {name: getattr(pr, name) for name, _ in _Progress._fields_}
+        d["more"] = bool(more)
+        return d
+
+    def close(self) -> None:
+        if self._h:
+            lib().orc_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -21,6 +21,7 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -771,92 +772,151 @@ void orc_chebyshev_apply(int nx, int ny, const double *aP, const double *aE, con
  * Krylov.jl cg! (third-party, v0.10.8) restated: warm start x0 = Delta_x, x accumulates the
  * correction from 0 and Delta_x is added at the end.
  * ------------------------------------------------------------------------------------------- */
-int orc_cg(int nx, int ny, const double *aP, const double *aE, const double *aW, const double *aN,
-           const double *aS, const double *rhs, double *x_io, const orc_cg_opts *o, orc_cheb_state *cs,
-           orc_cg_stats *st) {
+/* Squared norm of rhs over the GROUNDED rows (mask == 0): the rows whose unknown is a free head.
+ * The OCEAN/LAND/OTHER_BASIN rows are identity rows (aP = 1, rhs = the fixed head), decoupled from
+ * the rest; their residual is zero once h holds their fixed value, and their rhs (heads of order
+ * 1e3 m) would otherwise dominate ||b||.  mask == NULL: every row. */
+static double free_norm2(size_t n, const double *rhs, const double *mask) {
+    if (!mask) return dot(n, rhs, rhs);
+    double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+    for (long i = 0; i < (long)n; i++) s += (mask[i] == GROUNDED) ? rhs[i] * rhs[i] : 0.0;
+    return s;
+}
+
+/* One Krylov.jl cg! solve as a resumable object: cg_begin (initial residual, preconditioner,
+ * stopping scalars), cg_step (one iteration), cg_end (x = Delta_x + x accumulated, statistics).
+ * orc_cg_masked runs them back to back; the bounded run session below interleaves them with
+ * clock checks.  The arithmetic and its order are those of one uninterrupted solve. */
+typedef struct {
+    int nx, ny;
+    size_t n;
+    const double *aP, *aE, *aW, *aN, *aS, *rhs;
+    double *x_io;
+    orc_cg_opts o;
+    orc_cheb_state *cs;
+    double *x, *r, *z, *p, *Ap, *cr, *cp, *cAp;
+    double gamma, rNorm, bNorm, rr, pNorm2, eps_stop, rnorm0;
+    long iter, itmax;
+    int solved, zero_curv, trivial;
+} cg_work;
+
+static void cg_apply_m(cg_work *w, double *dst, const double *src) {
+    if (w->o.precond == 1) {
+        cheb_apply_ws(w->nx, w->ny, w->aP, w->aE, w->aW, w->aN, w->aS, w->o.cheb_degree, w->cs, src, dst, w->cr, w->cp,
+                      w->cAp);
+    } else {
+        const double *aP = w->aP;
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)w->n; i++) dst[i] = src[i] / aP[i];
+    }
+}
+
+static void cg_begin(cg_work *w, int nx, int ny, const double *aP, const double *aE, const double *aW,
+                     const double *aN, const double *aS, const double *rhs, const double *mask, double *x_io,
+                     const orc_cg_opts *o, orc_cheb_state *cs) {
     const size_t n = (size_t)nx * ny;
-    double *x = calloc(n, sizeof(double)), *r = malloc(n * sizeof(double)), *z = malloc(n * sizeof(double));
-    double *p = malloc(n * sizeof(double)), *Ap = malloc(n * sizeof(double));
-    double *cr = NULL, *cp = NULL, *cAp = NULL;
+    memset(w, 0, sizeof(*w));
+    w->nx = nx; w->ny = ny; w->n = n;
+    w->aP = aP; w->aE = aE; w->aW = aW; w->aN = aN; w->aS = aS; w->rhs = rhs;
+    w->x_io = x_io; w->o = *o; w->cs = cs;
+    w->x = calloc(n, sizeof(double)); w->r = malloc(n * sizeof(double)); w->z = malloc(n * sizeof(double));
+    w->p = malloc(n * sizeof(double)); w->Ap = malloc(n * sizeof(double));
     if (o->precond == 1) {
-        cr = malloc(n * sizeof(double)); cp = malloc(n * sizeof(double)); cAp = malloc(n * sizeof(double));
+        w->cr = malloc(n * sizeof(double)); w->cp = malloc(n * sizeof(double)); w->cAp = malloc(n * sizeof(double));
         /* _cg_precond! refreshes the bounds from this solve's rhs (src/linear_solver.jl:853-856) */
         orc_update_chebyshev_bounds(nx, ny, aP, aE, aW, aN, aS, rhs, o->cheb_nsteps, cs, NULL);
     }
-#define APPLY_M(dst, src)                                                                     \
-    do {                                                                                      \
-        if (o->precond == 1)                                                                  \
-            cheb_apply_ws(nx, ny, aP, aE, aW, aN, aS, o->cheb_degree, cs, src, dst, cr, cp, cAp); \
-        else {                                                                                \
-            _Pragma("omp parallel for schedule(static)")                                      \
-            for (long i_ = 0; i_ < (long)n; i_++) dst[i_] = src[i_] / aP[i_];                 \
-        }                                                                                     \
-    } while (0)
-
+    double *r = w->r;
     /* r = b - A*Delta_x */
     orc_matvec(nx, ny, aP, aE, aW, aN, aS, x_io, r);
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < (long)n; i++) r[i] = 1.0 * rhs[i] + (-1.0) * r[i];
-    APPLY_M(z, r);
-    memcpy(p, z, n * sizeof(double));
-    double gamma = dot(n, r, z);
-    double rNorm = sqrt(gamma);
-    double bNorm = (o->stop_rule == 1) ? sqrt(dot(n, rhs, rhs)) : 0.0;
-    double rr = (o->stop_rule == 1) ? sqrt(dot(n, r, r)) : 0.0;
-    st->rnorm0 = (o->stop_rule == 1) ? rr : rNorm;
-    st->niter = 0;
-    st->status = 0;
-    if (gamma == 0) {
+    cg_apply_m(w, w->z, r);
+    memcpy(w->p, w->z, n * sizeof(double));
+    w->gamma = dot(n, r, w->z);
+    w->rNorm = sqrt(w->gamma);
+    w->bNorm = (o->stop_rule == 1) ? sqrt(free_norm2(n, rhs, mask)) : 0.0;
+    w->rr = (o->stop_rule == 1) ? sqrt(dot(n, r, r)) : 0.0;
+    w->rnorm0 = (o->stop_rule == 1) ? w->rr : w->rNorm;
+    if (w->gamma == 0) {
+        w->trivial = 1;
+        return;
+    }
+    w->itmax = o->itmax > 0 ? o->itmax : 2 * (long)n;
+    w->pNorm2 = w->gamma;
+    w->eps_stop = o->atol + o->rtol * w->rNorm;
+    w->solved = (o->stop_rule == 1) ? (w->rr <= o->rtol * w->bNorm) : (w->rNorm <= w->eps_stop);
+}
+
+static int cg_done(const cg_work *w) { return w->trivial || w->solved || w->iter >= w->itmax || w->zero_curv; }
+
+/* One iteration (callers test cg_done first). */
+static void cg_step(cg_work *w) {
+    const size_t n = w->n;
+    double *x = w->x, *r = w->r, *z = w->z, *p = w->p, *Ap = w->Ap;
+    orc_matvec(w->nx, w->ny, w->aP, w->aE, w->aW, w->aN, w->aS, p, Ap);
+    double pAp = dot(n, p, Ap);
+    if (pAp <= DBL_EPSILON * w->pNorm2 && fabs(pAp) <= DBL_EPSILON * w->pNorm2) { w->zero_curv = 1; return; }
+    if (isnan(pAp)) { w->zero_curv = 1; return; }
+    double alpha = w->gamma / pAp;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)n; i++) {
+        x[i] += alpha * p[i];
+        r[i] += (-alpha) * Ap[i];
+    }
+    cg_apply_m(w, z, r);
+    double gamma_next = dot(n, r, z);
+    w->rNorm = sqrt(gamma_next);
+    if (w->o.stop_rule == 1) {
+        w->rr = sqrt(dot(n, r, r));
+        w->solved = w->rr <= w->o.rtol * w->bNorm;
+    } else {
+        w->solved = (w->rNorm <= w->eps_stop) || (w->rNorm + 1.0 <= 1.0);
+    }
+    if (!w->solved) {
+        double beta = gamma_next / w->gamma;
+        w->pNorm2 = gamma_next + beta * beta * w->pNorm2;
+        w->gamma = gamma_next;
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)n; i++) p[i] = 1.0 * z[i] + beta * p[i];
+    }
+    w->iter++;
+}
+
+static int cg_end(cg_work *w, orc_cg_stats *st) {
+    const size_t n = w->n;
+    double *x = w->x, *x_io = w->x_io;
+    st->rnorm0 = w->rnorm0;
+    if (w->trivial) {
+        st->niter = 0;
+        st->status = 0;
         st->rnorm = 0.0;
-#pragma omp parallel for schedule(static)
-        for (long i = 0; i < (long)n; i++) x_io[i] = x[i] + x_io[i];
-        goto done;
+    } else {
+        st->niter = w->iter;
+        st->rnorm = (w->o.stop_rule == 1) ? w->rr : w->rNorm;
+        st->status = w->zero_curv ? 2 : (w->solved ? 0 : 1);
     }
-    long itmax = o->itmax > 0 ? o->itmax : 2 * (long)n;
-    double pNorm2 = gamma;
-    double eps_stop = o->atol + o->rtol * rNorm;
-    int solved = (o->stop_rule == 1) ? (rr <= o->rtol * bNorm) : (rNorm <= eps_stop);
-    long iter = 0;
-    int zero_curv = 0;
-    while (!(solved || iter >= itmax || zero_curv)) {
-        orc_matvec(nx, ny, aP, aE, aW, aN, aS, p, Ap);
-        double pAp = dot(n, p, Ap);
-        if (pAp <= DBL_EPSILON * pNorm2 && fabs(pAp) <= DBL_EPSILON * pNorm2) { zero_curv = 1; break; }
-        if (isnan(pAp)) { zero_curv = 1; break; }
-        double alpha = gamma / pAp;
-#pragma omp parallel for schedule(static)
-        for (long i = 0; i < (long)n; i++) {
-            x[i] += alpha * p[i];
-            r[i] += (-alpha) * Ap[i];
-        }
-        APPLY_M(z, r);
-        double gamma_next = dot(n, r, z);
-        rNorm = sqrt(gamma_next);
-        if (o->stop_rule == 1) {
-            rr = sqrt(dot(n, r, r));
-            solved = rr <= o->rtol * bNorm;
-        } else {
-            solved = (rNorm <= eps_stop) || (rNorm + 1.0 <= 1.0);
-        }
-        if (!solved) {
-            double beta = gamma_next / gamma;
-            pNorm2 = gamma_next + beta * beta * pNorm2;
-            gamma = gamma_next;
-#pragma omp parallel for schedule(static)
-            for (long i = 0; i < (long)n; i++) p[i] = 1.0 * z[i] + beta * p[i];
-        }
-        iter++;
-    }
-    st->niter = iter;
-    st->rnorm = (o->stop_rule == 1) ? rr : rNorm;
-    st->status = zero_curv ? 2 : (solved ? 0 : 1);
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < (long)n; i++) x_io[i] = x[i] + x_io[i];
-done:
-#undef APPLY_M
-    free(x); free(r); free(z); free(p); free(Ap);
-    free(cr); free(cp); free(cAp);
+    free(w->x); free(w->r); free(w->z); free(w->p); free(w->Ap);
+    free(w->cr); free(w->cp); free(w->cAp);
     return st->status;
+}
+
+int orc_cg(int nx, int ny, const double *aP, const double *aE, const double *aW, const double *aN,
+           const double *aS, const double *rhs, double *x_io, const orc_cg_opts *o, orc_cheb_state *cs,
+           orc_cg_stats *st) {
+    return orc_cg_masked(nx, ny, aP, aE, aW, aN, aS, rhs, NULL, x_io, o, cs, st);
+}
+
+int orc_cg_masked(int nx, int ny, const double *aP, const double *aE, const double *aW, const double *aN,
+                  const double *aS, const double *rhs, const double *mask, double *x_io, const orc_cg_opts *o,
+                  orc_cheb_state *cs, orc_cg_stats *st) {
+    cg_work w;
+    cg_begin(&w, nx, ny, aP, aE, aW, aN, aS, rhs, mask, x_io, o, cs);
+    while (!cg_done(&w)) cg_step(&w);
+    return cg_end(&w, st);
 }
 
 /* ---------------------------------------------------------------------------------------------
@@ -883,7 +943,7 @@ static int solve_linear(orc_state *s, const orc_params *p, int kfs, int paraboli
     double *buf = malloc(6 * n * sizeof(double));
     double *aP = buf, *aE = buf + n, *aW = buf + 2 * n, *aN = buf + 3 * n, *aS = buf + 4 * n, *rhs = buf + 5 * n;
     orc_assemble_mfls(s, p, kfs, parabolic, dt, aP, aE, aW, aN, aS, rhs);
-    int rc = orc_cg(s->nx, s->ny, aP, aE, aW, aN, aS, rhs, s->h, cg, cs, cst);
+    int rc = orc_cg_masked(s->nx, s->ny, aP, aE, aW, aN, aS, rhs, s->mask, s->h, cg, cs, cst);
     free(buf);
     return rc;
 }
@@ -950,7 +1010,7 @@ int orc_parabolic_step(orc_state *s, const orc_params *p, const orc_sliding *sl,
 
 /* update_ieb! (src/melt_input.jl:30, :86-94) */
 void orc_update_ieb(orc_state *s, const orc_melt *mi, double t) {
-    if (mi->kind != 1) return;
+    if (mi->kind != 1 && mi->kind != 2) return;
     double yf = fmod(t / mi->seconds_per_year, 1.0);
     if (yf < 0) yf += 1.0;
     double i_ma = (mi->t_start <= yf && yf <= mi->t_start + mi->period)
@@ -958,7 +1018,13 @@ void orc_update_ieb(orc_state *s, const orc_melt *mi, double t) {
                       : mi->i_min;
     const double v = i_ma / mi->seconds_per_year;
     const size_t n = (size_t)s->nx * s->ny;
-    for (size_t i = 0; i < n; i++) s->ieb[i] = v;
+    if (mi->kind == 2 && mi->base) {
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)n; i++) s->ieb[i] = v + mi->base[i];
+    } else {
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)n; i++) s->ieb[i] = v;
+    }
 }
 
 /* run! loop body (src/run.jl:37-43) over step! (:82-88). */
@@ -987,4 +1053,158 @@ int orc_run(orc_state *s, const orc_params *p, const orc_sliding *sl, const orc_
         if (per_step) per_step[t] = pst;
     }
     return worst;
+}
+
+/* ---------------------------------------------------------------------------------------------
+ * Bounded run session: the run! loop above (update_ieb!, Picard_loop! or parabolic_solver!,
+ * step_b!) executed as a resumable sequence, so that a caller can spend a fixed amount of wall
+ * time on it, stop between two CG iterations, and continue later with nothing recomputed.  The
+ * arithmetic is that of orc_run.  Used to time the CPU restatement on workloads whose timesteps
+ * take longer than a benchmark can wait for.
+ * ------------------------------------------------------------------------------------------- */
+enum { SES_STEP_START = 0, SES_SOLVE_START = 1, SES_CG = 2, SES_STEP_END = 3 };
+
+struct orc_session {
+    orc_state *s;
+    orc_params p;
+    orc_sliding sl;
+    orc_melt mi;
+    orc_sim sim;
+    orc_cg_opts cg;
+    orc_picard_opts po;
+    orc_cheb_state *cs;
+    double total_time;
+    double *sys;     /* aP, aE, aW, aN, aS, rhs */
+    double *h_prev;
+    cg_work w;
+    int phase, pic_iter, step_converged;
+    long step_cg;
+    double step_s;   /* seconds spent on the timestep in progress */
+    orc_session_progress pr;
+};
+
+static double wtime(void) {
+#ifdef _OPENMP
+    return omp_get_wtime();
+#else
+    return (double)clock() / CLOCKS_PER_SEC;
+#endif
+}
+
+orc_session *orc_session_create(orc_state *s, const orc_params *p, const orc_sliding *sl, const orc_melt *mi,
+                                const orc_sim *sim, const orc_cg_opts *cg, orc_cheb_state *cs,
+                                const orc_picard_opts *po, double total_time) {
+    orc_session *S = calloc(1, sizeof(orc_session));
+    const size_t n = (size_t)s->nx * s->ny;
+    S->s = s; S->p = *p; S->sl = *sl; S->mi = *mi; S->sim = *sim; S->cg = *cg; S->po = *po; S->cs = cs;
+    S->total_time = total_time;
+    S->sys = malloc(6 * n * sizeof(double));
+    S->h_prev = malloc(n * sizeof(double));
+    S->phase = SES_STEP_START;
+    S->pr.all_converged = 1;
+    return S;
+}
+
+void orc_session_destroy(orc_session *S) {
+    if (!S) return;
+    if (S->phase == SES_CG) {
+        orc_cg_stats st;
+        cg_end(&S->w, &st);
+    }
+    free(S->sys);
+    free(S->h_prev);
+    free(S);
+}
+
+/* Advances the run by about `seconds` of wall time (it stops at the first CG-iteration, solve or
+ * timestep boundary after the budget; max_steps > 0 also stops it after that many completed
+ * timesteps in total).  Returns 1 while the run has more to do, 0 once max_steps are complete. */
+int orc_session_advance(orc_session *S, double seconds, int max_steps, orc_session_progress *out) {
+    orc_state *s = S->s;
+    const size_t n = (size_t)s->nx * s->ny;
+    const double t0 = wtime();
+    double mark = t0;
+    int more = 1;
+    const int check_every = S->po.check_every > 0 ? S->po.check_every : 1;
+    for (;;) {
+        if (max_steps > 0 && S->pr.steps_done >= max_steps) { more = 0; break; }
+        if (wtime() - t0 >= seconds) break;
+        if (S->phase == SES_STEP_START) {
+            orc_update_ieb(s, &S->mi, S->total_time);
+            S->pic_iter = 0;
+            S->step_cg = 0;
+            S->step_converged = S->sim.head_scheme == 0 ? 0 : -1;
+            S->phase = SES_SOLVE_START;
+        } else if (S->phase == SES_SOLVE_START) {
+            double *b = S->sys;
+            const int parabolic = S->sim.head_scheme != 0;
+            S->pic_iter++;
+            if (!parabolic) memcpy(S->h_prev, s->h, n * sizeof(double));
+            orc_assemble_mfls(s, &S->p, S->sim.kfs, parabolic, parabolic ? S->sim.dt : 0.0, b, b + n, b + 2 * n,
+                              b + 3 * n, b + 4 * n, b + 5 * n);
+            cg_begin(&S->w, s->nx, s->ny, b, b + n, b + 2 * n, b + 3 * n, b + 4 * n, b + 5 * n, s->mask, s->h,
+                     &S->cg, S->cs);
+            S->pr.cg_iter_now = 0;
+            S->phase = SES_CG;
+        } else if (S->phase == SES_CG) {
+            if (!cg_done(&S->w)) {
+                cg_step(&S->w);
+                S->pr.cg_iters++;
+                S->pr.cg_iter_now++;
+                S->step_cg++;
+                continue;
+            }
+            orc_cg_stats cst;
+            cg_end(&S->w, &cst);
+            if (cst.status == 2) S->pr.cg_breakdowns++;
+            S->pr.picard_iters++;
+            if (S->sim.head_scheme != 0) {
+                orc_picard_tail(s, &S->p, &S->sl);
+                S->phase = SES_STEP_END;
+                continue;
+            }
+            const double alpha = S->po.alpha;
+            if (alpha > 0) { /* relax_h! (src/elliptic_solver.jl:42-46) */
+#pragma omp parallel for schedule(static)
+                for (long i = 0; i < (long)n; i++) s->h[i] = alpha * s->h[i] + (1 - alpha) * S->h_prev[i];
+            }
+            orc_picard_tail(s, &S->p, &S->sl);
+            int stop = S->pic_iter >= S->po.iters;
+            if (S->pic_iter % check_every == 0 || S->pic_iter == S->po.iters) {
+                double dmax = 0.0, hmax = 0.0;
+                for (size_t i = 0; i < n; i++) {
+                    dmax = jl_max(dmax, fabs(s->h[i] - S->h_prev[i]));
+                    hmax = jl_max(hmax, fabs(s->h[i]));
+                }
+                if (dmax / (hmax + DBL_EPSILON) < S->po.tol) {
+                    S->step_converged = 1;
+                    stop = 1;
+                }
+            }
+            S->phase = stop ? SES_STEP_END : SES_SOLVE_START;
+        } else { /* SES_STEP_END */
+            orc_step_b(s, &S->p, S->sim.gap_scheme, S->sim.dt);
+            S->total_time += S->sim.dt;
+            const double now = wtime();
+            S->step_s += now - mark;
+            mark = now;
+            S->pr.steps_done++;
+            S->pr.completed_s += S->step_s;
+            S->pr.last_step_s = S->step_s;
+            S->pr.last_picard = S->pic_iter;
+            S->pr.last_cg = S->step_cg;
+            S->pr.last_converged = S->step_converged;
+            if (S->step_converged == 0) S->pr.all_converged = 0;
+            S->step_s = 0.0;
+            S->phase = SES_STEP_START;
+        }
+    }
+    const double now = wtime();
+    S->step_s += now - mark;
+    S->pr.elapsed += now - t0;
+    S->pr.pic_iter_now = S->phase == SES_STEP_START ? 0 : S->pic_iter;
+    S->pr.step_s_now = S->step_s;
+    S->pr.total_time = S->total_time;
+    if (out) *out = S->pr;
+    return more;
 }

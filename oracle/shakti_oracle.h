@@ -58,7 +58,8 @@ typedef struct {
 
 /* CG options: precond 0 = Jacobi (Diagonal(aP)), 1 = ChebyshevPreconditioner.
  * stop_rule 0 = Krylov.jl cg! default: sqrt(r'z) <= atol + rtol*sqrt(r0'z0) (z = M^-1 r).
- * stop_rule 1 = unpreconditioned relative residual ||r||_2 <= rtol*||b||_2 (atol ignored).
+ * stop_rule 1 = unpreconditioned relative residual ||r||_2 <= rtol*||b_G||_2 (atol ignored), b_G the
+ *               GROUNDED rows of b when a mask is given (orc_cg_masked and the Picard drivers).
  * itmax <= 0 means Krylov's default 2*n. */
 typedef struct {
     int precond, cheb_degree, cheb_nsteps, stop_rule;
@@ -136,6 +137,12 @@ void orc_chebyshev_apply(int nx, int ny, const double *aP, const double *aE, con
 int orc_cg(int nx, int ny, const double *aP, const double *aE, const double *aW, const double *aN,
            const double *aS, const double *rhs, double *x, const orc_cg_opts *o, orc_cheb_state *cs,
            orc_cg_stats *st);
+/* orc_cg with the relative-residual rule (stop_rule 1) measured against the GROUNDED rows of rhs
+ * only: ||rhs - A x||_2 (every row) <= rtol * ||rhs restricted to mask == GROUNDED||_2.  mask NULL:
+ * every row counts, as in orc_cg.  The Picard and parabolic drivers pass State.mask. */
+int orc_cg_masked(int nx, int ny, const double *aP, const double *aE, const double *aW, const double *aN,
+                  const double *aS, const double *rhs, const double *mask, double *x, const orc_cg_opts *o,
+                  orc_cheb_state *cs, orc_cg_stats *st);
 
 /* Picard / parabolic / gap / melt input / run loop */
 typedef struct {
@@ -151,10 +158,13 @@ typedef struct {
     int cg_breakdowns;
 } orc_picard_stats;
 
-/* Melt input (src/melt_input.jl).  kind 0 Constant, 1 Seasonal (uniform fill). */
+/* Melt input (src/melt_input.jl).  kind 0 Constant, 1 Seasonal (uniform fill), 2 Seasonal plus a
+ * fixed spatial field `base` (nx*ny, m/s; the library's SeasonalBaseMeltInput extension: ieb =
+ * seasonal value + base, e.g. point moulins). */
 typedef struct {
     int kind;
     double t_start, period, omega, amplitude, offset, i_min, seconds_per_year;
+    const double *base;
 } orc_melt;
 
 void orc_update_ieb(orc_state *s, const orc_melt *mi, double t);
@@ -186,6 +196,32 @@ typedef struct {
 int orc_run(orc_state *s, const orc_params *p, const orc_sliding *sl, const orc_melt *mi,
             const orc_sim *sim, const orc_cg_opts *cg, orc_cheb_state *cs, const orc_picard_opts *po,
             int tsteps, double *total_time, orc_picard_stats *per_step /* tsteps entries or NULL */);
+
+/* Bounded run session: the orc_run loop, resumable between CG iterations (see the .c file). */
+typedef struct {
+    int steps_done;          /* completed timesteps                                        */
+    long picard_iters;       /* completed linear solves (Picard iterations) in total       */
+    long cg_iters;           /* CG iterations in total (including the solve in progress)   */
+    int cg_breakdowns;
+    int pic_iter_now;        /* Picard iteration in progress (0 between timesteps)         */
+    long cg_iter_now;        /* CG iterations of the solve in progress                     */
+    double elapsed;          /* wall seconds spent inside orc_session_advance              */
+    double completed_s;      /* wall seconds of the completed timesteps                    */
+    double step_s_now;       /* wall seconds spent on the timestep in progress             */
+    double last_step_s;      /* the last completed timestep: seconds, Picard, CG, converged */
+    int last_picard;
+    long last_cg;
+    int last_converged;
+    int all_converged;
+    double total_time;
+} orc_session_progress;
+
+typedef struct orc_session orc_session;
+orc_session *orc_session_create(orc_state *s, const orc_params *p, const orc_sliding *sl, const orc_melt *mi,
+                                const orc_sim *sim, const orc_cg_opts *cg, orc_cheb_state *cs,
+                                const orc_picard_opts *po, double total_time);
+int orc_session_advance(orc_session *S, double seconds, int max_steps, orc_session_progress *out);
+void orc_session_destroy(orc_session *S);
 
 #ifdef __cplusplus
 }

@@ -63,10 +63,14 @@ __global__ void __launch_bounds__(kThreads) k_matvec(int nx, int ny, const T *aP
 
 // r = b - A x0 (x0 == nullptr: r = b), x = 0; JAC: partials r'z, r'r, b'b -> init finish;
 // otherwise partials r'r, b'b are parked for the Chebyshev init pass.
+// b'b is summed over the GROUNDED rows only when fmask (the uint8 mask) is given: the relative-
+// residual rule measures ||b - A x|| (every row) against the rows whose unknown is a free head.  The
+// OCEAN/LAND/OTHER_BASIN rows are identity rows holding a fixed head (of order 1e3 m), decoupled
+// from the rest; counted in ||b|| they would loosen "1e-8" to about 1e-3 on the free rows.
 template <typename T, bool JAC>
 __device__ __forceinline__ void cg_init_body(Blk B, int nx, int ny, const T *aP, const T *aE, const T *aN,
                                              const double *x0, const T *b, T *r, T *x, CgDev *cg, double *partials,
-                                             unsigned int *counter) {
+                                             unsigned int *counter, const uint8_t *fmask) {
     Tiles Tl(nx, ny);
     double red[3] = {0.0, 0.0, 0.0};
     for (int t = B.id; t < Tl.ntiles; t += B.n) {
@@ -89,7 +93,7 @@ __device__ __forceinline__ void cg_init_body(Blk B, int nx, int ny, const T *aP,
             red[0] += (double)rc * (double)zc;
         }
         red[1] += (double)rc * (double)rc;
-        red[2] += (double)bc * (double)bc;
+        if (!fmask || fmask[c] == M_GROUNDED) red[2] += (double)bc * (double)bc;
     }
     double out[3];
     if (grid_reduce<3, false>(B, red, partials, counter, out) && threadIdx.x == 0) {
@@ -104,8 +108,8 @@ __device__ __forceinline__ void cg_init_body(Blk B, int nx, int ny, const T *aP,
 template <typename T, bool JAC>
 __global__ void __launch_bounds__(kThreads) k_cg_init(int nx, int ny, const T *aP, const T *aE, const T *aN,
                                                       const double *x0, const T *b, T *r, T *x, CgDev *cg,
-                                                      double *partials, unsigned int *counter) {
-    cg_init_body<T, JAC>(grid_blk(), nx, ny, aP, aE, aN, x0, b, r, x, cg, partials, counter);
+                                                      double *partials, unsigned int *counter, const uint8_t *fmask) {
+    cg_init_body<T, JAC>(grid_blk(), nx, ny, aP, aE, aN, x0, b, r, x, cg, partials, counter, fmask);
 }
 
 // A: p_new = z + beta*p_old (p_new = z on the first iteration), Ap = A p_new, partial p'Ap.
@@ -399,10 +403,12 @@ int jacobi_smooth(Ctx *c, double *x, double *tmp, int sweeps, double omega) {
     return check_launch(c, "jacobi smoothing");
 }
 
-// ||rhs - A x||^2 and ||rhs||^2 of the assembled system for a given x (Float64)
+// ||rhs - A x||^2 (every row) and ||rhs||^2 over the GROUNDED rows of the assembled system for a
+// given x (Float64)
 __global__ void __launch_bounds__(kThreads) k_residual_of(int nx, int ny, const double *aP, const double *aE,
                                                           const double *aN, const double *x, const double *b,
-                                                          DevScalars *dv, double *partials, unsigned int *counter) {
+                                                          DevScalars *dv, double *partials, unsigned int *counter,
+                                                          const uint8_t *fmask) {
     Tiles Tl(nx, ny);
     double red[2] = {0.0, 0.0};
     for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
@@ -413,7 +419,7 @@ __global__ void __launch_bounds__(kThreads) k_residual_of(int nx, int ny, const 
         double ax = stencil_apply(aP, aE, aN, nx, ny, ix, iy, c, x[c], [&](size_t k) { return x[k]; });
         double rc = b[c] - ax;
         red[0] += rc * rc;
-        red[1] += b[c] * b[c];
+        if (!fmask || fmask[c] == M_GROUNDED) red[1] += b[c] * b[c];
     }
     double out[2];
     if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
@@ -650,11 +656,12 @@ __global__ void k_to_float_lapl(int nx, int ny, const double *aP, const double *
     }
 }
 
-// r32 = float(b - A h) with Float64 operator; partials ||r||^2, ||b||^2 (outer residual).
+// r32 = float(b - A h) with Float64 operator; partials ||r||^2 (every row), ||b||^2 (GROUNDED
+// rows) of the outer residual.
 __global__ void __launch_bounds__(kThreads) k_outer_residual(int nx, int ny, const double *aP, const double *aE,
                                                              const double *aN, const double *h, const double *b,
                                                              float *r32, DevScalars *dv, double *partials,
-                                                             unsigned int *counter) {
+                                                             unsigned int *counter, const uint8_t *fmask) {
     Tiles Tl(nx, ny);
     double red[2] = {0.0, 0.0};
     for (int t = blockIdx.x; t < Tl.ntiles; t += gridDim.x) {
@@ -666,7 +673,7 @@ __global__ void __launch_bounds__(kThreads) k_outer_residual(int nx, int ny, con
         double rc = b[c] - ax;
         r32[c] = (float)rc;
         red[0] += rc * rc;
-        red[1] += b[c] * b[c];
+        if (!fmask || fmask[c] == M_GROUNDED) red[1] += b[c] * b[c];
     }
     double out[2];
     if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
@@ -705,7 +712,7 @@ static int stream_grid(Ctx *c, long long n, size_t elem) {
 // ||rhs - A x||_2 and ||rhs||_2 of the assembled system (x: the current h when null; Float64).
 int residual_norms(Ctx *c, const double *x, double *rnorm, double *bnorm) {
     k_residual_of<<<c->grid_stencil, kThreads, 0, c->stream>>>(c->nx, c->ny, c->aP, c->aE, c->aN, x ? x : c->st.h,
-                                                              c->rhs, c->dev, c->partials, c->counter);
+                                                              c->rhs, c->dev, c->partials, c->counter, c->mask8);
     c->launches++;
     int rc = check_launch(c, "residual norm");
     if (rc) return rc;
@@ -870,11 +877,11 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
     cudaError_t e = cudaSuccess;
     if (jac) {
         k_cg_init<T, true><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, aP, aE, aN, x0, b, r, x, cgd, c->partials,
-                                                                       c->counter);
+                                                                       c->counter, c->mask8);
         c->launches++;
     } else {
         k_cg_init<T, false><<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, aP, aE, aN, x0, b, r, x, cgd,
-                                                                        c->partials, c->counter);
+                                                                        c->partials, c->counter, c->mask8);
         c->launches++;
         int prc = apply_precond(true);
         if (prc) return prc;
@@ -1151,7 +1158,8 @@ int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
         CgDev *cgh = &c->host_dev->cg_in;
         for (;;) {
             k_outer_residual<<<c->grid_stencil, kThreads, 0, c->stream>>>(nx, ny, c->aP, c->aE, c->aN, c->st.h, c->rhs,
-                                                                         c->b32, c->dev, c->partials, c->counter);
+                                                                         c->b32, c->dev, c->partials, c->counter,
+                                                                         c->mask8);
             c->launches++;
             int rc = read_scalars(c);
             if (rc) return rc;
@@ -1316,7 +1324,7 @@ __global__ void __launch_bounds__(kThreads) k_ens_cg_init(EnsInst *E, const int 
     const Blk B = ens_stage(I, E, b2i, EF_STENCIL);
     if (!I.pic_active) return;
     cg_init_body<double, true>(B, I.nx, I.ny, I.aP, I.aE, I.aN, I.st.h, I.rhs, I.r, I.x, I.cg, I.partials,
-                               I.counter);
+                               I.counter, I.mask8);
 }
 
 __global__ void __launch_bounds__(kMarchX, 6) k_ens_cg_A(EnsInst *E, const int *b2i, int parity) {
@@ -1454,7 +1462,8 @@ extern "C" SHK_API int shk_cg_solve_static(int nx, int ny, const double *aP, con
     init.stop_rule = o->stop_rule;
     init.first = 1;
     k_static_init<<<1, 32, 0, s>>>(cg, init, counter);
-    k_cg_init<double, true><<<grid_stencil, kThreads, 0, s>>>(nx, ny, aP, aE, aN, x, rhs, r, xc, cg, partials, counter);
+    k_cg_init<double, true><<<grid_stencil, kThreads, 0, s>>>(nx, ny, aP, aE, aN, x, rhs, r, xc, cg, partials, counter,
+                                                              nullptr);
     if (cudaGetLastError() != cudaSuccess) return SHK_CUDA_ERROR;
     CgDev h;
     long long enq = 0;

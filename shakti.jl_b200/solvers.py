@@ -197,7 +197,8 @@ class CGIterativeSolver(AbstractIterativeSolver):
     """CGIterativeSolver(g, MatrixFreeLinearSystem; chebyshev_degree, chebyshev_nsteps_estimate)
     (src/linear_solver.jl:760-843), with Krylov.jl's cg! keywords exposed:
       atol, rtol, itmax -- Krylov defaults sqrt(eps), sqrt(eps), 2n; stop_rule "krylov" is Krylov's
-      preconditioned-norm test, "relres" the unpreconditioned ||b - A x|| <= rtol ||b||.
+      preconditioned-norm test, "relres" the unpreconditioned ||b - A x|| <= rtol ||b_G|| (residual
+      over every row, b over the GROUNDED rows: the fixed-head rows would otherwise dominate ||b||).
       precision "fp64" (plain) or "mixed" (Float32 stencil + CG inside Float64 iterative refinement;
       relres rule; inner_rtol is the inner Float32 solve's relative tolerance)."""
 
