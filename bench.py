@@ -5,14 +5,16 @@ workload, rel-res 1e-8 linear solves, on 1..N GPUs (one independent replica inst
                     [--impl ours|reference]
 
 One step is one timestep (update_ieb!, Picard to convergence with every CG solve at
-||b - A h||_2 <= 1e-8 ||b||_2, step_b!).  `value` times K device-resident steps of the chosen form
-(default: Float64 CG preconditioned by the Float32 aggregation-multigrid V-cycle) with CUDA events
-after W warm-up steps; `plain_fp64_gpu` times the same window with plain Float64 Jacobi CG (the
-reference's algorithm on the GPU); `e2e` re-runs the chosen form's K steps from the same state
-through the public API (`HostIO.run`) with each step's forcing (the ieb field) copied in from
-pinned host memory and the step's result (h and b) copied back, the copies overlapping the
-neighbouring steps' computation.  The reference arm (--impl reference) times the CPU
-restatement of the reference algorithm on the host cores.
+||b - A h||_2 <= 1e-8 ||b_G||_2, b_G the GROUNDED rows of b, step_b!).  `value` times K
+device-resident steps of the chosen form (default: Float64 CG preconditioned by the Float32
+aggregation-multigrid V-cycle) with CUDA events after W warm-up steps; `plain_fp64_gpu` times plain
+Float64 Jacobi CG (the reference's algorithm on the GPU) over the window's first --plain-steps
+timesteps, from the same state, beside the chosen form's own time for those timesteps; `e2e`
+re-runs the chosen form's K steps from the same state through the public API (`HostIO.run`) with
+each step's forcing (the ieb field) copied in from pinned host memory and the step's result (h and
+b) copied back, the copies overlapping the neighbouring steps' computation.  `cpu_baseline` and
+the reference arm (--impl reference) run the CPU restatement of the reference algorithm's real
+run loop on the host cores for a bounded time.
 """
 from __future__ import annotations
 
@@ -52,13 +54,18 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="multigrid", choices=list(FORMS))
     ap.add_argument("--no-plain", action="store_true", help="skip the plain Float64 comparison pass")
-    ap.add_argument("--write-counts", default=None,
-                    help="write the plain pass's Picard/CG iteration counts of the timed window here")
     ap.add_argument("--precond", default="jacobi", choices=["jacobi", "chebyshev"])
     ap.add_argument("--workload", default="seasonal4096")
     ap.add_argument("--dt", type=float, default=1800.0)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cpu-sample-s", type=float, default=20.0)
+    ap.add_argument("--cpu-sample-s", type=float, default=25.0,
+                    help="cpu_baseline: wall seconds of the CPU restatement's run loop to time")
+    ap.add_argument("--ref-slice-s", type=float, default=5.0,
+                    help="reference arm: wall seconds of the CPU run loop per bench step")
+    ap.add_argument("--ref-precond", default="chebyshev", choices=["jacobi", "chebyshev"],
+                    help="CPU legs: the CPU restatement's preconditioner (Chebyshev(4): the CPU plan)")
+    ap.add_argument("--plain-steps", type=int, default=2,
+                    help="plain Float64 GPU comparison: timed steps from the chosen form's post-warm-up state")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--out", default=None, help="also write the JSON line here")
     ap.add_argument("--ensemble", type=int, default=0,
@@ -347,12 +354,20 @@ def roofline_for(shk, sim, form, w, peaks):
     return r
 
 
-def timed_pass(shk, w, args, form, pg, clocks=None):
-    """W warm-up steps, then K timed steps of `form` (device-resident); returns the record."""
+def timed_pass(shk, w, args, form, pg, clocks=None, steps=None, state=None, keep_snapshot=False):
+    """W warm-up steps, then K timed steps of `form` (device-resident), with a CUDA event after
+    every step; returns the record.  state: a snapshot (field -> tensor, plus 'total_time') to
+    start from instead of the workload's initial state; then no warm-up steps run.
+    keep_snapshot: also return the state after the warm-up (before the timed steps)."""
     import torch
+    steps = args.steps if steps is None else steps
     sim = make_sim(shk, w, args, form=form)
     warm = []
-    run_steps(shk, sim, args.warmup, warm)
+    if state is not None:
+        load_snapshot(sim, state)
+    else:
+        run_steps(shk, sim, args.warmup, warm)
+    snap = snapshot(sim) if keep_snapshot else None
     torch.cuda.synchronize()
     ctx = sim.ctx()
     launches0 = ctx.launches()
@@ -360,22 +375,52 @@ def timed_pass(shk, w, args, form, pg, clocks=None):
     torch.cuda.synchronize()
     if clocks:
         clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
     rec = []
-    e0.record()
-    run_steps(shk, sim, args.steps, rec)
-    e1.record()
+    evs[0].record()
+    for k in range(steps):
+        run_steps(shk, sim, 1, rec)
+        evs[k + 1].record()
     torch.cuda.synchronize()
     barrier(pg)
     clk = clocks.stop() if clocks else None
-    ms = e0.elapsed_time(e1)
-    return dict(sim=sim, rec=rec, warm=warm, ms=ms, ms_max=max_over_ranks(pg, ms),
-                launches=ctx.launches() - launches0, clocks=clk, h_after=sim.state.h.clone())
+    ms = evs[0].elapsed_time(evs[-1])
+    step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
+    for r, m in zip(rec, step_ms):
+        r["ms"] = round(m, 3)
+    return dict(sim=sim, rec=rec, warm=warm, ms=ms, ms_max=max_over_ranks(pg, ms), step_ms=step_ms,
+                launches=ctx.launches() - launches0, clocks=clk, h_after=sim.state.h.clone(), snap=snap)
+
+
+def snapshot(sim) -> dict:
+    """Device copies of every State field and the simulation clock."""
+    from shakti_b200 import _lib
+    snap = {f: getattr(sim.state, f).clone() for f in _lib.STATE_FIELDS}
+    snap["total_time"] = sim.total_time
+    return snap
+
+
+def load_snapshot(sim, snap: dict) -> None:
+    for f, t in snap.items():
+        if f != "total_time":
+            getattr(sim.state, f).copy_(t)
+    sim.total_time = snap["total_time"]
 
 
 def counts_of(rec):
     return {"steps": len(rec), "picard_iters": sum(r["picard"] for r in rec), "cg_iters": sum(r["cg"] for r in rec),
             "all_converged": all(r["converged"] for r in rec)}
+
+
+def bench_config(w, args, world) -> dict:
+    """The workload both arms time (the same dict in both JSON lines)."""
+    return {"workload": f"{w.name}: {w.nx}x{w.ny} cells, {w.lx / 1e3:g} km, seasonal melt + 64 moulins, "
+                        f"10% LAND/OTHER_BASIN blobs",
+            "stop": "relres 1e-8: ||b - A h||_2 (every row) <= 1e-8 ||b||_2 over the GROUNDED rows (Float64)",
+            "picard": "500 iters, tol 1e-6", "dt_s": args.dt, "sliding": f"RegularizedCoulomb C={w.sliding_C}",
+            "params": w.params, "gap": "implicit", "kface": "arithmetic",
+            "l2": "inputs larger than L2 (about 8 GB resident per GPU)",
+            "parallelism": f"replicas x{world} (independent instances, no data-path collective)"}
 
 
 def ours(args, world, rank, local, pg):
@@ -389,31 +434,40 @@ def ours(args, world, rank, local, pg):
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
 
     # ---- device-resident pass of the chosen form ---------------------------------------------
-    main = timed_pass(shk, w, args, args.form, pg, ClockSampler(torch.cuda.current_device()))
+    want_plain = not args.no_plain and args.form != "plain" and args.plain_steps > 0
+    main = timed_pass(shk, w, args, args.form, pg, ClockSampler(torch.cuda.current_device()),
+                      keep_snapshot=want_plain)
+    snap = main.pop("snap")
     value, _ = replica_value(pg, world, args.steps, main["ms"])
     roofline = roofline_for(shk, main["sim"], args.form, w, peaks)
     state_after = main.pop("h_after")
     del main["sim"]
     torch.cuda.empty_cache()
 
-    # ---- plain Float64 Jacobi CG on the GPU, same window -------------------------------------
+    # ---- plain Float64 Jacobi CG on the GPU over the window's first steps --------------------
+    # The plain form needs ~100x the chosen form's time per step, so it times the first
+    # --plain-steps steps of the window: it starts from the chosen form's state after the warm-up
+    # (the same timestep) and is compared with the chosen form's own time for those steps.
     plain = None
-    plain_rec = None
-    if not args.no_plain and args.form != "plain":
-        pp = timed_pass(shk, w, args, "plain", pg)
-        plain_rec = pp["rec"]
-        pv = world * args.steps / (pp["ms_max"] / 1e3)
-        plain = {"value": round(pv, 4), "unit": UNIT, "ms_per_step": round(pp["ms_max"] / args.steps, 3),
-                 "chosen_over_plain": round(value / pv, 3), "gpu_launches": int(sum_over_ranks(pg, pp["launches"])),
-                 "roofline": roofline_for(shk, pp["sim"], "plain", w, peaks), "timed_steps": counts_of(plain_rec)}
+    if want_plain:
+        ps = min(args.plain_steps, args.steps)
+        probe = make_sim(shk, w, args, form="plain")
+        load_snapshot(probe, snap)
+        plain_roof = roofline_for(shk, probe, "plain", w, peaks)  # also warms the plain form's graphs
+        del probe
+        pp = timed_pass(shk, w, args, "plain", pg, steps=ps, state=snap)
+        del snap
+        pv = world * ps / (pp["ms_max"] / 1e3)
+        chosen_ms = max_over_ranks(pg, sum(main["step_ms"][:ps]))
+        plain = {"value": round(pv, 4), "unit": UNIT, "steps": ps, "ms_per_step": round(pp["ms_max"] / ps, 3),
+                 "chosen_ms_per_step_same_steps": round(chosen_ms / ps, 3),
+                 "chosen_over_plain": round(pp["ms_max"] / chosen_ms, 3),
+                 "window": f"timesteps {args.warmup + 1}..{args.warmup + ps} (the first {ps} of the timed window), "
+                           f"from the chosen form's state after the warm-up",
+                 "gpu_launches": int(sum_over_ranks(pg, pp["launches"])), "roofline": plain_roof,
+                 "timed_steps": dict(counts_of(pp["rec"]), per_step=pp["rec"])}
         del pp
         torch.cuda.empty_cache()
-    elif args.form == "plain":
-        plain_rec = main["rec"]
-    if args.write_counts and rank == 0 and plain_rec is not None:
-        Path(args.write_counts).write_text(json.dumps(
-            dict(counts_of(plain_rec), workload=w.name, warmup=args.warmup, form="plain Float64 Jacobi CG, relres 1e-8",
-                 per_step=plain_rec), indent=1) + "\n")
 
     # ---- end-to-end pass through the public API with host buffers ---------------------------
     e2e = None
@@ -454,18 +508,10 @@ def ours(args, world, rank, local, pg):
         del sim
         torch.cuda.empty_cache()
 
-    # ---- CPU baseline (rank 0, N = 1 only): the reference algorithm's iteration counts --------
+    # ---- CPU baseline (rank 0, N = 1 only): the CPU restatement's real run loop, bounded -----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        counts_src = "this run's plain Float64 pass"
-        rec = plain_rec
-        if rec is None:
-            cf = ROOT / "profiles" / f"step_counts_{w.name}.json"
-            if cf.exists():
-                rec, counts_src = json.loads(cf.read_text())["per_step"], cf.name
-            else:
-                rec, counts_src = main["rec"], "the chosen form's own counts (plain counts unavailable)"
-        cpu = cpu_baseline(shk, w, args, rec, counts_src)
+        cpu = cpu_baseline(shk, w, args)
 
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -473,13 +519,8 @@ def ours(args, world, rank, local, pg):
         "scaling": "weak", "vs_baseline": None,
         "dtype": {"plain": "f64", "fp32cg": "f32+f64", "multigrid": "f64+f32"}[args.form],
         "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": f"{w.name}: {w.nx}x{w.ny} cells, {w.lx / 1e3:g} km, seasonal melt + 64 moulins, "
-                               f"10% LAND/OTHER_BASIN blobs",
-                   "form": FORMS[args.form], "stop": "relres 1e-8 (||b-Ah||/||b||, Float64)",
-                   "picard": "500 iters, tol 1e-6", "dt_s": args.dt, "sliding": f"RegularizedCoulomb C={w.sliding_C}",
-                   "params": w.params, "gap": "implicit", "kface": "arithmetic",
-                   "l2": "inputs larger than L2 (about 8 GB resident per GPU)",
-                   "parallelism": f"replicas x{world} (independent instances, no data-path collective)"},
+        "config": bench_config(w, args, world),
+        "form": FORMS[args.form],
         "roofline": roofline,
         "step_roofline": step_roofline(args.form, w, counts_of(main["rec"]), main["ms_max"] / args.steps, peaks),
         "plain_fp64_gpu": plain,
@@ -492,28 +533,53 @@ def ours(args, world, rank, local, pg):
     return line
 
 
-def cpu_baseline(shk, w, args, rec, counts_src):
-    """The CPU restatement of the reference algorithm on the host cores, on a bounded sample of
-    the same workload: the 4096^2 initial state, timing one assembly, one field-update tail, one
-    gap step and a run of Jacobi CG iterations; the timestep rate is these costs combined with the
-    timed window's Picard and CG iteration counts (identical for the reference algorithm: the
-    parity tests match iteration counts to +-1 per solve)."""
+def cpu_rate(pr: dict) -> tuple[float, str]:
+    """Timesteps/s of a bounded CPU run: measured over its completed timesteps, or, when it has not
+    completed one, the upper bound 1/(seconds spent on the first timestep so far)."""
+    if pr["steps_done"] >= 1:
+        return pr["steps_done"] / pr["completed_s"], "measured"
+    return 1.0 / pr["elapsed"], "upper bound"
+
+
+def cpu_session(orc, w, args, precond: str):
+    st, osl = oracle_state(orc, w)
+    spec = orc.CgSpec(precond=1 if precond == "chebyshev" else 0, cheb_degree=4, cheb_nsteps=15, stop_rule=1,
+                      rtol=1e-8, atol=0.0)
+    melt = orc.seasonal_melt(w.melt) if w.melt else None
+    return orc.RunSession(st, w.params, osl, args.dt, kfs=0, gap_scheme=1, cgspec=spec, melt=melt,
+                          picard_iters=500, picard_tol=1e-6)
+
+
+def cpu_sample_text(w, pr, threads, precond, bound, label):
+    prog = (f"{pr['steps_done']} timesteps completed" if pr["steps_done"] else
+            f"timestep 1 not completed: Picard iteration {pr['pic_iter_now']} in progress")
+    return (f"{label}: the CPU restatement's real run loop (update_ieb!, Picard_loop! with CG "
+            f"{'Chebyshev(4)' if precond == 'chebyshev' else 'Jacobi'} to the same relres 1e-8, step_b!; C, OpenMP "
+            f"{threads} threads) on the {w.nx}^2 workload from its initial state for {pr['elapsed']:.1f} s of wall "
+            f"time: {prog}, {pr['picard_iters']} linear solves and {pr['cg_iters']} CG iterations done; value = "
+            + ("completed timesteps / their time" if bound == "measured" else
+               "1 / elapsed, an upper bound on the CPU's timesteps/s (no timestep finished)"))
+
+
+def cpu_progress(pr: dict) -> dict:
+    return {k: pr[k] for k in ("steps_done", "picard_iters", "cg_iters", "pic_iter_now", "cg_iter_now", "elapsed",
+                               "completed_s")}
+
+
+def cpu_baseline(shk, w, args):
+    """The CPU restatement of the reference algorithm on the host cores, on a bounded sample of the
+    same workload: its real run loop from the workload's initial state for --cpu-sample-s seconds."""
     orc = entry.load_oracle()
     orc.build()
     threads = os.cpu_count() or 1
     orc.set_num_threads(threads)
-    costs = oracle_costs(orc, w, args.cpu_sample_s)
-    steps = len(rec)
-    pic = sum(r["picard"] for r in rec)
-    cg = sum(r["cg"] for r in rec)
-    sec = pic * (costs["assemble_s"] + costs["tail_s"]) + cg * costs["cg_iter_s"] + steps * costs["gap_s"]
-    return {"value": round(steps / sec, 6), "unit": UNIT, "cores": orc.num_threads(), "kind": "port",
-            "sample": (f"CPU restatement (C, OpenMP {orc.num_threads()} threads) on the {w.nx}^2 initial state: "
-                       f"1 assembly ({costs['assemble_s']:.3f} s), 1 tail ({costs['tail_s']:.3f} s), 1 gap step "
-                       f"({costs['gap_s']:.3f} s), {costs['cg_iters']} Jacobi CG iterations "
-                       f"({costs['cg_iter_s'] * 1e3:.1f} ms each); rate = these costs x the timed window's "
-                       f"{pic} Picard and {cg} CG iterations over {steps} steps ({counts_src})"),
-            "costs": costs}
+    S = cpu_session(orc, w, args, args.ref_precond)
+    pr = S.advance(args.cpu_sample_s)
+    S.close()
+    v, bound = cpu_rate(pr)
+    return {"value": round(v, 6), "unit": UNIT, "cores": orc.num_threads(), "kind": "port", "bound": bound,
+            "sample": cpu_sample_text(w, pr, orc.num_threads(), args.ref_precond, bound, "bounded sample"),
+            "progress": cpu_progress(pr)}
 
 
 def oracle_state(orc, w):
@@ -523,76 +589,49 @@ def oracle_state(orc, w):
     return st, osl
 
 
-def oracle_costs(orc, w, budget_s, prepared=None):
-    st, osl = prepared or oracle_state(orc, w)
-    t0 = time.perf_counter()
-    A = orc.assemble(st, w.params)
-    t_asm = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    orc.picard_tail(st, w.params, osl)
-    t_tail = time.perf_counter() - t0
-    b_saved = st["b"].copy(), st["beta"].copy(), st["b_x"].copy(), st["b_y"].copy()
-    t0 = time.perf_counter()
-    orc.step_b(st, w.params, 1, 1800.0)
-    t_gap = time.perf_counter() - t0
-    for arr, v in zip((st["b"], st["beta"], st["b_x"], st["b_y"]), b_saved):
-        arr[...] = v
-    n = 4
-    t0 = time.perf_counter()
-    orc.cg(A, st["h"], orc.CgSpec(precond=0, stop_rule=1, rtol=0.0, atol=0.0, itmax=n))
-    t_first = time.perf_counter() - t0
-    per = t_first / n
-    n2 = max(4, min(200, int(max(budget_s - t_first, 1.0) / max(per, 1e-6))))
-    t0 = time.perf_counter()
-    _, s2 = orc.cg(A, st["h"], orc.CgSpec(precond=0, stop_rule=1, rtol=0.0, atol=0.0, itmax=n2))
-    t_cg = time.perf_counter() - t0
-    # one CG call = one initial residual matvec + n2 iterations; subtract the setup share
-    t_setup = max(t_first - n * (t_cg / n2), 0.0)
-    cg_iter = max((t_cg - t_setup) / max(s2["niter"], 1), 1e-9)
-    return {"assemble_s": t_asm, "tail_s": t_tail, "gap_s": t_gap, "cg_iter_s": cg_iter, "cg_iters": int(s2["niter"])}
-
-
 # ---------------------------------------------------------------------------------------------
 # reference arm: the CPU restatement of the reference algorithm on the host cores
 # ---------------------------------------------------------------------------------------------
 def reference(args, world, rank, local, pg):
+    """The reference algorithm's CPU implementation (the C restatement; Julia is absent) on all host
+    cores: its real run loop on the same workload from the initial state, W + K bench steps of
+    --ref-slice-s seconds each (the loop continues across steps; nothing is re-timed or modeled).
+    A 4096^2 timestep of the CPU run takes longer than the whole benchmark, so the value is the
+    measured rate if any timestep completes and otherwise the upper bound 1/(time spent on the
+    first timestep)."""
     if rank != 0:
         return None
     shk = entry.load_package()
     orc = entry.load_oracle()
     orc.build()
     w = shk.configs.WORKLOADS[args.workload]()
-    counts_file = ROOT / "profiles" / f"step_counts_{w.name}.json"
-    counts = json.loads(counts_file.read_text()) if counts_file.exists() else None
     threads = os.cpu_count() or 1
     orc.set_num_threads(threads)
-    per_step = []
-    prepared = oracle_state(orc, w)
-    for k in range(args.warmup + args.steps):
-        c = oracle_costs(orc, w, max(args.cpu_sample_s / 4, 2.0), prepared)
-        if k >= args.warmup:
-            per_step.append(c)
-    mean = {k: statistics.mean(c[k] for c in per_step) for k in ("assemble_s", "tail_s", "gap_s", "cg_iter_s")}
-    if counts:
-        pic, cg, steps = counts["picard_iters"], counts["cg_iters"], counts["steps"]
-    else:
-        pic, cg, steps = 1, 0, 1
-    sec = pic * (mean["assemble_s"] + mean["tail_s"]) + cg * mean["cg_iter_s"] + steps * mean["gap_s"]
-    value = steps / sec
-    sample = (f"CPU restatement of the reference algorithm (C, OpenMP {orc.num_threads()} threads; Julia is absent) "
-              f"on the {w.nx}^2 workload: each step times 1 assembly, 1 tail, 1 gap step and a run of Jacobi CG "
-              f"iterations on the initial state; timesteps/s = these costs x the per-step Picard/CG iteration counts "
-              f"of the same workload's timed window ({pic} Picard, {cg} CG over {steps} steps"
-              f"{', from ' + counts_file.name if counts else ', counts unavailable: 1 Picard iteration per step'})")
+    S = cpu_session(orc, w, args, args.ref_precond)
+    for _ in range(args.warmup):
+        S.advance(args.ref_slice_s)
+    slices = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        pr = S.advance(args.ref_slice_s)
+        slices.append(time.perf_counter() - t0)
+    S.close()
+    value, bound = cpu_rate(pr)
+    ms_step = 1e3 * sum(slices) / max(len(slices), 1)
+    sample = cpu_sample_text(w, pr, orc.num_threads(), args.ref_precond, bound,
+                             f"{args.warmup} + {args.steps} bench steps of {args.ref_slice_s:g} s each")
+    cpu = {"value": round(value, 6), "unit": UNIT, "cores": orc.num_threads(), "kind": "port", "bound": bound,
+           "sample": sample}
     return {"metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(1e3 / value, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": f"{w.name}: {w.nx}x{w.ny} cells", "form": "reference Threads/Float64 CG (Jacobi)"},
-            "impl": "reference",
-            "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": orc.num_threads(), "kind": "port",
-                             "sample": sample},
+            "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no dataset)",
+            "config": bench_config(w, args, world),
+            "form": f"CPU restatement of the reference algorithm (Threads/Float64 CG, "
+                    f"{'Chebyshev(4)' if args.ref_precond == 'chebyshev' else 'Jacobi'})",
+            "impl": "reference", "cpu_baseline": cpu,
             "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "costs": mean}
+            "progress": cpu_progress(pr),
+            "step_note": "each bench step is one slice of the continuing CPU run loop; ms_per_step is the slice"}
 
 
 def profile_cg(args):
