@@ -358,8 +358,10 @@ SHK_API int shk_set_cg_warm_start(void *ctx, const double *x0);
  * message on stderr.  The first call on each device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current: make that first call before any stream
  * capture.  All calls share the array and it keeps the last call's contents, so calls that overlap
- * on the GPU (different streams or host threads) race: serialise them.  Returns the solve's
- * status (SHK_OK, SHK_NOT_CONVERGED, SHK_BREAKDOWN) or an error code. */
+ * on the GPU (different streams or host threads) race: serialise them.  The call waits on
+ * `stream` between batches of iterations (it reads the stopping flag back to the host), so it
+ * returns with the solve complete.  Returns the solve's status (SHK_OK, SHK_NOT_CONVERGED,
+ * SHK_BREAKDOWN) or an error code; *st is filled in either case. */
 SHK_API int shk_cg_solve_static(int nx, int ny, const double *aP, const double *aE, const double *aN,
                                 const double *rhs, double *x, const shk_cg_opts *o, shk_cg_stats *st,
                                 void *stream);

@@ -151,15 +151,15 @@ def seasonal(nx: int, lx: float, seed: int = 20262, n_moulins: int = 64, blob_fr
     return w
 
 
-# The 4096^2 mixed-precision workload uses two settings that keep every timestep well-posed on
-# the reference algorithm itself (demonstrated with the CPU restatement):
-#  - C = 0.25, the reference fixture's regularized-Coulomb coefficient.  With C = 1e4 the
-#    regularized-Coulomb stress reaches ~1e10 Pa, shear heating ~1e4 W/m^2, b grows ~5 cm per
-#    30-minute step, Re ~ 6e5, and Picard stops converging by the third step.
+# The 4096^2 mixed-precision workload uses two settings that differ from its written description:
+#  - C = 0.25, the reference fixture's regularized-Coulomb coefficient.  With C = 1e4 the reference
+#    algorithm's own Picard loop (the CPU restatement, Jacobi CG to rel-res 1e-8 on the GROUNDED
+#    rows) exhausts its 500 iterations from the second timestep on at 256^2; with C = 0.25 every
+#    step converges (tests/test_workload_settings.py).
 #  - b_min = 0.002 m, b_max = 1 m: the cap the reference's ModelParameters docstring recommends for
-#    the b -> K -> q -> mdot runaway where N approaches or drops below zero; without it the 1-20
-#    m^3/s single-cell moulins drive N to about -3e7 Pa, the implicit gap denominator turns
-#    negative and b runs away within two steps.
+#    the b -> K -> q -> mdot feedback where N falls below zero.  Without it, at 1024^2 (the same
+#    cell size as 4096^2) the single-cell 1-20 m^3/s moulins double the largest gap within three
+#    steps (0.056 -> 0.110 m) while N falls to -8.9e6 Pa; Picard still converges over those steps.
 SEASONAL_PARAMS = dict(b_min=0.002, b_max=1.0)
 SEASONAL_C = 0.25
 

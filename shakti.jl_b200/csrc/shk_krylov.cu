@@ -1472,7 +1472,18 @@ extern "C" SHK_API int shk_cg_solve_static(int nx, int ny, const double *aP, con
         if (cudaMemcpyAsync(&h, cg, sizeof(CgDev), cudaMemcpyDeviceToHost, s) != cudaSuccess) return SHK_CUDA_ERROR;
         if (cudaStreamSynchronize(s) != cudaSuccess) return SHK_CUDA_ERROR;
         if (h.done) break;
-        if (h.iter > h.itmax + 4 || enq > h.itmax + 2LL * 256 + 8) return SHK_CUDA_ERROR;
+        if (h.iter > h.itmax + 4 || enq > h.itmax + 2LL * 256 + 8) {
+            // The device loop ran past every bound it can reach: report what it reached.
+            if (st) {
+                memset(st, 0, sizeof(*st));
+                st->niter = (long)h.iter;
+                st->status = SHK_CUDA_ERROR;
+                st->rnorm0 = h.rnorm0;
+                st->rnorm = h.rnorm;
+                st->lambda_min = st->lambda_max = 1.0;
+            }
+            return SHK_CUDA_ERROR;
+        }
         for (int k = 0; k < batch; k++, enq++) {
             double *p_old = p[enq & 1], *p_new = p[(enq + 1) & 1];
             k_cg_A<double, true><<<march_blocks, kMarchX, 0, s>>>(nx, ny, march_th, aP, aE, aN, r, nullptr, p_old,
