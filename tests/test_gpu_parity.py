@@ -173,28 +173,30 @@ def test_chebyshev_zero_rhs_keeps_placeholder(shk, orc, cuda):
 
 
 def run_pair(shk, orc, cuda, w, tsteps, dt, *, precond=1, kfs="arithmetic", gap="implicit", p=None, rtol=None,
-             atol=None, melt=None, sliding=None):
+             atol=None, melt=None, sliding=None, alpha=None, check_every=1, stop_rule="krylov"):
     g, pm, sl, osl, s, st = setup_pair(shk, orc, cuda, w, sliding=sliding, p=p)
     kw = {}
     if rtol is not None:
         kw.update(rtol=rtol, atol=atol)
-    ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, chebyshev_degree=4 if precond else None, **kw)
+    ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, chebyshev_degree=4 if precond else None,
+                               stop_rule=stop_rule, **kw)
     mi, omelt = shk.ConstantMeltInput(), None
     if melt is not None:
         mi = shk.SeasonalMeltInput(**melt)
         omelt = dict(kind=1, t_start=mi.t_start, period=mi.period, omega=mi.omega, amplitude=mi.amplitude,
                      offset=mi.offset, i_min=mi.i_min, seconds_per_year=mi.seconds_per_year)
     if pm.e_v == 0:
-        ps = shk.PicardSolver(500, 1e-6, ls, g)
+        ps = shk.PicardSolver(500, 1e-6, ls, g, alpha=alpha, check_every=check_every)
         sim = shk.Simulation(g, s, tsteps, dt, pm, gap, [], mi, sl, ps=ps, k_face_choice=kfs)
     else:
         sim = shk.Simulation(g, s, tsteps, dt, pm, gap, [], mi, sl, ls=ls, k_face_choice=kfs)
     shk.run(sim)
-    cg = orc.CgSpec(precond=precond, cheb_degree=4)
+    cg = orc.CgSpec(precond=precond, cheb_degree=4, stop_rule=0 if stop_rule == "krylov" else 1)
     if rtol is not None:
         cg.rtol, cg.atol = rtol, atol
     rc, tt, stats = orc.run(st, p, osl, tsteps, dt, kfs=1 if kfs == "harmonic" else 0,
-                            gap_scheme=1 if gap == "implicit" else 0, cgspec=cg, melt=omelt)
+                            gap_scheme=1 if gap == "implicit" else 0, cgspec=cg, melt=omelt,
+                            alpha=float("nan") if alpha is None else alpha, check_every=check_every)
     return sim, s, st, stats
 
 
@@ -232,6 +234,19 @@ def test_run_plain64_default_tolerances(shk, orc, cuda):
 def test_run_schemes(shk, orc, cuda, kfs, gap, precond):
     sim, s, st, stats = run_pair(shk, orc, cuda, shk.configs.plain64(), 3, 1800.0, precond=precond, kfs=kfs, gap=gap,
                                  rtol=1e-13, atol=0.0)
+    assert_fields_close(s, st)
+
+
+@pytest.mark.parametrize("alpha,check_every", [(0.5, 1), (0.7, 3)])
+def test_run_head_relaxation(shk, orc, cuda, alpha, check_every):
+    """PicardSolver(500, 1e-6, ls, g; alpha, check_every): relax_h! blends each Picard iterate with
+    the previous head, h = alpha h + (1 - alpha) h_prev (src/elliptic_solver.jl:33-46), and the
+    convergence test runs every check_every iterations (:162-172).  Same Picard counts step by step
+    as the oracle, fields within 1e-10."""
+    sim, s, st, stats = run_pair(shk, orc, cuda, shk.configs.plain64(), 4, 3600.0, rtol=1e-12, atol=0.0,
+                                 alpha=alpha, check_every=check_every, stop_rule="relres")
+    for a, b in zip(sim.step_stats, stats):
+        assert a["last_iter"] == b["last_iter"] and a["converged"] == b["converged"]
     assert_fields_close(s, st)
 
 
