@@ -221,7 +221,8 @@ SHK_API int shk_create(int nx, int ny, double lx, double ly, void *stream, void 
     }
     c->max_blocks = c->grid_stencil > c->march_blocks ? c->grid_stencil : c->march_blocks;
     if (c->max_blocks < c->num_sms * 8) c->max_blocks = c->num_sms * 8;
-    rc = ctx_alloc(c);
+    rc = mg_set_first_wait_polls();
+    if (!rc) rc = ctx_alloc(c);
     if (rc) {
         if (c->arena) cudaFree(c->arena);
         if (c->host_dev) cudaFreeHost(c->host_dev);

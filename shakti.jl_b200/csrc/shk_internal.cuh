@@ -219,6 +219,7 @@ int check_launch(Ctx *c, const char *what);
 
 // shk_fields.cu
 int build_mask8(Ctx *c);
+int mg_set_first_wait_polls();
 int launch_initial_conditions(Ctx *c);
 int launch_assemble(Ctx *c, int parabolic, double dt, bool copy_h_prev);
 int launch_export_mfls(Ctx *c, double *aP, double *aE, double *aW, double *aN, double *aS, double *rhs);

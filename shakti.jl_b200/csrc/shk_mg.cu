@@ -17,6 +17,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <float.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -549,8 +550,13 @@ __device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, uint
 }
 
 // Bounded wait for the stage's phase `parity`; false when the polls ran out.
-__device__ __forceinline__ bool tma_wait(uint64_t *bar, uint32_t parity) {
-    for (long i = 0; i < kTmaSpin; i++) {
+// Polls allowed to the first tile wait of every TMA-staged launch: kTmaSpin, except in the test
+// of the give-up path, which sets 0 (SHK_TEST_TMA_FIRST_WAIT, read at context creation) so that
+// the first wait gives up at once while its copies still arrive and are drained.
+__device__ long g_tma_first_spin = kTmaSpin;
+
+__device__ __forceinline__ bool tma_wait(uint64_t *bar, uint32_t parity, long spin = kTmaSpin) {
+    for (long i = 0; i < spin; i++) {
         uint32_t ok;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
@@ -679,11 +685,15 @@ __device__ __forceinline__ void pair_sweep(const Pair &P, const float *XI, float
     st2(XO + P.k, __ffma2_rn(P.W, sub2(P.B, pair_ax(P, XI)), ld2(XI + P.k)));
 }
 
-// Records a failed wait (the solve stops and reports it) after waiting, bounded, for the copies
-// still in flight into the other stage.
-__device__ __forceinline__ void tma_give_up(CgDev *cg, uint64_t *other, uint32_t parity, bool pending) {
+// Records a failed wait (the solve stops and reports it).  Before the block returns, thread 0
+// waits, with the normal bound, for every copy the block issued: the stage whose wait ran out
+// (its copies may still be on their way) and, when pending, the other stage.  A block exits only
+// after its staged copies have landed, so no copy writes shared memory a later block owns.
+__device__ __forceinline__ void tma_give_up(CgDev *cg, uint64_t *cur, uint32_t cur_parity, bool cur_issued,
+                                            uint64_t *other, uint32_t other_parity, bool other_pending) {
     if (threadIdx.x == 0) {
-        if (pending) tma_wait(other, parity);
+        if (cur_issued) tma_wait(cur, cur_parity);
+        if (other_pending) tma_wait(other, other_parity);
         cg->fault = 1;
         atomicExch(&cg->done, 1);
     }
@@ -697,7 +707,7 @@ __device__ __forceinline__ void tma_tiles(int nx, int ny, unsigned char *sm, CgD
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Y::o_bar);
     const int tiles_x = (nx + kFW - 1) / kFW, ntiles = tiles_x * ((ny + kFH - 1) / kFH);
     if (su32(sm) & 127u) {  // the boxes' 128-byte alignment is not met: no copy is issued
-        tma_give_up(cg, &bar[0], 0, false);
+        tma_give_up(cg, nullptr, 0, false, nullptr, 0, false);
         return;
     }
     if (threadIdx.x == 0) {
@@ -718,9 +728,9 @@ __device__ __forceinline__ void tma_tiles(int nx, int ny, unsigned char *sm, CgD
         }
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
         pre(x0, y0);
-        const bool ok = tma_wait(&bar[s], (it >> 1) & 1);
+        const bool ok = tma_wait(&bar[s], (it >> 1) & 1, it == 0 ? g_tma_first_spin : kTmaSpin);
         if (__syncthreads_or(!ok)) {
-            tma_give_up(cg, &bar[s ^ 1], ((it + 1) >> 1) & 1, tn < ntiles);
+            tma_give_up(cg, &bar[s], (it >> 1) & 1, true, &bar[s ^ 1], ((it + 1) >> 1) & 1, tn < ntiles);
             return;
         }
         body(sm + s * Y::stage, x0, y0);
@@ -1800,6 +1810,14 @@ int mg_levels_for(int nx, int ny, int *dims, int maxl) {
         b = (b + 1) / 2;
     }
     return l;
+}
+
+// The first-wait poll count of the TMA-staged kernels on the current device: kTmaSpin, or the
+// value of SHK_TEST_TMA_FIRST_WAIT (the give-up path's test).  Called at context creation.
+int mg_set_first_wait_polls() {
+    long v = kTmaSpin;
+    if (const char *e = getenv("SHK_TEST_TMA_FIRST_WAIT")) v = std::max(0L, atol(e));
+    return cudaMemcpyToSymbol(g_tma_first_spin, &v, sizeof(v)) == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
 }
 
 } // namespace shk

@@ -11,6 +11,7 @@ import numpy as np
 from . import _lib
 from .model import (Arithmetic, Harmonic, ModelParameters, PrescribedSlidingLaw, State, Grid, AbstractMeltInput,
                     AbstractSlidingLaw)
+from .observers import FILE_WRITERS, IOObserver
 from .solvers import (_Context, AbstractLinearSolver, CGIterativeSolver, PicardSolver, solve_parabolic_linear_system)
 
 
@@ -68,8 +69,8 @@ class NoOpenBySliding(AbstractOpenBySlidingScheme):
 
 
 # ---------------------------------------------------------------------------------------------
-# Observers (src/observer.jl): NoObserver and the in-memory LiveObserver.  File writers (NetCDF,
-# HDF5, JLD2, CSV) are host I/O outside the solve path and are not provided.
+# Observers (src/observer.jl): NoObserver and the in-memory LiveObserver here; IOObserver and its
+# file writers in observers.py.
 # ---------------------------------------------------------------------------------------------
 class AbstractObserver:
     def prepare(self, state):
@@ -144,8 +145,17 @@ class Simulation:
         elif which_observer is None:
             raise ValueError('which_observer should be specified as "IO" or "Live" when tracked_obs is not empty.')
         elif which_observer == "IO":
-            raise NotImplementedError("IOObserver (NetCDF/HDF5/JLD2/CSV file writers) is host I/O outside the "
-                                      "solve path and is not provided by this library; use \"Live\".")
+            if which_file_writer is None:
+                raise ValueError('which_file_writer should be specified as "NetCDF", "HDF5", "JLD2", or "CSV" when '
+                                 'which_observer is "IO".')
+            if which_file_writer not in FILE_WRITERS:
+                raise ValueError(f'Unknown which_file_writer: "{which_file_writer}" (expected "NetCDF", "HDF5", '
+                                 f'"JLD2", or "CSV")')
+            if tracked_times is None:
+                raise ValueError('tracked_times should be specified when which_observer is "IO".')
+            if path is None:
+                raise ValueError('path should be specified when which_observer is "IO".')
+            self.observer = IOObserver(tracked_obs, tracked_times, FILE_WRITERS[which_file_writer](), path)
         elif which_observer == "Live":
             if tracked_times is None:
                 raise ValueError('tracked_times should be specified when which_observer is "Live".')

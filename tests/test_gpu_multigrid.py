@@ -140,3 +140,24 @@ def test_tma_multigrid_run_matches_oracle(shk, orc, cuda, monkeypatch):
     host = s.to_numpy(["h", "N", "b"])
     for f in ("h", "N", "b"):
         assert relerr(host[f], st[f]) <= 1e-8, (f, relerr(host[f], st[f]))
+
+
+def test_tma_wait_give_up_reports_and_recovers(shk, cuda, monkeypatch):
+    """The bounded-wait fault path of the TMA-staged kernels, without a fault: a test-only setting
+    (SHK_TEST_TMA_FIRST_WAIT=0, read at context creation) gives every launch's first tile wait zero
+    polls, so it gives up at once while the copies it issued still arrive.  Each block then waits,
+    with the normal bound, for all of its copies before it returns, marks the fault and stops the
+    solve; the host reports SHK_CUDA_ERROR "a tile copy did not complete".  A context created
+    afterwards with the normal setting solves as usual."""
+    w = tma_workload(shk, 512, 360)
+    monkeypatch.setenv("SHK_MG_TMA", "1")
+    monkeypatch.setenv("SHK_TEST_TMA_FIRST_WAIT", "0")
+    with pytest.raises(shk._lib.ShaktiError) as exc:
+        solve(shk, w, {}, monkeypatch)
+    assert exc.value.status == shk._lib.CUDA_ERROR and "tile copy" in str(exc.value)
+    cuda.cuda.synchronize()  # the context is still usable: nothing faulted
+    monkeypatch.delenv("SHK_TEST_TMA_FIRST_WAIT")
+    h, st = solve(shk, w, {}, monkeypatch)
+    assert st.status == 0 and st.niter > 0
+    h_l, st_l = solve(shk, w, {"SHK_MG_TMA": "0"}, monkeypatch)
+    assert abs(st.niter - st_l.niter) <= 1 and relerr(h, h_l) <= 1e-7
