@@ -108,7 +108,14 @@ struct Ens {
     int *b2i[EF_N] = {};
     int nb[EF_N] = {};
     cudaGraphExec_t step_exec = nullptr;
+    int graph_precond = -1;  // the form step_exec was built for
     std::string err;
+    // multigrid form (built at its first run): descriptors, per-depth tables
+    EnsMg *dM = nullptr;
+    int dmax = 0, lmax = 0;
+    size_t bottom_smem = 0;
+    int *b2i_vc[kMgMaxLevels] = {}, nb_vc[kMgMaxLevels] = {};
+    int *b2i_set[kMgMaxLevels + 1] = {}, nb_set[kMgMaxLevels + 1] = {};
 };
 
 static int efail(Ens *e, int status, const std::string &msg) {
@@ -155,6 +162,63 @@ static int ens_layout(Ens *e) {
                     "upload ensemble tables");
         if (rc) return rc;
     }
+    return echeck(e, cudaMemcpy(e->dE, e->hE.data(), e->n * sizeof(EnsInst), cudaMemcpyHostToDevice),
+                  "upload ensemble descriptors");
+}
+
+// The multigrid form's per-depth block tables and per-instance descriptors (each instance's blocks
+// at depth d are the grid its own context launches for level d).
+static int ens_mg_layout(Ens *e) {
+    std::vector<EnsMgPlan> plan(e->n);
+    e->dmax = 0;
+    e->lmax = 0;
+    e->bottom_smem = 0;
+    for (int i = 0; i < e->n; i++) {
+        Ctx *c = e->ctx[i];
+        if (c->mg_levels >= kMgMaxLevels) return efail(e, SHK_BAD_ARG, "multigrid hierarchy too deep for the ensemble");
+        if (ens_mg_plan(c, &plan[i])) return efail(e, SHK_BAD_ARG, c->err);
+        e->dmax = std::max(e->dmax, plan[i].lb);
+        e->lmax = std::max(e->lmax, plan[i].nlev);
+        e->bottom_smem = std::max(e->bottom_smem, plan[i].bottom_smem);
+    }
+    std::vector<std::vector<int>> vc(kMgMaxLevels), set(kMgMaxLevels + 1);
+    std::vector<std::vector<int>> b0vc(e->n, std::vector<int>(kMgMaxLevels, 0)),
+        b0set(e->n, std::vector<int>(kMgMaxLevels + 1, 0));
+    for (int i = 0; i < e->n; i++) {
+        for (int d = 0; d < e->dmax; d++) {
+            b0vc[i][d] = (int)vc[d].size();
+            vc[d].insert(vc[d].end(), plan[i].vc_blocks[d], i);
+        }
+        for (int st = 1; st <= e->lmax; st++) {
+            b0set[i][st] = (int)set[st].size();
+            if (st <= plan[i].nlev) set[st].insert(set[st].end(), plan[i].set_blocks[st], i);
+        }
+    }
+    auto upload = [&](std::vector<int> &t, int **dst, int *nb) -> int {
+        if (*dst) cudaFree(*dst);
+        *dst = nullptr;
+        *nb = (int)t.size();
+        if (t.empty()) return SHK_OK;
+        int rc = echeck(e, cudaMalloc(dst, t.size() * sizeof(int)), "cudaMalloc(ensemble multigrid tables)");
+        if (!rc) rc = echeck(e, cudaMemcpy(*dst, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice),
+                             "upload ensemble multigrid tables");
+        return rc;
+    };
+    for (int d = 0; d < e->dmax; d++)
+        if (int rc = upload(vc[d], &e->b2i_vc[d], &e->nb_vc[d])) return rc;
+    for (int st = 1; st <= e->lmax; st++)
+        if (int rc = upload(set[st], &e->b2i_set[st], &e->nb_set[st])) return rc;
+    if (!e->dM && !(e->dM = ens_mg_alloc(e->n))) return efail(e, SHK_CUDA_ERROR, "cudaMalloc(ensemble multigrid)");
+    for (int i = 0; i < e->n; i++) {
+        int b0v[kMgMaxLevels], b0s[kMgMaxLevels];
+        for (int d = 0; d < kMgMaxLevels; d++) {
+            b0v[d] = b0vc[i][d];
+            b0s[d] = b0set[i][d];
+        }
+        if (ens_mg_upload(e->dM, i, e->ctx[i], b0v, b0s)) return efail(e, SHK_CUDA_ERROR, "upload ensemble multigrid");
+        e->hE[i].mg = ens_mg_at(e->dM, i);
+    }
+    if (ens_mg_kernel_attrs()) return efail(e, SHK_CUDA_ERROR, "ensemble multigrid bottom shared memory");
     return echeck(e, cudaMemcpy(e->dE, e->hE.data(), e->n * sizeof(EnsInst), cudaMemcpyHostToDevice),
                   "upload ensemble descriptors");
 }
@@ -215,11 +279,19 @@ static int ens_build_graph(Ens *e) {
         cudaError_t r2 = cudaStreamEndCapture(e->cap[0], &graph);
         if (r == cudaSuccess) r = r2;
     }
+    const bool mg = e->hC.precond == SHK_PRECOND_MULTIGRID;
     if (r == cudaSuccess) r = cudaStreamBeginCaptureToGraph(e->cap[1], body1, nullptr, nullptr, 0, mode);
     if (r == cudaSuccess) {
         ens_assemble(e->cap[1], E, e->b2i[EF_STENCIL], e->nb[EF_STENCIL]);
+        if (mg) ens_mg_setup(e->cap[1], E, e->dM, e->b2i_set, e->nb_set, e->lmax);
         ens_cg_reset(e->cap[1], E, C, e->n);
-        ens_cg_init(e->cap[1], E, e->b2i[EF_STENCIL], e->nb[EF_STENCIL]);
+        if (mg) {
+            ens_cg_init_mg(e->cap[1], E, e->b2i[EF_STENCIL], e->nb[EF_STENCIL]);
+            ens_mg_vcycle(e->cap[1], E, e->dM, e->b2i_vc, e->nb_vc, e->dmax, nullptr, e->n, e->bottom_smem,
+                          ENS_VC_INIT, 0);
+        } else {
+            ens_cg_init(e->cap[1], E, e->b2i[EF_STENCIL], e->nb[EF_STENCIL]);
+        }
         // nested loop: a default value is applied once per graph launch, not at each start of the
         // loop, so each solve sets its own condition before the loop (any CG still running)
         r = capture_handle(e->cap[1], &h2);
@@ -238,8 +310,14 @@ static int ens_build_graph(Ens *e) {
     if (r == cudaSuccess) r = cudaStreamBeginCaptureToGraph(e->cap[2], body2, nullptr, nullptr, 0, mode);
     if (r == cudaSuccess) {
         for (int par = 0; par < 2; par++) {
-            ens_cg_A(e->cap[2], E, e->b2i[EF_MARCH], e->nb[EF_MARCH], par);
-            ens_cg_B(e->cap[2], E, e->b2i[EF_STREAM], e->nb[EF_STREAM], par);
+            if (mg) {
+                ens_cg_A_mg(e->cap[2], E, e->b2i[EF_MARCH], e->nb[EF_MARCH], par);
+                ens_mg_vcycle(e->cap[2], E, e->dM, e->b2i_vc, e->nb_vc, e->dmax, nullptr, e->n, e->bottom_smem,
+                              ENS_VC_ITER, par);
+            } else {
+                ens_cg_A(e->cap[2], E, e->b2i[EF_MARCH], e->nb[EF_MARCH], par);
+                ens_cg_B(e->cap[2], E, e->b2i[EF_STREAM], e->nb[EF_STREAM], par);
+            }
         }
         ens_cg_cond(e->cap[2], E, C, e->n, h2);
         cudaGraph_t g = nullptr;
@@ -253,6 +331,7 @@ static int ens_build_graph(Ens *e) {
         e->step_exec = nullptr;
         return echeck(e, r, "ensemble timestep graph");
     }
+    e->graph_precond = e->hC.precond;
     return SHK_OK;
 }
 
@@ -260,8 +339,12 @@ static int ens_upload_ctl(Ens *e, double dt, const shk_picard_opts *po, const sh
     if (!po || po->iters < 1) return efail(e, SHK_BAD_ARG, "PicardSolver needs iters >= 1");
     if (po->alpha > 0) return efail(e, SHK_BAD_ARG, "the ensemble runs without head relaxation (alpha)");
     if (!o) return efail(e, SHK_BAD_ARG, "null cg options");
-    if (o->precond != SHK_PRECOND_JACOBI || o->precision != SHK_FP64)
-        return efail(e, SHK_BAD_ARG, "the ensemble runs Float64 Jacobi-preconditioned CG");
+    if ((o->precond != SHK_PRECOND_JACOBI && o->precond != SHK_PRECOND_MULTIGRID) || o->precision != SHK_FP64)
+        return efail(e, SHK_BAD_ARG, "the ensemble runs Float64 CG, Jacobi- or multigrid-preconditioned");
+    if (o->precond == SHK_PRECOND_MULTIGRID && !e->dM) {
+        int rc = ens_mg_layout(e);
+        if (rc) return rc;
+    }
     EnsCtl &C = e->hC;
     C.n = e->n;
     C.picard_iters = po->iters;
@@ -271,6 +354,7 @@ static int ens_upload_ctl(Ens *e, double dt, const shk_picard_opts *po, const sh
     C.rtol = o->rtol;
     C.itmax = o->itmax;
     C.stop_rule = o->stop_rule;
+    C.precond = o->precond;
     C.dt = dt;
     return echeck(e, cudaMemcpyAsync(e->dC, &C, sizeof(EnsCtl), cudaMemcpyHostToDevice, e->stream),
                   "upload ensemble control");
@@ -329,6 +413,8 @@ SHK_API int shk_ensemble_create(int n, void *const *ctxs, void *stream, void **e
         I.mask8 = c->mask8;
         I.aP = c->aP; I.aE = c->aE; I.aN = c->aN; I.rhs = c->rhs; I.x = c->x; I.r = c->r;
         I.p0 = c->p[0]; I.p1 = c->p[1]; I.Ap = c->Ap; I.h_prev = c->h_prev;
+        I.z = c->z; I.r2 = c->r2;
+        I.mg = nullptr;
         I.partials = c->partials;
         I.counter = c->counter;
         I.cg = &c->dev->cg;
@@ -367,6 +453,11 @@ SHK_API int shk_ensemble_destroy(void *ens) {
         if (e->cap[k]) cudaStreamDestroy(e->cap[k]);
     for (int f = 0; f < EF_N; f++)
         if (e->b2i[f]) cudaFree(e->b2i[f]);
+    for (int d = 0; d < kMgMaxLevels; d++)
+        if (e->b2i_vc[d]) cudaFree(e->b2i_vc[d]);
+    for (int d = 0; d <= kMgMaxLevels; d++)
+        if (e->b2i_set[d]) cudaFree(e->b2i_set[d]);
+    ens_mg_free(e->dM);
     if (e->dE) cudaFree(e->dE);
     if (e->dC) cudaFree(e->dC);
     delete e;
@@ -463,6 +554,10 @@ SHK_API int shk_ensemble_run(void *ens, double dt, int tsteps, const shk_picard_
     if (tsteps < 0) return efail(e, SHK_BAD_ARG, "tsteps must be >= 0");
     int rc = ens_upload_ctl(e, dt, po, o);
     if (rc) return rc;
+    if (e->step_exec && e->graph_precond != e->hC.precond) {
+        cudaGraphExecDestroy(e->step_exec);
+        e->step_exec = nullptr;
+    }
     if (!e->step_exec && (rc = ens_build_graph(e))) return rc;
     for (int k = 0; k < tsteps; k++)
         if ((rc = echeck(e, cudaGraphLaunch(e->step_exec, e->stream), "ensemble timestep"))) return rc;

@@ -189,11 +189,13 @@ struct alignas(8) EnsInst {
     shk_state st;
     const uint8_t *mask8;
     double *aP, *aE, *aN, *rhs, *x, *r, *p0, *p1, *Ap, *h_prev;
+    double *z, *r2;  // multigrid form: preconditioned residual, the second residual buffer
     double *partials;
     unsigned int *counter;
     CgDev *cg;
     PicDev *pic;
     double *snap;  // optional copy of h after each timestep's first Picard iteration
+    const struct EnsMg *mg;  // multigrid form: this instance's hierarchy and block ranges (else null)
     // loop control and statistics, written on the device
     int pic_active, pic_iter, pic_converged, cg_breakdowns;
     long long cg_iters, cg_solves;
@@ -204,6 +206,7 @@ struct alignas(8) EnsInst {
 struct alignas(8) EnsCtl {
     int n;                      // instances
     int picard_iters, check_every, stop_rule;
+    int precond;                // SHK_PRECOND_JACOBI or SHK_PRECOND_MULTIGRID
     double picard_tol, atol, rtol;
     long long itmax;            // 0: 2 n cells per instance
     unsigned int pic_trips, cg_trips;
@@ -251,6 +254,28 @@ void ens_cg_A(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, int parit
 void ens_cg_B(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, int parity);
 void ens_cg_finish(cudaStream_t s, EnsInst *E, const EnsCtl *ctl, int n, const int *b2i, int nblocks);
 void ens_cg_cond(cudaStream_t s, EnsInst *E, EnsCtl *ctl, int n, cudaGraphConditionalHandle h);
+
+// ensemble multigrid form: shk_mg.cu.  Each instance's hierarchy, its bottom level and, per level
+// depth, the instance's block range in the batched launch of that depth.
+struct EnsMgPlan {
+    int nlev, lb;                  // levels of the instance; its bottom level (the one-block kernel)
+    int vc_blocks[kMgMaxLevels];   // blocks of the level-d tile kernels (the context's own grid)
+    int set_blocks[kMgMaxLevels];  // blocks of the set-up kernel that produces level d
+    size_t bottom_smem;
+};
+int ens_mg_plan(Ctx *c, EnsMgPlan *plan);
+struct EnsMg *ens_mg_alloc(int n);  // device array of n descriptors
+int ens_mg_upload(struct EnsMg *dM, int i, Ctx *c, const int *blk0_vc, const int *blk0_set);
+void ens_mg_free(struct EnsMg *dM);
+int ens_mg_kernel_attrs();
+const struct EnsMg *ens_mg_at(const struct EnsMg *dM, int i);  // &dM[i]
+void ens_mg_setup(cudaStream_t s, EnsInst *E, const struct EnsMg *M, const int *const *b2i_set, const int *nb_set,
+                  int lmax);
+void ens_mg_vcycle(cudaStream_t s, EnsInst *E, const struct EnsMg *M, const int *const *b2i_vc, const int *nb_vc,
+                   int dmax, const int *b2i_bottom, int n, size_t bottom_smem, int mode, int parity);
+void ens_cg_init_mg(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks);
+void ens_cg_A_mg(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, int parity);
+enum { ENS_VC_INIT = 0, ENS_VC_ITER = 1 };
 
 // shk_mg.cu
 int mg_levels_for(int nx, int ny, int *dims, int maxl);

@@ -1327,6 +1327,26 @@ __global__ void __launch_bounds__(kThreads) k_ens_cg_init(EnsInst *E, const int 
                                I.counter, I.mask8);
 }
 
+// Multigrid form: r = b - A h with r'r and the GROUNDED b'b parked for the V-cycle's finish.
+__global__ void __launch_bounds__(kThreads) k_ens_cg_init_mg(EnsInst *E, const int *b2i) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_STENCIL);
+    if (!I.pic_active) return;
+    cg_init_body<double, false>(B, I.nx, I.ny, I.aP, I.aE, I.aN, I.st.h, I.rhs, I.r, I.x, I.cg, I.partials,
+                                I.counter, I.mask8);
+}
+
+// Multigrid form: p = z + beta p, Ap, p'Ap (the V-cycle's z in place of r/aP).
+__global__ void __launch_bounds__(kMarchX, 6) k_ens_cg_A_mg(EnsInst *E, const int *b2i, int parity) {
+    __shared__ EnsInst I;
+    const Blk B = ens_stage(I, E, b2i, EF_MARCH);
+    if (!I.pic_active) return;
+    const double *p_old = parity ? I.p1 : I.p0;
+    double *p_new = parity ? I.p0 : I.p1;
+    cg_A_body<double, false, false>(B, I.nx, I.ny, I.march_th, I.aP, I.aE, I.aN, I.r, I.z, p_old, p_new, I.Ap,
+                                    I.cg, I.partials, I.counter, DBL_EPSILON, nullptr);
+}
+
 __global__ void __launch_bounds__(kMarchX, 6) k_ens_cg_A(EnsInst *E, const int *b2i, int parity) {
     __shared__ EnsInst I;
     const Blk B = ens_stage(I, E, b2i, EF_MARCH);
@@ -1396,6 +1416,12 @@ void ens_cg_reset(cudaStream_t s, EnsInst *E, EnsCtl *ctl, int n) {
 }
 void ens_cg_init(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks) {
     k_ens_cg_init<<<nblocks, kThreads, 0, s>>>(E, b2i);
+}
+void ens_cg_init_mg(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks) {
+    k_ens_cg_init_mg<<<nblocks, kThreads, 0, s>>>(E, b2i);
+}
+void ens_cg_A_mg(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, int parity) {
+    k_ens_cg_A_mg<<<nblocks, kMarchX, 0, s>>>(E, b2i, parity);
 }
 void ens_cg_A(cudaStream_t s, EnsInst *E, const int *b2i, int nblocks, int parity) {
     k_ens_cg_A<<<nblocks, kMarchX, 0, s>>>(E, b2i, parity);

@@ -52,13 +52,11 @@ __global__ void k_mg_act0(int n, const uint8_t *m8, const double *aP, double ome
 // inverse diagonal (the arrays k_to_float_lapl and k_mg_act0 write), and per 2x2 aggregate the
 // level-1 Float64 operator (the sums above, dP computed from aP on the fly).  One thread per
 // aggregate on a 2D grid, so a warp reads 64 consecutive fine cells of each of its two rows.
-__global__ void __launch_bounds__(256) k_mg_level0(int nx, int ny, int nxc, int nyc, const uint8_t *m8,
-                                                   const double *aP, const double *aE, const double *aN,
-                                                   double omega, float *fE, float *fN, float *fD, float *fW,
-                                                   uint8_t *act0, double *aEc, double *aNc, double *dPc,
-                                                   uint8_t *actc) {
-    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
-    if (I >= nxc || J >= nyc) return;
+__device__ __forceinline__ void level0_aggregate(int I, int J, int nx, int ny, int nxc, const uint8_t *m8,
+                                                 const double *aP, const double *aE, const double *aN,
+                                                 double omega, float *fE, float *fN, float *fD, float *fW,
+                                                 uint8_t *act0, double *aEc, double *aNc, double *dPc,
+                                                 uint8_t *actc) {
     auto active = [&](size_t c) { return m8[c] == M_GROUNDED || m8[c] == M_UNKNOWN; };
     double dp[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     bool a[2][2] = {{false, false}, {false, false}};
@@ -109,15 +107,25 @@ __global__ void __launch_bounds__(256) k_mg_level0(int nx, int ny, int nxc, int 
     actc[k] = (uint8_t)act;
 }
 
+__global__ void __launch_bounds__(256) k_mg_level0(int nx, int ny, int nxc, int nyc, const uint8_t *m8,
+                                                   const double *aP, const double *aE, const double *aN,
+                                                   double omega, float *fE, float *fN, float *fD, float *fW,
+                                                   uint8_t *act0, double *aEc, double *aNc, double *dPc,
+                                                   uint8_t *actc) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= nxc || J >= nyc) return;
+    level0_aggregate(I, J, nx, ny, nxc, m8, aP, aE, aN, omega, fE, fN, fD, fW, act0, aEc, aNc, dPc, actc);
+}
+
 // The sums above and k_mg_finish_level's Float32 copies of coarse level l+1 (fine level l >= 1) in
 // one pass.  The damped diagonal needs the coarse west and south couplings of the neighbouring
 // aggregates; each thread recomputes them from the fine boundary they sum (same terms, same
 // order), so they equal the values those aggregates store.
-__global__ void k_mg_coarsen_finish(int nxf, int nyf, int nxc, int nyc, const double *aEf, const double *aNf,
-                                    const double *dPf, const uint8_t *actf, double omega, double *aEc,
-                                    double *aNc, double *dPc, uint8_t *actc, float *fE, float *fN, float *fD,
-                                    float *fW) {
-    GSTRIDE(k, nxc * nyc) {
+__device__ __forceinline__ void coarsen_finish_cell(int k, int nxf, int nyf, int nxc, const double *aEf,
+                                                    const double *aNf, const double *dPf, const uint8_t *actf,
+                                                    double omega, double *aEc, double *aNc, double *dPc,
+                                                    uint8_t *actc, float *fE, float *fN, float *fD, float *fW) {
+    {
         const int I = k % nxc, J = k / nxc;
         auto af = [&](int i, int j) { return i >= 0 && j >= 0 && i < nxf && j < nyf && actf[(size_t)i + (size_t)j * nxf]; };
         double d = 0.0, e = 0.0, no = 0.0;
@@ -171,18 +179,30 @@ __global__ void k_mg_coarsen_finish(int nxf, int nyf, int nxc, int nyc, const do
     }
 }
 
+__global__ void k_mg_coarsen_finish(int nxf, int nyf, int nxc, int nyc, const double *aEf, const double *aNf,
+                                    const double *dPf, const uint8_t *actf, double omega, double *aEc,
+                                    double *aNc, double *dPc, uint8_t *actc, float *fE, float *fN, float *fD,
+                                    float *fW) {
+    GSTRIDE(k, nxc * nyc)
+    coarsen_finish_cell(k, nxf, nyf, nxc, aEf, aNf, dPf, actf, omega, aEc, aNc, dPc, actc, fE, fN, fD, fW);
+}
+
 // Float32 copies and the smoother's damped inverse diagonal wD = omega/aP with the Jacobi diagonal
 // aP = dP + the four couplings (identity rows: aP = 1, wD = 1).
+__device__ __forceinline__ void finish_level_cell(int k, int nx, const double *aE, const double *aN,
+                                                  const double *dP, const uint8_t *act, double omega, float *fE,
+                                                  float *fN, float *fD, float *fW) {
+    const int ix = k % nx, iy = k / nx;
+    const double w = ix > 0 ? aE[k - 1] : 0.0, s = iy > 0 ? aN[k - nx] : 0.0;
+    fE[k] = (float)aE[k];
+    fN[k] = (float)aN[k];
+    fD[k] = (float)dP[k];
+    fW[k] = act[k] ? (float)(omega / (dP[k] + (aE[k] + w + aN[k] + s))) : 1.0f;
+}
+
 __global__ void k_mg_finish_level(int nx, int ny, const double *aE, const double *aN, const double *dP,
                                   const uint8_t *act, double omega, float *fE, float *fN, float *fD, float *fW) {
-    GSTRIDE(k, nx * ny) {
-        const int ix = k % nx, iy = k / nx;
-        const double w = ix > 0 ? aE[k - 1] : 0.0, s = iy > 0 ? aN[k - nx] : 0.0;
-        fE[k] = (float)aE[k];
-        fN[k] = (float)aN[k];
-        fD[k] = (float)dP[k];
-        fW[k] = act[k] ? (float)(omega / (dP[k] + (aE[k] + w + aN[k] + s))) : 1.0f;
-    }
+    GSTRIDE(k, nx * ny) finish_level_cell(k, nx, aE, aN, dP, act, omega, fE, fN, fD, fW);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -420,8 +440,8 @@ __device__ __forceinline__ void sweep_sm(FusedSm &S, const float (&XI)[kFSH][kFS
 // Descending half of level L: x1 = two sweeps from zero (written to xo), and the coarse rhs
 // bc = restriction of b - A x1.  1D grid striding over 32 x 16 tiles.
 template <typename TB, bool FB = false>
-__global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo, int nxc, int nyc, float *bc,
-                                                    FusedB fbv = FusedB{}, const CgDev *cg = nullptr) {
+__device__ __forceinline__ void mg_down_body(Blk B, const Lv &L, const TB *b, float *xo, int nxc, int nyc, float *bc,
+                                             FusedB fbv, const CgDev *cg) {
     if constexpr (FB) {
         const CgView cv = block_cg_view(cg);
         if (cv.done) return;
@@ -432,7 +452,7 @@ __global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo
     __shared__ FusedSm S;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // output rows: 32 x 8 threads
     const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (int t = B.id; t < ntiles; t += B.n) {
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
         stage_level<TB, false, FB>(S, L, b, x0, y0, nullptr, nullptr, nullptr, 0, 0.0f, &fbv);
         __syncthreads();
@@ -465,20 +485,26 @@ __global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo
     }
 }
 
+template <typename TB, bool FB = false>
+__global__ void __launch_bounds__(256, 6) k_mg_down(Lv L, const TB *b, float *xo, int nxc, int nyc, float *bc,
+                                                    FusedB fbv = FusedB{}, const CgDev *cg = nullptr) {
+    mg_down_body<TB, FB>(grid_blk(), L, b, xo, nxc, nyc, bc, fbv, cg);
+}
+
 // Ascending half of level L: xt = xi + omega_c P xc, then two sweeps.  LAST (level 0): the second
 // sweep writes z in Float64 and the outer CG's r'z, r'r finish the init or the iteration;
 // otherwise it writes the level's result to xo.
 template <typename TB, bool LAST>
-__global__ void __launch_bounds__(256, 6) k_mg_up(Lv L, const TB *b, const float *xi, const float *xc, int nxc, float wc,
-                                                  float *xo, double *z, CgDev *cg, int init, double *partials,
-                                                  unsigned int *counter) {
+__device__ __forceinline__ void mg_up_body(Blk B, const Lv &L, const TB *b, const float *xi, const float *xc, int nxc,
+                                           float wc, float *xo, double *z, CgDev *cg, int init, double *partials,
+                                           unsigned int *counter) {
     if (cg_finished(L.done)) return;
     __shared__ FusedSm S;
     __shared__ double r64[LAST ? kFCells : 1];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // output rows: 32 x 8 threads
     const int tiles_x = (L.nx + kFW - 1) / kFW, ntiles = tiles_x * ((L.ny + kFH - 1) / kFH);
     double red[2] = {0.0, 0.0};
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (int t = B.id; t < ntiles; t += B.n) {
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
         stage_level<TB, true>(S, L, b, x0, y0, LAST ? r64 : nullptr, xi, xc, nxc, wc);
         __syncthreads();
@@ -504,11 +530,18 @@ __global__ void __launch_bounds__(256, 6) k_mg_up(Lv L, const TB *b, const float
     }
     if (LAST) {
         double out[2];
-        if (grid_reduce<2, false>(red, partials, counter, out) && threadIdx.x == 0) {
+        if (grid_reduce<2, false>(B, red, partials, counter, out) && threadIdx.x == 0) {
             if (init) cg_init_finish(cg, out[0], cg->rr, cg->bnorm);
             else cg_iter_finish(cg, out[0], out[1]);
         }
     }
+}
+
+template <typename TB, bool LAST>
+__global__ void __launch_bounds__(256, 6) k_mg_up(Lv L, const TB *b, const float *xi, const float *xc, int nxc, float wc,
+                                                  float *xo, double *z, CgDev *cg, int init, double *partials,
+                                                  unsigned int *counter) {
+    mg_up_body<TB, LAST>(grid_blk(), L, b, xi, xc, nxc, wc, xo, z, cg, init, partials, counter);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1232,8 +1265,8 @@ struct BottomPlan {
     const int *done;
 };
 
-__global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b_top, float *x_top, int nu,
-                                                    float wc) {
+__device__ __forceinline__ void mg_bottom_body(const BottomPlan &P, const float *b_top, float *x_top, int nu,
+                                               float wc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (cg_finished(P.done)) return;
     const int T = P.total;
@@ -1321,6 +1354,11 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b
     }
     const float *X0 = Xb[L == 1 ? 0 : cur_up];
     for (int i = tid; i < P.lv[0].nx * P.lv[0].ny; i += nt) x_top[i] = X0[i];
+}
+
+__global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b_top, float *x_top, int nu,
+                                                    float wc) {
+    mg_bottom_body(P, b_top, x_top, nu, wc);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1810,6 +1848,214 @@ int mg_levels_for(int nx, int ny, int *dims, int maxl) {
         b = (b + 1) / 2;
     }
     return l;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Ensemble multigrid form: the V-cycle and its set-up batched over instances of uneven size.
+//
+// Each batched launch runs one level depth d of every instance that has it: the instance's blocks
+// form a contiguous range (its block -> instance table and range start per depth), and each block
+// runs the single-instance body on that instance's level with the instance's own block count, so
+// the descending halves, the bottom solve and the ascending halves run in the order the instance's
+// own V-cycle would: every instance's descending kernels depth by depth, then every instance's
+// bottom kernel (one block each, whatever its bottom level), then the ascending kernels from the
+// deepest depth up.  Instances between depths simply have no blocks in a launch.  The tile
+// kernels are the LDG-staged ones (a launch's TMA tensor maps describe one array, not one per
+// instance); the outer CG's x/r update is fused into the level-0 descending kernel as in the
+// single-instance LDG path, alternating the two residual buffers with the iteration parity.
+// ---------------------------------------------------------------------------------------------
+struct EnsMg {
+    int nlev, lb;
+    int blk0_vc[kMgMaxLevels], nblk_vc[kMgMaxLevels];
+    int blk0_set[kMgMaxLevels], nblk_set[kMgMaxLevels];
+    MgLevel lv[kMgMaxLevels];
+    BottomPlan bp;
+    float wc;
+    int nu;
+    double omega;
+};
+
+// block -> (instance, position in its range) for table `tab` of depth d
+struct EnsMgBlk {
+    int i;
+    Blk B;
+};
+__device__ __forceinline__ EnsMgBlk ens_mg_blk(const int *b2i, const EnsMg *M, bool vc, int d) {
+    const int i = b2i[blockIdx.x];
+    const EnsMg &G = M[i];
+    const int b0 = vc ? G.blk0_vc[d] : G.blk0_set[d], nb = vc ? G.nblk_vc[d] : G.nblk_set[d];
+    return EnsMgBlk{i, Blk{(int)blockIdx.x - b0, nb}};
+}
+
+// set-up of level d: d == 1 the level-0 pass (Float32 level 0 + level-1 sums), d == 2 level 1's
+// Float32 copies, d >= 3 the coarsening of level d - 2 into level d - 1 (stage numbers, not levels:
+// see ens_mg_setup)
+__global__ void __launch_bounds__(256) k_ens_mg_setup(EnsInst *E, const EnsMg *M, const int *b2i, int stage) {
+    const EnsMgBlk q = ens_mg_blk(b2i, M, false, stage);
+    if (!E[q.i].pic_active) return;
+    const EnsMg &G = M[q.i];
+    const int tid = q.B.id * blockDim.x + threadIdx.x, nth = q.B.n * blockDim.x;
+    if (stage == 1) {
+        const EnsInst &I = E[q.i];
+        const MgLevel &f = G.lv[0], &g = G.lv[1];
+        for (int k = tid; k < g.nx * g.ny; k += nth)
+            level0_aggregate(k % g.nx, k / g.nx, f.nx, f.ny, g.nx, I.mask8, I.aP, I.aE, I.aN, G.omega, (float *)f.aE,
+                             (float *)f.aN, (float *)f.dP, (float *)f.wD, f.act, g.aE64, g.aN64, g.dP64, g.act);
+    } else if (stage == 2) {
+        const MgLevel &g = G.lv[1];
+        for (int k = tid; k < g.nx * g.ny; k += nth)
+            finish_level_cell(k, g.nx, g.aE64, g.aN64, g.dP64, g.act, G.omega, (float *)g.aE, (float *)g.aN,
+                              (float *)g.dP, (float *)g.wD);
+    } else {
+        const MgLevel &f = G.lv[stage - 2], &g = G.lv[stage - 1];
+        for (int k = tid; k < g.nx * g.ny; k += nth)
+            coarsen_finish_cell(k, f.nx, f.ny, g.nx, f.aE64, f.aN64, f.dP64, f.act, G.omega, g.aE64, g.aN64, g.dP64,
+                                g.act, (float *)g.aE, (float *)g.aN, (float *)g.dP, (float *)g.wD);
+    }
+}
+
+// level 0 descending half: INIT stages r; an iteration applies the CG's x/r update (FB)
+template <bool FB>
+__global__ void __launch_bounds__(256, 6) k_ens_mg_down0(EnsInst *E, const EnsMg *M, const int *b2i, int parity) {
+    const EnsMgBlk q = ens_mg_blk(b2i, M, true, 0);
+    const EnsInst &I = E[q.i];
+    if (!I.pic_active) return;
+    const EnsMg &G = M[q.i];
+    const MgLevel &m = G.lv[0], &g = G.lv[1];
+    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done};
+    if constexpr (FB) {
+        const double *r_in = parity ? I.r2 : I.r;
+        double *r_out = parity ? I.r : I.r2;
+        const double *p_new = parity ? I.p0 : I.p1;
+        mg_down_body<double, true>(q.B, L, r_in, m.x[0], g.nx, g.ny, g.b, FusedB{I.Ap, p_new, I.x, r_out, 0.0}, I.cg);
+    } else {
+        mg_down_body<double, false>(q.B, L, I.r, m.x[0], g.nx, g.ny, g.b, FusedB{}, nullptr);
+    }
+}
+
+__global__ void __launch_bounds__(256, 6) k_ens_mg_down(EnsInst *E, const EnsMg *M, const int *b2i, int d) {
+    const EnsMgBlk q = ens_mg_blk(b2i, M, true, d);
+    const EnsInst &I = E[q.i];
+    if (!I.pic_active) return;
+    const EnsMg &G = M[q.i];
+    const MgLevel &m = G.lv[d], &g = G.lv[d + 1];
+    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done};
+    mg_down_body<float, false>(q.B, L, m.b, m.x[0], g.nx, g.ny, g.b, FusedB{}, nullptr);
+}
+
+// every instance's bottom solve, one block each (block i = instance i)
+__global__ void __launch_bounds__(1024) k_ens_mg_bottom(EnsInst *E, const EnsMg *M) {
+    const EnsInst &I = E[blockIdx.x];
+    if (!I.pic_active) return;
+    const EnsMg &G = M[blockIdx.x];
+    const MgLevel &m = G.lv[G.lb];
+    mg_bottom_body(G.bp, m.b, m.x[0], G.nu, G.wc);
+}
+
+__global__ void __launch_bounds__(256, 6) k_ens_mg_up(EnsInst *E, const EnsMg *M, const int *b2i, int d) {
+    const EnsMgBlk q = ens_mg_blk(b2i, M, true, d);
+    const EnsInst &I = E[q.i];
+    if (!I.pic_active) return;
+    const EnsMg &G = M[q.i];
+    const MgLevel &m = G.lv[d], &g = G.lv[d + 1];
+    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done};
+    const float *xc = g.x[d + 1 == G.lb ? 0 : 1];
+    mg_up_body<float, false>(q.B, L, m.b, m.x[0], xc, g.nx, G.wc, m.x[1], nullptr, nullptr, 0, nullptr, nullptr);
+}
+
+// level 0 ascending half: z and the CG's r'z, r'r (init or iteration finish) over the instance's
+// own reduction buffers
+__global__ void __launch_bounds__(256, 6) k_ens_mg_up0(EnsInst *E, const EnsMg *M, const int *b2i, int init,
+                                                       int parity) {
+    const EnsMgBlk q = ens_mg_blk(b2i, M, true, 0);
+    const EnsInst &I = E[q.i];
+    if (!I.pic_active) return;
+    const EnsMg &G = M[q.i];
+    const MgLevel &m = G.lv[0], &g = G.lv[1];
+    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done};
+    const double *r = init ? I.r : (parity ? I.r : I.r2);  // the iteration's new residual buffer
+    const float *xc = g.x[1 == G.lb ? 0 : 1];
+    mg_up_body<double, true>(q.B, L, r, m.x[0], xc, g.nx, G.wc, nullptr, I.z, I.cg, init, I.partials, I.counter);
+}
+
+int ens_mg_plan(Ctx *c, EnsMgPlan *plan) {
+    if (c->mg_levels < 2) return fail(c, SHK_BAD_ARG, "the ensemble's multigrid form needs two or more levels");
+    if (!(c->mg_fused && c->mg_nu == 2)) return fail(c, SHK_BAD_ARG, "the ensemble's multigrid form runs nu = 2");
+    plan->nlev = c->mg_levels;
+    plan->lb = bottom_level(c);
+    for (int l = 0; l < kMgMaxLevels; l++) plan->vc_blocks[l] = plan->set_blocks[l] = 0;
+    for (int l = 0; l < plan->lb; l++) plan->vc_blocks[l] = fused_grid(c, c->mg[l]);
+    // set-up stages 1 .. nlev: 1 and 2 produce level 1, s >= 3 level s - 1
+    for (int st = 1; st <= plan->nlev; st++) {
+        const MgLevel &g = c->mg[st <= 2 ? 1 : st - 1];
+        plan->set_blocks[st] = st - 1 < plan->nlev ? mg_grid(c, (long long)g.nx * g.ny) : 0;
+    }
+    BottomPlan P;
+    plan->bottom_smem = bottom_plan(c, plan->lb, &P);
+    return SHK_OK;
+}
+
+EnsMg *ens_mg_alloc(int n) {
+    EnsMg *d = nullptr;
+    if (cudaMalloc(&d, (size_t)n * sizeof(EnsMg)) != cudaSuccess) return nullptr;
+    return d;
+}
+const EnsMg *ens_mg_at(const EnsMg *dM, int i) { return dM + i; }
+void ens_mg_free(EnsMg *dM) {
+    if (dM) cudaFree(dM);
+}
+
+int ens_mg_upload(EnsMg *dM, int i, Ctx *c, const int *blk0_vc, const int *blk0_set) {
+    EnsMgPlan plan;
+    int rc = ens_mg_plan(c, &plan);
+    if (rc) return rc;
+    EnsMg G;
+    memset(&G, 0, sizeof(G));
+    G.nlev = plan.nlev;
+    G.lb = plan.lb;
+    for (int l = 0; l < kMgMaxLevels; l++) {
+        G.blk0_vc[l] = blk0_vc[l];
+        G.nblk_vc[l] = plan.vc_blocks[l];
+        G.blk0_set[l] = blk0_set[l];
+        G.nblk_set[l] = plan.set_blocks[l];
+    }
+    for (int l = 0; l < G.nlev; l++) G.lv[l] = c->mg[l];
+    bottom_plan(c, plan.lb, &G.bp);
+    G.bp.done = &c->dev->cg.done;
+    G.wc = c->mg_omega_c;
+    G.nu = c->mg_nu;
+    G.omega = (double)c->mg_omega;
+    return cudaMemcpy(dM + i, &G, sizeof(G), cudaMemcpyHostToDevice) == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+// The set-up of every instance's hierarchy after its assembly (mg_setup's sequence, stage by stage).
+void ens_mg_setup(cudaStream_t s, EnsInst *E, const EnsMg *M, const int *const *b2i_set, const int *nb_set,
+                  int lmax) {
+    for (int st = 1; st <= lmax; st++)
+        if (nb_set[st] > 0) k_ens_mg_setup<<<nb_set[st], 256, 0, s>>>(E, M, b2i_set[st], st);
+}
+
+// One V-cycle of every instance: INIT on r (the CG's set-up), ITER with the CG's x/r update of
+// iteration `parity` fused into level 0.
+void ens_mg_vcycle(cudaStream_t s, EnsInst *E, const EnsMg *M, const int *const *b2i_vc, const int *nb_vc, int dmax,
+                   const int *b2i_bottom, int n, size_t bottom_smem, int mode, int parity) {
+    (void)b2i_bottom;
+    if (mode == ENS_VC_INIT) k_ens_mg_down0<false><<<nb_vc[0], 256, 0, s>>>(E, M, b2i_vc[0], parity);
+    else k_ens_mg_down0<true><<<nb_vc[0], 256, 0, s>>>(E, M, b2i_vc[0], parity);
+    for (int d = 1; d < dmax; d++)
+        if (nb_vc[d] > 0) k_ens_mg_down<<<nb_vc[d], 256, 0, s>>>(E, M, b2i_vc[d], d);
+    k_ens_mg_bottom<<<n, 1024, bottom_smem, s>>>(E, M);
+    for (int d = dmax - 1; d >= 1; d--)
+        if (nb_vc[d] > 0) k_ens_mg_up<<<nb_vc[d], 256, 0, s>>>(E, M, b2i_vc[d], d);
+    k_ens_mg_up0<<<nb_vc[0], 256, 0, s>>>(E, M, b2i_vc[0], mode == ENS_VC_INIT ? 1 : 0, parity);
+}
+
+// The ensemble bottom kernel's dynamic shared memory limit on the current device.
+int ens_mg_kernel_attrs() {
+    return cudaFuncSetAttribute(k_ens_mg_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBottomBytes) ==
+                   cudaSuccess
+               ? SHK_OK
+               : SHK_CUDA_ERROR;
 }
 
 // The first-wait poll count of the TMA-staged kernels on the current device: kTmaSpin, or the

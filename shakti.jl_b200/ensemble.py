@@ -5,7 +5,9 @@ instances (parameter sweeps, uncertainty ensembles) loops over them.  `Ensemble(
 them together: every kernel of a timestep is one launch over all instances, each timestep is one
 CUDA graph launch whose Picard and CG loops run on the device, and the CG stencil kernel's tile
 height is autotuned per grid size.  Each instance ends with the fields its own `run` would give
-(Float64 Jacobi CG, elliptic head scheme, constant melt input, no head relaxation).
+(Float64 CG preconditioned by Jacobi or by the Float32 multigrid V-cycle -- the mixed-precision
+form, with every level kernel batched over the instances -- elliptic head scheme, constant melt
+input, no head relaxation).
 """
 from __future__ import annotations
 
@@ -29,8 +31,8 @@ class Ensemble:
             if sim.dt != dt:
                 raise ValueError("every simulation of an ensemble uses the same dt")
             ls, ps = sim.ls, sim.hs.ps
-            if ls.multigrid or ls.precond is not None or ls.precision != "fp64":
-                raise ValueError(f"simulation {k}: the ensemble runs Float64 Jacobi CG")
+            if ls.precond is not None or ls.precision != "fp64":
+                raise ValueError(f"simulation {k}: the ensemble runs Float64 CG, Jacobi- or multigrid-preconditioned")
             if ps.hr.alpha > 0:
                 raise ValueError(f"simulation {k}: the ensemble runs without head relaxation")
         self.sims = sims
@@ -41,8 +43,8 @@ class Ensemble:
             po, o = sim.hs.ps.opts(), sim.ls.opts()
             if (po.iters, po.tol, po.check_every) != (self._po.iters, self._po.tol, self._po.check_every):
                 raise ValueError(f"simulation {k}: every PicardSolver of an ensemble has the same iters/tol")
-            if (o.atol, o.rtol, o.stop_rule, o.itmax) != (self._o.atol, self._o.rtol, self._o.stop_rule,
-                                                          self._o.itmax):
+            if (o.atol, o.rtol, o.stop_rule, o.itmax, o.precond) != (self._o.atol, self._o.rtol, self._o.stop_rule,
+                                                                      self._o.itmax, self._o.precond):
                 raise ValueError(f"simulation {k}: every CGIterativeSolver of an ensemble has the same tolerances")
         self._ctxs = [sim.ctx() for sim in sims]  # binds each instance's state, parameters and law
         self.L = self._ctxs[0].L

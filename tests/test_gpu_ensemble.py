@@ -25,7 +25,7 @@ SPECS = [(48, 48, 11, 5e3, 1e-9), (64, 40, 12, 2e4, 1e-8), (37, 53, 13, 5e4, 5e-
          (64, 64, 15, 3e4, 3e-8)]
 
 
-def make_sim(shk, nx, ny, seed, C, melt, tsteps, rtol=None):
+def make_sim(shk, nx, ny, seed, C, melt, tsteps, rtol=None, multigrid=False):
     w = shk.configs.plain(nx, 10e3 * nx / 64, seed=seed, ny=ny, ly=10e3 * ny / 64, C=C)
     w.inputs["ieb"] = np.full((nx, ny), melt, order="F")
     g = shk.Grid(w.nx, w.ny, w.lx, w.ly)
@@ -36,7 +36,8 @@ def make_sim(shk, nx, ny, seed, C, melt, tsteps, rtol=None):
     if rtol is None:  # Krylov.jl defaults, the reference's configuration
         ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem)
     else:
-        ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, stop_rule="relres", rtol=rtol, atol=0.0)
+        ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, stop_rule="relres", rtol=rtol, atol=0.0,
+                                   multigrid=multigrid)
     ps = shk.PicardSolver(500, 1e-6, ls, g)
     return shk.Simulation(g, s, tsteps, 3600.0, pm, "implicit", [], shk.ConstantMeltInput(), sl, ps=ps)
 
@@ -98,10 +99,51 @@ def test_ensemble_continues_across_runs_and_reports_blocks(shk, cuda):
     ens.close()
 
 
+# ragged sizes whose V-cycles end at different bottom levels (depths 1 to 3 above the bottom kernel)
+MG_SPECS = [(48, 48, 31, 5e3, 1e-9), (200, 150, 32, 2e4, 1e-8), (256, 256, 33, 5e4, 5e-8), (37, 53, 34, 1e4, 1e-7),
+            (512, 384, 35, 3e4, 3e-8)]
+
+
+def test_ensemble_multigrid_form_matches_single_instance_runs(shk, cuda, monkeypatch):
+    """The mixed-precision form (Float64 CG, Float32 multigrid V-cycle) batched over instances: every
+    level kernel is one launch over the instances that have that level, each instance's bottom
+    solve one block of one launch.  Against each instance's own run through the same (LDG-staged)
+    level kernels, with the context's own CG tile height (no autotune): equal Picard counts, fields
+    within 1e-10."""
+    monkeypatch.setenv("SHK_MG_TMA", "0")  # read at context creation: the single runs' staging
+    steps = 3
+    ens_sims = [make_sim(shk, *sp, steps, rtol=1e-10, multigrid=True) for sp in MG_SPECS]
+    ref_sims = [make_sim(shk, *sp, steps, rtol=1e-10, multigrid=True) for sp in MG_SPECS]
+    ens = shk.Ensemble(ens_sims, autotune_iters=0)
+    stats = ens.run(steps)
+    for sim, st in zip(ref_sims, stats):
+        pic = cg = 0
+        for _ in range(steps):
+            shk.step(sim)
+            sim.total_time += sim.dt
+            pic += sim.hs.ps.last_iter
+            cg += sim.hs.ps.cg_iters_total
+            assert sim.hs.ps.converged
+        assert st["steps_converged"] == steps
+        assert st["picard_iters"] == pic, (sim.grid.nx, st["picard_iters"], pic)
+        assert abs(st["cg_iters"] - cg) <= pic, (sim.grid.nx, st["cg_iters"], cg)
+    for e, r in zip(ens_sims, ref_sims):
+        a, b = e.state.to_numpy(list(FIELDS)), r.state.to_numpy(list(FIELDS))
+        for f in FIELDS:
+            assert relerr(a[f], b[f]) <= 1e-10, (e.grid.nx, e.grid.ny, f, relerr(a[f], b[f]))
+    # the Jacobi form afterwards on the same ensemble (the timestep graph is rebuilt for the form)
+    for sim in ens_sims:
+        sim.hs.ps.ls.multigrid = False
+    ens._o = ens_sims[0].ls.opts()
+    stats = ens.run(1)
+    assert all(s["steps"] == steps + 1 for s in stats)
+    ens.close()
+
+
 def test_ensemble_rejects_unsupported_forms(shk, cuda):
     sim = make_sim(shk, *SPECS[0], 1)
     g = sim.grid
-    sim.hs.ps.ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, multigrid=True, stop_rule="relres",
+    sim.hs.ps.ls = shk.CGIterativeSolver(g, shk.MatrixFreeLinearSystem, chebyshev_degree=4, stop_rule="relres",
                                          rtol=1e-8, atol=0.0)
     with pytest.raises(ValueError):
         shk.Ensemble([sim])
