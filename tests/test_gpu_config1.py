@@ -3,10 +3,10 @@ Harmonic k-faces, Jacobi and Chebyshev(4) CG, explicit and implicit gap schemes,
 parabolic run with e_v = 1e-3, each against the oracle (the CPU restatement of the reference
 algorithm, Float64) through the C ABI.
 
-The workload description asks for 100 timesteps; a 1024^2 timestep of the CPU oracle takes 5-15 s
-on the host cores, so the elliptic runs cover 2 timesteps with Jacobi and 1 with Chebyshev(4) (four
-matvecs per iteration on the CPU) per gap scheme, and the parabolic run 4, at
-a tight linear tolerance (||b - A h|| <= 1e-12 ||b_G||, b_G the GROUNDED rows) so that the two
+The workload description asks for 100 timesteps; a 1024^2 timestep of the CPU oracle takes tens of
+seconds to minutes on the host cores (thousands of CG iterations at this tolerance, four matvecs
+each with Chebyshev(4)), so each elliptic run covers one timestep -- its Picard loop and then the
+explicit or implicit gap update -- and the parabolic run 4, at a tight linear tolerance (||b - A h|| <= 1e-12 ||b_G||, b_G the GROUNDED rows) so that the two
 sides' Krylov iterates stay together.  Bar: Picard iteration counts equal step by step, fields h,
 N, b, q within 1e-10 (relative max-norm), the north-star tolerance."""
 import numpy as np
@@ -16,15 +16,14 @@ from test_gpu_parity import assert_fields_close, run_pair
 
 pytestmark = pytest.mark.gpu
 
-STEPS = 2
+STEPS = 1
 
 
 @pytest.mark.parametrize("precond,gap", [(0, "explicit"), (0, "implicit"), (1, "explicit"), (1, "implicit")])
 def test_config1_elliptic(shk, orc, cuda, precond, gap):
     w = shk.configs.plain1024()
-    # Chebyshev(4) costs the CPU oracle four matvecs per iteration: one timestep
-    sim, s, st, stats = run_pair(shk, orc, cuda, w, STEPS if precond == 0 else 1, 1800.0, precond=precond,
-                                 kfs="harmonic", gap=gap, rtol=1e-12, atol=0.0, stop_rule="relres")
+    sim, s, st, stats = run_pair(shk, orc, cuda, w, STEPS, 1800.0, precond=precond, kfs="harmonic", gap=gap,
+                                 rtol=1e-12, atol=0.0, stop_rule="relres")
     for a, b in zip(sim.step_stats, stats):
         assert a["converged"] and b["converged"]
         assert a["last_iter"] == b["last_iter"], (a, b)
