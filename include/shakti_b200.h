@@ -289,6 +289,10 @@ SHK_API int shk_ensemble_launch_counts(const void *ens, int *stencil, int *march
 SHK_API int shk_nn_conv3x3(const void *X, const void *Wt, const float *bias, void *Y, float *Yf, int N,
                            int H, int W, int Cin, int Cout, int relu, int flip, void *stream);
 /* dW[tap][co][ci] += sum_p dY[p][co] X[p + off(tap)][ci]   (Cout % 16 == 0, Cin % 8 == 0) */
+/* The tensor-core convolution's fault word on the current device: 1 when one of its bounded waits
+ * ran out since the last call (its results are then invalid); read and cleared.  No counterpart in
+ * the reference. */
+SHK_API int shk_nn_conv_fault(int *fault);
 SHK_API int shk_nn_conv3x3_wgrad(const void *X, const void *dY, float *dW, int N, int H, int W, int Cin,
                                  int Cout, void *stream);
 /* dYm = dY * (Y > 0) (relu = 0: dY) as BF16; db[c] += sum over the P pixels (db may be NULL) */

@@ -112,6 +112,7 @@ SIGNATURES = {
     "shk_nn_conv3x3": (C.c_int, [VP, VP, FP, VP, FP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                  C.c_int, VP]),
     "shk_nn_conv3x3_wgrad": (C.c_int, [VP, VP, FP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, VP]),
+    "shk_nn_conv_fault": (C.c_int, [C.POINTER(C.c_int)]),
     "shk_nn_relu_grad": (C.c_int, [FP, VP, VP, FP, C.c_longlong, C.c_int, C.c_int, VP]),
     "shk_nn_pool2": (C.c_int, [VP, VP, C.c_int, C.c_int, C.c_int, C.c_int, VP]),
     "shk_nn_pool2_grad": (C.c_int, [FP, FP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, VP]),

@@ -20,6 +20,7 @@
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 
 #include "../../include/shakti_b200.h"
 
@@ -105,6 +106,200 @@ __global__ void __launch_bounds__(128) k_conv3x3(const bf16 *__restrict__ X, con
             if (Yf) { Yf[r1 * Cout + co] = o[2]; Yf[r1 * Cout + co + 1] = o[3]; }
         }
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// 3x3 convolution on the 5th-generation tensor cores (tcgen05, sm_100a): the same implicit GEMM,
+// D[pixel, co] = sum_{tap, ci} X[pixel + off(tap), ci] W[tap, co, ci], with a CTA tile of 128
+// pixels (M) x NT output channels (N, Cout rounded up to a multiple of 16) and the Float32
+// accumulator in tensor memory (TMEM, NT columns of 128 lanes).  K runs over (tap, 32- or
+// 16-channel chunk); each chunk's A (128 x KC) and B (NT x KC) tiles are staged in shared memory in
+// the canonical K-major layout without swizzle -- 8-row x 16-byte core matrices, the two 8-element
+// K halves 128 B apart (LBO), 8-row groups 256 B apart (SBO) -- by all threads (zero fill outside
+// the image and past Cout), then one thread issues the chunk's K = 16 MMAs and commits them to the
+// stage's mbarrier.  Two stages: chunk c + 1 is staged while the tensor cores run chunk c.  The
+// epilogue reads each warp's 32 TMEM lanes (its 32 pixels) 8 columns at a time (tcgen05.ld),
+// adds the bias, applies ReLU and stores BF16 and/or Float32.  Every mbarrier wait is bounded; a
+// wait that runs out sets *err, and the CTA still waits for its MMAs and frees its TMEM.
+// ---------------------------------------------------------------------------------------------
+constexpr long kTcSpin = 1L << 22;
+
+__device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (sm_100 format): start address, LBO and SBO in 16-byte units,
+// version 1 at bit 46, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of kind::f16: Float32 D (bit 4), BF16 A (bits 7-9) and B (bits 10-12),
+// both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity) {
+    for (long i = 0; i < kTcSpin; i++) {
+        uint32_t ok;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(ok)
+                     : "r"(su32(bar)), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+constexpr int kTcM = 128, kTcKC = 32;  // pixels per CTA, largest channel chunk
+
+// Shared memory per CTA: two stages, the two mbarriers and the TMEM address slot, padded so that
+// the CTAs resident on an SM (228 KB of shared memory, 1 KB reserved per CTA) never ask for more
+// than the 512 TMEM columns together.
+template <int NT>
+struct TcLayout {
+    static constexpr uint32_t cols = NT < 32 ? 32 : NT;
+    static constexpr uint32_t a = kTcM * kTcKC * 2, b = NT * kTcKC * 2, stage = a + b;
+    static constexpr uint32_t bars = 2 * stage, slot = bars + 16, used = slot + 16;
+    static constexpr uint32_t pad = 233472u / (512u / cols) - 2048u;
+    static constexpr uint32_t bytes = used > pad ? used : pad;
+};
+
+template <int NT>
+__global__ void __launch_bounds__(128) k_conv3x3_tc(const bf16 *__restrict__ X, const bf16 *__restrict__ Wt,
+                                                    const float *__restrict__ bias, bf16 *__restrict__ Y,
+                                                    float *__restrict__ Yf, int N, int H, int W, int Cin, int Cout,
+                                                    int relu, int flip, int *err) {
+    using Lay = TcLayout<NT>;
+    constexpr uint32_t kCols = Lay::cols;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Lay::bars);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(sm + Lay::slot);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long P = (long long)N * H * W, p0 = (long long)blockIdx.x * kTcM;
+    const int KC = (Cin % kTcKC == 0) ? kTcKC : 16, nk = KC / 16, per_tap = Cin / KC, nch = 9 * per_tap;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(slot)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *slot;
+
+    // this thread's pixels' coordinates are recomputed per segment (each thread stages several rows)
+    auto stage_chunk = [&](int c, int st) {
+        const int tap = c / per_tap, c0 = (c % per_tap) * KC;
+        int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        if (flip) { dy = -dy; dx = -dx; }
+        unsigned char *A = sm + st * Lay::stage, *B = A + Lay::a;
+        const int segs_row = KC / 8;
+        for (int q = tid; q < kTcM * segs_row; q += blockDim.x) {
+            const int r = q / segs_row, g8 = q % segs_row, j = g8 >> 1, kh = g8 & 1;
+            const long long p = p0 + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (p < P) {
+                const long long hw = (long long)H * W;
+                const int n = (int)(p / hw), rem = (int)(p % hw), y = rem / W + dy, x = rem % W + dx;
+                if (y >= 0 && y < H && x >= 0 && x < W)
+                    v = *reinterpret_cast<const uint4 *>(X + (((long long)n * H + y) * W + x) * Cin + c0 + g8 * 8);
+            }
+            *reinterpret_cast<uint4 *>(A + j * (kTcM * 32) + (r >> 3) * 256 + kh * 128 + (r & 7) * 16) = v;
+        }
+        for (int q = tid; q < NT * segs_row; q += blockDim.x) {
+            const int r = q / segs_row, g8 = q % segs_row, j = g8 >> 1, kh = g8 & 1;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (r < Cout) v = *reinterpret_cast<const uint4 *>(Wt + ((long long)tap * Cout + r) * Cin + c0 + g8 * 8);
+            *reinterpret_cast<uint4 *>(B + j * (NT * 32) + (r >> 3) * 256 + kh * 128 + (r & 7) * 16) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
+    };
+
+    constexpr uint32_t idesc = umma_idesc_bf16(kTcM, NT);
+    bool ok = true;
+    stage_chunk(0, 0);
+    __syncthreads();
+    for (int c = 0; c < nch; c++) {
+        const int st = c & 1;
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t A = su32(sm + st * Lay::stage), B = A + Lay::a;
+            for (int j = 0; j < nk; j++) {
+                const uint64_t da = umma_desc(A + j * (kTcM * 32), 128, 256);
+                const uint64_t db = umma_desc(B + j * (NT * 32), 128, 256);
+                const uint32_t acc = (c > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t .reg .pred pacc;\n\t setp.ne.b32 pacc, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, pacc;\n\t}"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             su32(&bar[st]))
+                         : "memory");
+        }
+        if (c + 1 < nch) {
+            // stage st ^ 1 was last read by chunk c - 1's MMAs
+            if (c >= 1) ok = ok && tc_wait(&bar[st ^ 1], ((c - 1) >> 1) & 1);
+            ok = __syncthreads_and(ok) != 0;  // uniform: every thread leaves the loop together
+            if (!ok) break;
+            stage_chunk(c + 1, st ^ 1);
+            __syncthreads();
+        }
+    }
+    // the last commit covers every MMA this CTA issued
+    const int last = ok ? nch - 1 : -1;
+    bool done_all = true;
+    if (last >= 0) done_all = tc_wait(&bar[last & 1], (last >> 1) & 1);
+    else {  // gave up early: wait (bounded) for whatever was committed before freeing TMEM
+        for (int st = 0; st < 2; st++) tc_wait(&bar[st], 0);
+        done_all = false;
+    }
+    done_all = __syncthreads_and(done_all) != 0;  // uniform: tcgen05.ld below is warp-collective
+    if (!done_all && tid == 0) atomicExch(err, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (done_all) {
+        const long long p = p0 + warp * 32 + lane;
+        for (int cb = 0; cb < NT; cb += 8) {
+            uint32_t v[8];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (p >= P || cb >= Cout) continue;
+            float o[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                o[k] = __uint_as_float(v[k]) + (bias ? bias[cb + k] : 0.0f);
+                if (relu) o[k] = o[k] > 0.0f ? o[k] : 0.0f;
+            }
+            if (Y) {
+                uint4 pk = make_uint4(pack2(__float2bfloat16(o[0]), __float2bfloat16(o[1])),
+                                      pack2(__float2bfloat16(o[2]), __float2bfloat16(o[3])),
+                                      pack2(__float2bfloat16(o[4]), __float2bfloat16(o[5])),
+                                      pack2(__float2bfloat16(o[6]), __float2bfloat16(o[7])));
+                *reinterpret_cast<uint4 *>(Y + p * Cout + cb) = pk;
+            }
+            if (Yf) {
+                *reinterpret_cast<float4 *>(Yf + p * Cout + cb) = make_float4(o[0], o[1], o[2], o[3]);
+                *reinterpret_cast<float4 *>(Yf + p * Cout + cb + 4) = make_float4(o[4], o[5], o[6], o[7]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -357,21 +552,79 @@ static int grid_for(long long n) {
 
 using namespace shk::nn;
 
+// Per device: the tensor-core convolution's fault word (set when one of its bounded waits runs out).
+static int *g_tc_fault[64] = {};
+
+static int tc_fault_word(int dev, int **out) {
+    if (dev < 0 || dev >= 64) return SHK_BAD_ARG;
+    if (!g_tc_fault[dev]) {
+        int *p = nullptr;
+        if (cudaMalloc(&p, sizeof(int)) != cudaSuccess || cudaMemset(p, 0, sizeof(int)) != cudaSuccess)
+            return SHK_CUDA_ERROR;
+        g_tc_fault[dev] = p;
+    }
+    *out = g_tc_fault[dev];
+    return SHK_OK;
+}
+
+template <int NT>
+static int launch_conv_tc(const bf16 *x, const bf16 *w, const float *bias, bf16 *y, float *Yf, int N, int H, int W,
+                          int Cin, int Cout, int relu, int flip, cudaStream_t s) {
+    static int attr_done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int *fault = nullptr;
+    if (int rc = tc_fault_word(dev, &fault)) return rc;
+    if (!attr_done[dev]) {
+        if (cudaFuncSetAttribute(k_conv3x3_tc<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TcLayout<NT>::bytes) != cudaSuccess)
+            return SHK_CUDA_ERROR;
+        attr_done[dev] = 1;
+    }
+    const long long P = (long long)N * H * W;
+    k_conv3x3_tc<NT><<<(unsigned)((P + kTcM - 1) / kTcM), 128, TcLayout<NT>::bytes, s>>>(
+        x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, fault);
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+// tcgen05 form (default): N tile = Cout rounded up to 16 (<= 256).  SHK_NN_MMA_SYNC=1 selects the
+// mma.sync form (kept as the comparison for the tensor-core form's tests).
 extern "C" {
 
 SHK_API int shk_nn_conv3x3(const void *X, const void *Wt, const float *bias, void *Y, float *Yf, int N, int H, int W,
                            int Cin, int Cout, int relu, int flip, void *stream) {
     if (!X || !Wt || (!Y && !Yf) || N < 1 || H < 1 || W < 1 || Cin % 16 || Cout % 8) return SHK_BAD_ARG;
     const long long P = (long long)N * H * W;
-    const int NT = Cout % 64 == 0 ? 64 : (Cout % 32 == 0 ? 32 : 8);
-    dim3 grid((unsigned)((P + 63) / 64), (unsigned)(Cout / NT));
     cudaStream_t s = (cudaStream_t)stream;
     const bf16 *x = (const bf16 *)X, *w = (const bf16 *)Wt;
     bf16 *y = (bf16 *)Y;
+    static const bool legacy = getenv("SHK_NN_MMA_SYNC") && atoi(getenv("SHK_NN_MMA_SYNC")) != 0;
+    if (!legacy && Cout <= 256) {
+        const int nt = (Cout + 15) / 16 * 16;
+        if (nt <= 16) return launch_conv_tc<16>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s);
+        if (nt <= 32) return launch_conv_tc<32>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s);
+        if (nt <= 64) return launch_conv_tc<64>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s);
+        if (nt <= 128) return launch_conv_tc<128>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s);
+        return launch_conv_tc<256>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s);
+    }
+    const int NT = Cout % 64 == 0 ? 64 : (Cout % 32 == 0 ? 32 : 8);
+    dim3 grid((unsigned)((P + 63) / 64), (unsigned)(Cout / NT));
     if (NT == 64) k_conv3x3<64><<<grid, 128, 0, s>>>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip);
     else if (NT == 32) k_conv3x3<32><<<grid, 128, 0, s>>>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip);
     else k_conv3x3<8><<<grid, 128, 0, s>>>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip);
     return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+// The tensor-core convolution's fault word on the current device (1 when one of its bounded waits
+// ran out since the last call), read and cleared; synchronises the device.
+SHK_API int shk_nn_conv_fault(int *fault) {
+    if (!fault) return SHK_BAD_ARG;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int *w = nullptr;
+    if (int rc = tc_fault_word(dev, &w)) return rc;
+    if (cudaMemcpy(fault, w, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SHK_CUDA_ERROR;
+    return cudaMemset(w, 0, sizeof(int)) == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
 }
 
 SHK_API int shk_nn_conv3x3_wgrad(const void *X, const void *dY, float *dW, int N, int H, int W, int Cin, int Cout,

@@ -36,6 +36,50 @@ def ws(shk, cuda):
     return warmstart
 
 
+@pytest.mark.parametrize("ci,co,N,H,W", [(16, 32, 1, 40, 37), (32, 64, 2, 16, 24), (64, 128, 1, 33, 17),
+                                         (128, 256, 1, 20, 20), (32, 8, 1, 13, 11)])
+def test_tensor_core_convolution(ws, cuda, monkeypatch, ci, co, N, H, W):
+    """The tcgen05 convolution (128-pixel x Cout tiles, TMEM accumulator): forward with bias and ReLU
+    and the flipped input-gradient form, against the oracle and the mma.sync form; ragged pixel
+    counts, 16-channel chunks (Cin = 16), Cout padded to the 16-wide tile (Cout = 8), the 256-wide
+    tile.  Both tensor-core forms accumulate BF16 products in Float32 (1e-5)."""
+    torch = cuda
+    net = ws.WarmStartNet(seed=3)
+    L, s = net.L, net._s()
+    g = np.random.default_rng(ci + co)
+    X = torch.from_numpy(g.normal(0, 1, size=(N, H, W, ci)).astype(np.float32)).cuda().to(torch.bfloat16)
+    Wf = g.normal(0, 0.1, size=(9, co, ci)).astype(np.float32)
+    bias = torch.from_numpy(g.normal(0, 0.1, size=co).astype(np.float32)).cuda()
+    wb = torch.from_numpy(Wf).cuda().to(torch.bfloat16)
+    Xn, Wn = X.float().cpu().numpy(), wb.float().cpu().numpy()
+    out = {}
+    for form in ("tc", "mma_sync"):
+        if form == "mma_sync":
+            monkeypatch.setenv("SHK_NN_MMA_SYNC", "1")
+        Yf = torch.empty((N, H, W, co), dtype=torch.float32, device="cuda")
+        Yb = torch.empty((N, H, W, co), dtype=torch.bfloat16, device="cuda")
+        assert L.shk_nn_conv3x3(ws._p(X), ws._p(wb), ws._fp(bias), ws._p(Yb), ws._fp(Yf), N, H, W, ci, co, 1, 0,
+                                s) == 0
+        dX = None
+        if co % 16 == 0:  # the input gradient needs Cin % 16 == 0 on its own input
+            wt = torch.from_numpy(np.ascontiguousarray(Wf.transpose(0, 2, 1))).cuda().to(torch.bfloat16)
+            dX = torch.empty((N, H, W, ci), dtype=torch.float32, device="cuda")
+            assert L.shk_nn_conv3x3(ws._p(Yb), ws._p(wt), None, None, ws._fp(dX), N, H, W, co, ci, 0, 1, s) == 0
+        torch.cuda.synchronize()
+        out[form] = (Yf.cpu().numpy(), Yb.float().cpu().numpy(), None if dX is None else dX.cpu().numpy())
+        monkeypatch.delenv("SHK_NN_MMA_SYNC", raising=False)
+    fault = C.c_int(-1)
+    assert L.shk_nn_conv_fault(C.byref(fault)) == 0 and fault.value == 0
+    ref = no.conv3x3(Xn, Wn, bias.cpu().numpy(), relu=True)
+    assert rel(out["tc"][0], ref) < 1e-5
+    assert rel(out["tc"][0], out["mma_sync"][0]) < 1e-5
+    assert np.array_equal(out["tc"][1], no.bf16(out["tc"][0]))  # the BF16 output is the rounded Float32 one
+    if out["tc"][2] is not None:
+        ref_dx = no.conv3x3(out["tc"][1], Wn.transpose(0, 2, 1), None, flip=True)
+        assert rel(out["tc"][2], ref_dx) < 1e-5
+        assert rel(out["tc"][2], out["mma_sync"][2]) < 1e-5
+
+
 def test_kernels_match_oracle(ws, cuda):
     torch = cuda
     net = ws.WarmStartNet(seed=3)
