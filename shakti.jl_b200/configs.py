@@ -205,14 +205,15 @@ def ensemble_member(nx: int, seed: int, slope: float, melt: float, C: float, b0:
     return Workload(f"member{nx}", nx, ny, lx, ly, inputs, sliding_C=C, seed=seed)
 
 
-def ensemble_specs(n: int = 256, seed: int = 20263, sizes=(128, 256, 512, 1024)) -> list[dict]:
+def ensemble_specs(n: int = 256, seed: int = 20263, sizes=(128, 256, 512, 1024), c_range=(5e3, 5e4)) -> list[dict]:
     """The ragged ensemble: n instances, sizes drawn uniformly from `sizes`; per-instance bed slope
-    U(0.005, 0.02), melt U(1e-9, 1e-7) m/s, C U(5e3, 5e4), initial gap U(0.001, 0.01) m."""
+    U(0.005, 0.02), melt U(1e-9, 1e-7) m/s, C U(c_range) (the described 5e3-5e4 by default),
+    initial gap U(0.001, 0.01) m."""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(n):
         out.append(dict(nx=int(rng.choice(sizes)), seed=seed + 1 + k, slope=float(rng.uniform(0.005, 0.02)),
-                        melt=float(rng.uniform(1e-9, 1e-7)), C=float(rng.uniform(5e3, 5e4)),
+                        melt=float(rng.uniform(1e-9, 1e-7)), C=float(rng.uniform(*c_range)),
                         b0=float(rng.uniform(0.001, 0.01))))
     return out
 

@@ -1265,6 +1265,8 @@ struct BottomPlan {
     const int *done;
 };
 
+// Every loop over a level runs on a 2D thread map (32 columns x blockDim/32 rows), so no cell's
+// coordinates need an integer division; the arithmetic per cell is unchanged.
 __device__ __forceinline__ void mg_bottom_body(const BottomPlan &P, const float *b_top, float *x_top, int nu,
                                                float wc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1272,7 +1274,7 @@ __device__ __forceinline__ void mg_bottom_body(const BottomPlan &P, const float 
     const int T = P.total;
     float *sE = (float *)smem_raw, *sN = sE + T, *sD = sN + T, *sP = sD + T, *sX = sP + T, *sY = sX + T, *sB = sY + T;
     uint8_t *sA = (uint8_t *)(sB + T);
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, tx = tid & 31, ty = tid >> 5, nty = nt >> 5;
     for (int l = 0; l < P.nlev; l++) {
         const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
         for (int i = tid; i < n; i += nt) {
@@ -1285,9 +1287,9 @@ __device__ __forceinline__ void mg_bottom_body(const BottomPlan &P, const float 
         }
     }
     __syncthreads();
-    // (A X)_i on level l (level-local index i)
-    auto Ax = [&](int l, const float *X, int i) -> float {
-        const int nx = P.lv[l].nx, ny = P.lv[l].ny, o = P.lv[l].off, ix = i % nx, iy = i / nx;
+    // (A X)_i on level l at (ix, iy), level-local index i
+    auto Ax = [&](int l, const float *X, int ix, int iy, int i) -> float {
+        const int nx = P.lv[l].nx, ny = P.lv[l].ny, o = P.lv[l].off;
         const float xc = X[o + i];
         float y = sD[o + i] * xc;
         if (ix < nx - 1) y += sE[o + i] * (xc - X[o + i + 1]);
@@ -1303,10 +1305,14 @@ __device__ __forceinline__ void mg_bottom_body(const BottomPlan &P, const float 
     // the coarsest level's exact solve in sX.
     float *Xb[2] = {sX, sY};
     auto sweep = [&](int l, int cur) {
-        const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
+        const int nx = P.lv[l].nx, ny = P.lv[l].ny, o = P.lv[l].off;
         const float *XI = Xb[cur];
         float *XO = Xb[cur ^ 1];
-        for (int i = tid; i < n; i += nt) XO[o + i] = XI[o + i] + sP[o + i] * (sB[o + i] - Ax(l, XI, i));
+        for (int iy = ty; iy < ny; iy += nty)
+            for (int ix = tx; ix < nx; ix += 32) {
+                const int i = ix + iy * nx;
+                XO[o + i] = XI[o + i] + sP[o + i] * (sB[o + i] - Ax(l, XI, ix, iy, i));
+            }
         __syncthreads();
         return cur ^ 1;
     };
@@ -1320,19 +1326,19 @@ __device__ __forceinline__ void mg_bottom_body(const BottomPlan &P, const float 
         for (int s = 1; s < nu; s++) cur = sweep(l, cur);
         const float *XC = Xb[cur];
         const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, nxc = P.lv[l + 1].nx, nyc = P.lv[l + 1].ny, oc = P.lv[l + 1].off;
-        for (int c = tid; c < nxc * nyc; c += nt) {
-            const int I = c % nxc, J = c / nxc;
-            float sres = 0.0f;
-            for (int dj = 0; dj < 2; dj++)
-                for (int di = 0; di < 2; di++) {
-                    const int i = 2 * I + di, j = 2 * J + dj;
-                    if (i >= nxf || j >= nyf) continue;
-                    const int f = i + j * nxf;
-                    if (!sA[o + f]) continue;
-                    sres += sB[o + f] - Ax(l, XC, f);
-                }
-            sB[oc + c] = sres;
-        }
+        for (int J = ty; J < nyc; J += nty)
+            for (int I = tx; I < nxc; I += 32) {
+                float sres = 0.0f;
+                for (int dj = 0; dj < 2; dj++)
+                    for (int di = 0; di < 2; di++) {
+                        const int i = 2 * I + di, j = 2 * J + dj;
+                        if (i >= nxf || j >= nyf) continue;
+                        const int f = i + j * nxf;
+                        if (!sA[o + f]) continue;
+                        sres += sB[o + f] - Ax(l, XC, i, j, f);
+                    }
+                sB[oc + I + J * nxc] = sres;
+            }
         __syncthreads();
     }
     {  // coarsest level: exact solve
@@ -1344,10 +1350,11 @@ __device__ __forceinline__ void mg_bottom_body(const BottomPlan &P, const float 
         const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, o = P.lv[l].off, nxc = P.lv[l + 1].nx, oc = P.lv[l + 1].off;
         float *XF = Xb[cur_down];
         const float *XC = Xb[l + 1 == L - 1 ? 0 : cur_up];
-        for (int f = tid; f < nxf * nyf; f += nt) {
-            const int i = f % nxf, j = f / nxf;
-            if (sA[o + f]) XF[o + f] += wc * XC[oc + (i >> 1) + (j >> 1) * nxc];
-        }
+        for (int j = ty; j < nyf; j += nty)
+            for (int i = tx; i < nxf; i += 32) {
+                const int f = i + j * nxf;
+                if (sA[o + f]) XF[o + f] += wc * XC[oc + (i >> 1) + (j >> 1) * nxc];
+            }
         __syncthreads();
         int cur = cur_down;
         for (int s = 0; s < nu; s++) cur = sweep(l, cur);

@@ -195,30 +195,44 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(const bf16 *__restrict__ X, 
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *slot;
 
-    // this thread's pixels' coordinates are recomputed per segment (each thread stages several rows)
+    // Staging map, fixed for the CTA: thread tid stages 16-byte segment g8 = tid % spr (spr = KC/8
+    // segments per row) of rows tid / spr + k * (128 / spr), k < spr, of A (pixels) and the same of
+    // B (output channels), so the pixel coordinates are computed once, not per chunk.
+    const int spr = KC / 8, g8 = tid % spr, r0 = tid / spr, rstep = kTcM / spr;
+    const uint32_t soff = (uint32_t)((g8 >> 1) * (kTcM * 32) + (g8 & 1) * 128);  // A segment offset in a row group
+    const uint32_t boff = (uint32_t)((g8 >> 1) * (NT * 32) + (g8 & 1) * 128);
+    int py[4], px[4];
+    long long pbase[4];  // element offset of the pixel's channel 0 (n, y, x unshifted), -1 past P
+    for (int k = 0; k < spr; k++) {
+        const long long p = p0 + r0 + k * rstep;
+        py[k] = px[k] = 0;
+        pbase[k] = -1;
+        if (p < P) {
+            const long long hw = (long long)H * W;
+            const int n = (int)(p / hw), rem = (int)(p % hw);
+            py[k] = rem / W;
+            px[k] = rem % W;
+            pbase[k] = (((long long)n * H + py[k]) * W + px[k]) * Cin;
+        }
+    }
     auto stage_chunk = [&](int c, int st) {
         const int tap = c / per_tap, c0 = (c % per_tap) * KC;
         int dy = tap / 3 - 1, dx = tap % 3 - 1;
         if (flip) { dy = -dy; dx = -dx; }
+        const long long shift = ((long long)dy * W + dx) * Cin + c0 + g8 * 8;
         unsigned char *A = sm + st * Lay::stage, *B = A + Lay::a;
-        const int segs_row = KC / 8;
-        for (int q = tid; q < kTcM * segs_row; q += blockDim.x) {
-            const int r = q / segs_row, g8 = q % segs_row, j = g8 >> 1, kh = g8 & 1;
-            const long long p = p0 + r;
+        for (int k = 0; k < spr; k++) {
+            const int r = r0 + k * rstep, y = py[k] + dy, x = px[k] + dx;
             uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (p < P) {
-                const long long hw = (long long)H * W;
-                const int n = (int)(p / hw), rem = (int)(p % hw), y = rem / W + dy, x = rem % W + dx;
-                if (y >= 0 && y < H && x >= 0 && x < W)
-                    v = *reinterpret_cast<const uint4 *>(X + (((long long)n * H + y) * W + x) * Cin + c0 + g8 * 8);
-            }
-            *reinterpret_cast<uint4 *>(A + j * (kTcM * 32) + (r >> 3) * 256 + kh * 128 + (r & 7) * 16) = v;
+            if (pbase[k] >= 0 && y >= 0 && y < H && x >= 0 && x < W)
+                v = *reinterpret_cast<const uint4 *>(X + pbase[k] + shift);
+            *reinterpret_cast<uint4 *>(A + soff + (r >> 3) * 256 + (r & 7) * 16) = v;
         }
-        for (int q = tid; q < NT * segs_row; q += blockDim.x) {
-            const int r = q / segs_row, g8 = q % segs_row, j = g8 >> 1, kh = g8 & 1;
+        const bf16 *wrow = Wt + (long long)tap * Cout * Cin + c0 + g8 * 8;
+        for (int r = r0; r < NT; r += rstep) {
             uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (r < Cout) v = *reinterpret_cast<const uint4 *>(Wt + ((long long)tap * Cout + r) * Cin + c0 + g8 * 8);
-            *reinterpret_cast<uint4 *>(B + j * (NT * 32) + (r >> 3) * 256 + kh * 128 + (r & 7) * 16) = v;
+            if (r < Cout) v = *reinterpret_cast<const uint4 *>(wrow + (long long)r * Cin);
+            *reinterpret_cast<uint4 *>(B + boff + (r >> 3) * 256 + (r & 7) * 16) = v;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
     };
