@@ -401,25 +401,31 @@ __device__ __forceinline__ void assemble_body(Blk B, int nx, int ny, const Param
         T.cell(t, ix, iy);
         if (ix >= nx || iy >= ny) continue;
         const size_t c = CI(ix, iy);
+        // every input is loaded before the first branch, so that the loads are in flight together
+        // (the Dirichlet and OTHER_BASIN rows use few of them)
+        const bool hE = ix < nx - 1, hW = ix > 0, hN = iy < ny - 1, hS = iy > 0;
         const uint8_t m = m8[c];
-        const double h = s.h[c];
+        const uint8_t mE = hE ? m8[c + 1] : 0, mW = hW ? m8[c - 1] : 0, mN = hN ? m8[c + nx] : 0,
+                      mS = hS ? m8[c - nx] : 0;
+        const double h = s.h[c], zb = s.zb[c], K = s.K[c];
+        const double KE = hE ? s.K[c + 1] : 0.0, KW = hW ? s.K[c - 1] : 0.0, KN = hN ? s.K[c + nx] : 0.0,
+                     KS = hS ? s.K[c - nx] : 0.0;
+        const double Nc = s.N[c], A = s.A_visc[c], b = s.b[c], mdot = s.mdot[c], beta = s.beta[c],
+                     aub = s.abs_ub[c], ieb = s.ieb[c];
         if (h_prev) h_prev[c] = h;
         double oP, oE = 0.0, oN = 0.0, orhs;
         if (is_dirichlet(m)) {
             oP = 1;
-            orhs = dirichlet_head(P, m, s.zb[c]);
+            orhs = dirichlet_head(P, m, zb);
         } else if (m == M_OTHER) {
             oP = 1;
             orhs = h;
         } else {
-            const double K = s.K[c];
             double eE = 0.0, eW = 0.0, eN = 0.0, eS = 0.0;
-            uint8_t mE = 0, mW = 0, mN = 0, mS = 0;
-            if (ix < nx - 1) { mE = m8[c + 1]; eE = bK(kfs, K, s.K[c + 1], mE) / P.dx2; }
-            if (ix > 0) { mW = m8[c - 1]; eW = bK(kfs, K, s.K[c - 1], mW) / P.dx2; }
-            if (iy < ny - 1) { mN = m8[c + nx]; eN = bK(kfs, K, s.K[c + nx], mN) / P.dy2; }
-            if (iy > 0) { mS = m8[c - nx]; eS = bK(kfs, K, s.K[c - nx], mS) / P.dy2; }
-            const double Nc = s.N[c], A = s.A_visc[c], b = s.b[c];
+            if (hE) eE = bK(kfs, K, KE, mE) / P.dx2;
+            if (hW) eW = bK(kfs, K, KW, mW) / P.dx2;
+            if (hN) eN = bK(kfs, K, KN, mN) / P.dy2;
+            if (hS) eS = bK(kfs, K, KS, mS) / P.dy2;
             const double Nn = jl_pow(fabs(Nc), P.nm1, P.nm1_int);
             if (PARABOLIC) oP = (eE + eW + eN + eS) + P.e_v / dt;
             else oP = (eE + eW + eN + eS) + P.n * P.rho_w * P.g * A * Nn * b;
@@ -435,11 +441,11 @@ __device__ __forceinline__ void assemble_body(Blk B, int nx, int ny, const Param
             }
             if (iy > 0 && is_dirichlet(mS)) drhs += eS * dirichlet_head(P, mS, s.zb[c - nx]);
             if (PARABOLIC)
-                orhs = s.mdot[c] * (1 / P.rho_w - 1 / P.rho_i) - s.beta[c] * s.abs_ub[c] + A * Nn * Nc * b +
-                       s.ieb[c] + (P.e_v / dt) * h + drhs;
+                orhs = mdot * (1 / P.rho_w - 1 / P.rho_i) - beta * aub + A * Nn * Nc * b + ieb + (P.e_v / dt) * h +
+                       drhs;
             else
-                orhs = s.mdot[c] * (1 / P.rho_w - 1 / P.rho_i) - s.beta[c] * s.abs_ub[c] + A * Nn * Nc * b +
-                       A * Nn * (P.n * P.rho_w * P.g * h) * b + s.ieb[c] + drhs;
+                orhs = mdot * (1 / P.rho_w - 1 / P.rho_i) - beta * aub + A * Nn * Nc * b +
+                       A * Nn * (P.n * P.rho_w * P.g * h) * b + ieb + drhs;
         }
         aP[c] = oP;
         aE[c] = oE;

@@ -37,9 +37,11 @@ constexpr int kMaxRedValues = 4;
 // measured fastest at 4096^2: 1310 us per call against 1376 with four, 1485 with six and 1616 with
 // three (no spills): the tail needs warps in flight more than registers.
 constexpr int kTailBlocksPerSm = 5;
-// Resident blocks per SM of the assembly kernel (256 threads): five measured fastest at 4096^2
-// (494 us per call against 553 with four, 565 with six, 600 with seven and 605 with eight).
-constexpr int kAsmBlocksPerSm = 5;
+// Resident blocks per SM of the assembly kernel (256 threads).  With every input loaded before the
+// cell's first branch (64 registers), four measured fastest at 4096^2: 406 us per call against
+// 419 with five (which spills); with the loads inside the branches, five had been fastest at
+// 494-507 us (553 with four, 565 with six, 600 with seven, 605 with eight).
+constexpr int kAsmBlocksPerSm = 4;
 constexpr int kMarchX = 128;        // columns per block of the row-marching stencil kernels
 constexpr int kUnrollB = 2;         // 16-byte vectors in flight per thread in streaming kernels
 constexpr int kRingRows = 6;        // shared-memory ring depth of the row-marching kernels

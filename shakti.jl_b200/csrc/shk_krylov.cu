@@ -989,8 +989,6 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
             cudaGraphExec_t exec = nullptr;
             long long per_trip = -1;
             cudaGraphConditionalHandle handle;
-            if (getenv("SHK_MG_CARVEOUT") && atoi(getenv("SHK_MG_CARVEOUT")) != 0)  // see shk_mg.cu
-                cudaFuncSetAttribute(k_cg_loop_cond, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess &&
                       cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
             if (ok) {

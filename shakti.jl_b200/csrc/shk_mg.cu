@@ -1428,14 +1428,6 @@ static size_t bottom_plan(const Ctx *c, int lb, BottomPlan *P) {
 struct MgTma;
 static MgTma *tma_maps(Ctx *c, int *rc);
 
-// SHK_MG_CARVEOUT=1: every kernel of the CG iteration asks for the largest shared-memory carveout,
-// so consecutive kernels never make the SMs switch their L1 / shared-memory split.
-static bool max_carveout() {
-    static const bool on = getenv("SHK_MG_CARVEOUT") && atoi(getenv("SHK_MG_CARVEOUT")) != 0;
-    return on;
-}
-
-
 // Rebuilds every level's operator from the assembled Float64 system (after k_to_float_lapl).
 int mg_setup(Ctx *c) {
     if (c->mg_levels < 1) return fail(c, SHK_CUDA_ERROR, "multigrid hierarchy not allocated");
@@ -1472,8 +1464,6 @@ int mg_setup(Ctx *c) {
         if (!attr_set[c->device]) {
             cudaError_t e = cudaFuncSetAttribute(k_mg_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)kBottomBytes);
-            if (e == cudaSuccess && max_carveout())
-                e = cudaFuncSetAttribute(k_mg_bottom, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             if (e != cudaSuccess) return check_cuda(c, e, "multigrid bottom shared memory");
             attr_set[c->device] = true;
         }
@@ -1520,10 +1510,6 @@ template <typename K>
 static int tma_kernel_bps(Ctx *c, K kernel, unsigned smem, int *blocks_per_sm) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return check_cuda(c, e, "multigrid TMA kernel shared memory");
-    if (max_carveout()) {
-        e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e != cudaSuccess) return check_cuda(c, e, "multigrid kernel carveout");
-    }
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, 256, smem);
     if (e != cudaSuccess) return check_cuda(c, e, "multigrid TMA kernel occupancy");
     return SHK_OK;

@@ -8,13 +8,16 @@
 //
 // Tensors are NHWC (channels innermost): activations BF16, gradients Float32, weights BF16 for the
 // tensor cores with a Float32 master copy for the optimiser.  A 3x3 convolution is an implicit
-// GEMM on mma.sync m16n8k16 (BF16 inputs, Float32 accumulation):
+// GEMM (BF16 inputs, Float32 accumulation) on the tcgen05 tensor cores -- by default reading its A
+// operand straight out of TMA-loaded halo tiles, alternatively from per-tap gathered tiles -- or on
+// mma.sync m16n8k16 (the comparison form):
 //   forward      Y[p, co]  = sum_{tap, ci} X[p + off(tap), ci] W[tap, co, ci]        (+ bias, ReLU)
 //   input grad   dX[p, ci] = sum_{tap, co} dY[p - off(tap), co] W[tap, co, ci]       (the forward
 //                kernel on the per-tap transposed weights with the offsets negated)
 //   weight grad  dW[tap, co, ci] = sum_p dY[p, co] X[p + off(tap), ci]                (split over
 //                pixel chunks, Float32 atomics)
 // with zero padding at each image's border.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -317,6 +320,277 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(const bf16 *__restrict__ X, 
 }
 
 // ---------------------------------------------------------------------------------------------
+// 3x3 convolution on halo tiles (tcgen05 + TMA; the default form).  A CTA computes super-tiles of
+// MT x 128 pixels of one image -- 16 rows x 8 MT columns -- for NT output channels; M tile j
+// (columns 8j .. 8j + 7) accumulates in TMEM columns [j NT, (j + 1) NT) of one of ACC buffers.
+// K runs over 16-channel chunks.  A stage holds a chunk's input halo (18 rows x (8 MT + 2) columns,
+// one TMA box per 8-channel group laid out [row][column][8 channels], 16 B per pixel, zero outside
+// the image) and the chunk's weights for all nine taps (one box per group: [tap][co][8 channels]).
+// The MMA of M tile j, tap (dy, dx) reads its A operand straight out of the halo: the descriptor
+// starts at halo pixel (1 + dy, 8j + 1 + dx); a core matrix (8 rows x 16 B) is 8 consecutive pixels
+// of one halo row, consecutive core matrices along M are consecutive rows (SBO = the halo row
+// pitch) and along K the next channel group (LBO = one group's halo): no im2col gather, each input
+// pixel crosses from memory once per super-tile.  B is the tap's NT x 16 slice of the staged
+// weights (SBO = 8 rows, LBO = one group's weights).
+// Warp 4's lane 0 issues the stages' TMA copies (S - 1 stages ahead) and the MMAs; tcgen05.commit
+// frees a stage (empty[]) and, after a super-tile's last chunk, hands the accumulator to warps 0-3
+// (accf[]), which read their 32 TMEM lanes (tcgen05.ld, 16 columns at a time), add the bias, apply
+// ReLU, store BF16 and/or Float32, and give the buffer back (acce[]).  Every wait is bounded; one
+// that runs out sets *err and the CTA winds down: no new copies or MMAs, the copies and MMAs in
+// flight are waited for, TMEM is freed.
+// ---------------------------------------------------------------------------------------------
+constexpr int kHxRows = 16, kHxThreads = 160;
+
+template <int NT>
+struct HxCfg {
+    static constexpr int MT = NT >= 128 ? 2 : 4;                 // M tiles per super-tile
+    static constexpr int ACC = 2 * MT * NT <= 512 ? 2 : 1;       // accumulator buffers
+    static constexpr int HW = 8 * MT + 2, HH = kHxRows + 2;      // halo columns, rows
+    static constexpr uint32_t HB = HH * HW * 16;                 // bytes of one 8-channel halo box
+    static constexpr uint32_t HG = (HB + 127) / 128 * 128;       // its pitch (TMA destinations 128-B aligned)
+    static constexpr uint32_t WG = 9 * NT * 16;                  // one 8-channel group of the weights
+    static constexpr uint32_t stage = 2 * HG + 2 * WG;
+    static constexpr int S = 4 * stage <= 200u * 1024 ? 4 : (3 * stage <= 200u * 1024 ? 3 : 2);
+    static constexpr uint32_t bars = S * stage;                  // full[S], empty[S], accf[ACC], acce[ACC]
+    static constexpr uint32_t misc = bars + 8 * (2 * S + 2 * ACC);  // TMEM address, abort flag
+    static constexpr uint32_t used = misc + 16;
+    // more than half of an SM's shared memory: one CTA per SM, which then owns all 512 TMEM columns
+    static constexpr uint32_t bytes = used > 120u * 1024 ? used : 120u * 1024;
+};
+
+__device__ __forceinline__ void hx_expect(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void hx_load4(void *dst, const CUtensorMap *map, uint64_t *bar, int c, int x, int y, int n) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(su32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c), "r"(x), "r"(y), "r"(n), "r"(su32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void hx_load3(void *dst, const CUtensorMap *map, uint64_t *bar, int c, int o, int t) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(su32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c), "r"(o), "r"(t), "r"(su32(bar))
+        : "memory");
+}
+
+// Bounded wait that also gives up once the CTA's abort flag is set (abort == nullptr: only the bound).
+__device__ __forceinline__ bool hx_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    for (long i = 0; i < kTcSpin; i++) {
+        uint32_t ok;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(ok)
+                     : "r"(su32(bar)), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+        if ((i & 255) == 255 && abort && *abort) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void hx_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t .reg .pred pacc;\n\t setp.ne.b32 pacc, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, pacc;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void hx_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+                 : "memory");
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kHxThreads, 1) k_conv3x3_hx(const __grid_constant__ CUtensorMap mx,
+                                                              const __grid_constant__ CUtensorMap mw,
+                                                              const float *__restrict__ bias, bf16 *__restrict__ Y,
+                                                              float *__restrict__ Yf, int N, int H, int W, int Cin,
+                                                              int Cout, int relu, int flip, int *err) {
+    using Cf = HxCfg<NT>;
+    constexpr int MT = Cf::MT, ACC = Cf::ACC, S = Cf::S;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm + Cf::bars), *empty = full + S, *accf = empty + S,
+             *acce = accf + ACC;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + Cf::misc);
+    volatile int *abort = reinterpret_cast<volatile int *>(sm + Cf::misc + 4);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles_x = (W + 8 * MT - 1) / (8 * MT), tiles_y = (H + kHxRows - 1) / kHxRows;
+    const long long T = (long long)N * tiles_x * tiles_y;
+    const long long G = gridDim.x, b0 = blockIdx.x;
+    const long long my_tiles = b0 < T ? (T - b0 + G - 1) / G : 0;
+    const int nc = Cin / 16;
+    const long long total = my_tiles * nc;  // stages this CTA consumes
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(su32(tslot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 32) {
+        for (int i = 0; i < S; i++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&full[i])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&empty[i])) : "memory");
+        }
+        for (int i = 0; i < ACC; i++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&accf[i])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(su32(&acce[i])) : "memory");
+        }
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tslot;
+
+    auto tile_at = [&](long long ti, int &n, int &y0, int &x0) {
+        const long long t = b0 + ti * G;
+        const long long per = (long long)tiles_x * tiles_y;
+        n = (int)(t / per);
+        const int r = (int)(t % per);
+        y0 = (r / tiles_x) * kHxRows;
+        x0 = (r % tiles_x) * 8 * MT;
+    };
+
+    if (warp == 4) {
+        if (lane == 0 && total > 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mx)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mw)) : "memory");
+            auto load = [&](long long q) {
+                const int slot = (int)(q % S), kc = (int)(q % nc);
+                int n, y0, x0;
+                tile_at(q / nc, n, y0, x0);
+                unsigned char *st = sm + slot * Cf::stage;
+                hx_expect(&full[slot], 2 * (Cf::HB + Cf::WG));
+                for (int g = 0; g < 2; g++) {
+                    hx_load4(st + g * Cf::HG, &mx, &full[slot], kc * 16 + g * 8, x0 - 1, y0 - 1, n);
+                    hx_load3(st + 2 * Cf::HG + g * Cf::WG, &mw, &full[slot], kc * 16 + g * 8, 0, 0);
+                }
+            };
+            constexpr uint32_t idesc = umma_idesc_bf16(kTcM, NT);
+            long long issued = 0, consumed = 0;
+            bool ok = true;
+            for (; issued < total && issued < S - 1; issued++) load(issued);
+            for (long long q = 0; q < total && ok; q++) {
+                const int slot = (int)(q % S), kc = (int)(q % nc);
+                const long long ti = q / nc;
+                const int buf = (int)(ti % ACC);
+                ok = hx_wait(&full[slot], (uint32_t)((q / S) & 1), abort);
+                if (ok && kc == 0 && ti >= ACC) ok = hx_wait(&acce[buf], (uint32_t)((ti / ACC - 1) & 1), abort);
+                if (!ok) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t st = su32(sm + slot * Cf::stage), wt = st + 2 * Cf::HG;
+#pragma unroll 1
+                for (int t = 0; t < 9; t++) {
+                    int dy = t / 3 - 1, dx = t % 3 - 1;
+                    if (flip) { dy = -dy; dx = -dx; }
+                    const uint64_t db = umma_desc(wt + (uint32_t)(t * NT * 16), Cf::WG, 128);
+#pragma unroll
+                    for (int j = 0; j < MT; j++) {
+                        const uint32_t a = st + (uint32_t)(((1 + dy) * Cf::HW + 8 * j + 1 + dx) * 16);
+                        const uint64_t da = umma_desc(a, Cf::HG, Cf::HW * 16);
+                        hx_mma(tmem + (uint32_t)((buf * MT + j) * NT), da, db, idesc, (kc > 0 || t > 0) ? 1u : 0u);
+                    }
+                }
+                hx_commit(&empty[slot]);
+                if (kc == nc - 1) hx_commit(&accf[buf]);
+                consumed = q + 1;
+                // refill the stage that chunk q - 1 used, once its MMAs (queued before this chunk's) finish
+                if (issued < total) {
+                    const int rs = (int)(issued % S);
+                    if (issued >= S) ok = hx_wait(&empty[rs], (uint32_t)((issued / S - 1) & 1), abort);
+                    if (ok) load(issued++);
+                }
+            }
+            if (!ok) {
+                atomicExch(err, 1);
+                *abort = 1;
+            }
+            // wind down: every copy issued has landed and every MMA committed has finished
+            for (long long q = consumed; q < issued; q++) hx_wait(&full[q % S], (uint32_t)((q / S) & 1), nullptr);
+            if (consumed > 0) {
+                const long long q = consumed - 1;
+                if (!hx_wait(&empty[q % S], (uint32_t)((q / S) & 1), nullptr)) atomicExch(err, 1);
+            }
+        }
+    } else {
+        // epilogue: warp w holds TMEM lanes 32w .. 32w + 31, the super-tile rows 4w .. 4w + 3
+        const int m = warp * 32 + lane, r = m >> 3, cpx = m & 7;
+        for (long long ti = 0; ti < my_tiles; ti++) {
+            const int buf = (int)(ti % ACC);
+            const bool ok = hx_wait(&accf[buf], (uint32_t)((ti / ACC) & 1), abort);
+            if (!__all_sync(0xffffffffu, ok)) {  // the warp leaves together (tcgen05.ld is warp-collective)
+                if (lane == 0) {
+                    atomicExch(err, 1);
+                    *abort = 1;
+                }
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            int n, y0, x0;
+            tile_at(ti, n, y0, x0);
+            const int y = y0 + r;
+#pragma unroll 1
+            for (int j = 0; j < MT; j++) {
+                const int x = x0 + 8 * j + cpx;
+                const bool valid = y < H && x < W;
+                const long long p = ((long long)n * H + y) * W + x;
+#pragma unroll 1
+                for (int cb = 0; cb < NT; cb += 16) {
+                    uint32_t v[16];
+                    const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((buf * MT + j) * NT + cb);
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                        "%12, %13, %14, %15}, [%16];"
+                        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                          "=r"(v[14]), "=r"(v[15])
+                        : "r"(taddr));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    if (!valid || cb >= Cout) continue;
+                    const int nv = Cout - cb >= 16 ? 16 : 8;  // Cout % 8 == 0
+                    float o[16];
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        o[k] = __uint_as_float(v[k]) + (bias && k < nv ? bias[cb + k] : 0.0f);
+                        if (relu) o[k] = o[k] > 0.0f ? o[k] : 0.0f;
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        if (h * 8 >= nv) break;
+                        const float *q8 = o + 8 * h;
+                        if (Y) {
+                            const uint4 pk = make_uint4(pack2(__float2bfloat16(q8[0]), __float2bfloat16(q8[1])),
+                                                        pack2(__float2bfloat16(q8[2]), __float2bfloat16(q8[3])),
+                                                        pack2(__float2bfloat16(q8[4]), __float2bfloat16(q8[5])),
+                                                        pack2(__float2bfloat16(q8[6]), __float2bfloat16(q8[7])));
+                            *reinterpret_cast<uint4 *>(Y + p * Cout + cb + 8 * h) = pk;
+                        }
+                        if (Yf) {
+                            *reinterpret_cast<float4 *>(Yf + p * Cout + cb + 8 * h) =
+                                make_float4(q8[0], q8[1], q8[2], q8[3]);
+                            *reinterpret_cast<float4 *>(Yf + p * Cout + cb + 8 * h + 4) =
+                                make_float4(q8[4], q8[5], q8[6], q8[7]);
+                        }
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(&acce[buf])) : "memory");
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
+// ---------------------------------------------------------------------------------------------
 // Weight gradient dW[tap, co, ci] += sum over a chunk of pixels of dY[p, co] X[p + off(tap), ci].
 // GEMM M = co (16 per block), N = ci (64 per block, 16 per warp), K = pixels (16 per step).  The
 // fragments gather pixel pairs (NHWC keeps channels, not pixels, contiguous), so they are built
@@ -601,8 +875,72 @@ static int launch_conv_tc(const bf16 *x, const bf16 *w, const float *bias, bf16 
     return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
 }
 
-// tcgen05 form (default): N tile = Cout rounded up to 16 (<= 256).  SHK_NN_MMA_SYNC=1 selects the
-// mma.sync form (kept as the comparison for the tensor-core form's tests).
+typedef CUresult (*HxEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                               const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static HxEncodeFn hx_encoder() {
+    static HxEncodeFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *fp = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fp, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess && fp)
+            fn = (HxEncodeFn)fp;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// The halo-tile form; *launched = false (and SHK_OK) when its tensor maps cannot be built here.
+template <int NT>
+static int launch_conv_hx(const bf16 *x, const bf16 *w, const float *bias, bf16 *y, float *Yf, int N, int H, int W,
+                          int Cin, int Cout, int relu, int flip, cudaStream_t s, bool *launched) {
+    using Cf = HxCfg<NT>;
+    *launched = false;
+    const HxEncodeFn fn = hx_encoder();
+    if (!fn || (uintptr_t)x % 16 || (uintptr_t)w % 16) return SHK_OK;
+    static int attr_done[64] = {}, sms[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return SHK_BAD_ARG;
+    int *fault = nullptr;
+    if (int rc = tc_fault_word(dev, &fault)) return rc;
+    if (!attr_done[dev]) {
+        if (cudaFuncSetAttribute(k_conv3x3_hx<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cf::bytes) !=
+                cudaSuccess ||
+            cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return SHK_CUDA_ERROR;
+        attr_done[dev] = 1;
+    }
+    CUtensorMap mx, mw;
+    const cuuint64_t xd[4] = {(cuuint64_t)Cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+    const cuuint64_t xs[3] = {(cuuint64_t)Cin * 2, (cuuint64_t)W * Cin * 2, (cuuint64_t)H * W * Cin * 2};
+    const cuuint32_t xb[4] = {8, (cuuint32_t)Cf::HW, (cuuint32_t)Cf::HH, 1}, e4[4] = {1, 1, 1, 1};
+    const cuuint64_t wd[3] = {(cuuint64_t)Cin, (cuuint64_t)Cout, 9};
+    const cuuint64_t ws[2] = {(cuuint64_t)Cin * 2, (cuuint64_t)Cout * Cin * 2};
+    const cuuint32_t wb[3] = {8, (cuuint32_t)NT, 9};
+    if (fn(&mx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(x), xd, xs, xb, e4,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+        fn(&mw, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16 *>(w), wd, ws, wb, e4,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return SHK_OK;
+    const long long tiles = (long long)N * ((W + 8 * Cf::MT - 1) / (8 * Cf::MT)) * ((H + kHxRows - 1) / kHxRows);
+    const int grid = (int)(tiles < sms[dev] ? tiles : sms[dev]);
+    k_conv3x3_hx<NT><<<grid, kHxThreads, Cf::bytes, s>>>(mx, mw, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, fault);
+    *launched = true;
+    return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
+}
+
+// Forms: the halo-tile tcgen05 kernel (default); SHK_NN_TC_GATHER=1 the tcgen05 kernel that gathers
+// each tap's A tile (also the form used when tensor maps are unavailable); SHK_NN_MMA_SYNC=1 the
+// mma.sync kernel (kept as the comparison for the tensor-core forms' tests).  The variables are read
+// at every call.  N tile = Cout rounded up to 16 (<= 256).
 extern "C" {
 
 SHK_API int shk_nn_conv3x3(const void *X, const void *Wt, const float *bias, void *Y, float *Yf, int N, int H, int W,
@@ -612,7 +950,19 @@ SHK_API int shk_nn_conv3x3(const void *X, const void *Wt, const float *bias, voi
     cudaStream_t s = (cudaStream_t)stream;
     const bf16 *x = (const bf16 *)X, *w = (const bf16 *)Wt;
     bf16 *y = (bf16 *)Y;
-    static const bool legacy = getenv("SHK_NN_MMA_SYNC") && atoi(getenv("SHK_NN_MMA_SYNC")) != 0;
+    const char *e1 = getenv("SHK_NN_MMA_SYNC"), *e2 = getenv("SHK_NN_TC_GATHER");
+    const bool legacy = e1 && atoi(e1) != 0, gather = e2 && atoi(e2) != 0;
+    if (!legacy && !gather && Cout <= 256) {
+        const int nt = (Cout + 15) / 16 * 16;
+        bool launched = false;
+        int rc = SHK_OK;
+        if (nt <= 16) rc = launch_conv_hx<16>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s, &launched);
+        else if (nt <= 32) rc = launch_conv_hx<32>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s, &launched);
+        else if (nt <= 64) rc = launch_conv_hx<64>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s, &launched);
+        else if (nt <= 128) rc = launch_conv_hx<128>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s, &launched);
+        else rc = launch_conv_hx<256>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s, &launched);
+        if (rc || launched) return rc;
+    }
     if (!legacy && Cout <= 256) {
         const int nt = (Cout + 15) / 16 * 16;
         if (nt <= 16) return launch_conv_tc<16>(x, w, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, s);

@@ -3,11 +3,14 @@
  - Each tensor-core kernel against the CPU restatement (oracle/nn_oracle.py) on identical inputs:
    the forward and input-gradient convolutions, the weight gradient, the ReLU/bias gradient, and
    the pooling / upsampling pairs, to Float32 accumulation accuracy.
- - The whole network's loss and every layer's gradients against the oracle.  The oracle rounds to
-   BF16 where the GPU does, but its sums are exact where the tensor cores accumulate in Float32;
-   an activation whose two sums fall on either side of a BF16 rounding boundary then differs by
-   one BF16 step, and those steps multiply through fifteen layers (a few % of a deep layer's
-   gradient), so the bar is direction (cosine >= 0.99) and 15 % in norm.
+ - The whole network's loss and every layer's gradients against the oracle, two ways.  Given the
+   GPU's own stored activations, the oracle's backward pass agrees with the GPU's for every layer
+   within 1 % in norm for the weights (measured <= 0.25 %) and 2 % for the biases.  End to end, the oracle's own
+   forward pass sums exactly where the tensor cores accumulate in Float32, so a stored BF16
+   activation whose two sums straddle a rounding boundary differs by one BF16 step; the stored
+   activations drift apart by 1e-4 .. 3e-3 (relative) over the fifteen layers and the weight
+   gradients, which depend on them through the ReLU masks, by up to ~8 %: that bar is direction
+   (cosine >= 0.99) and 15 % in norm.
  - Training lowers the loss; the seeding falls back to the current head when its residual is not
    smaller (bit-identical timestep), and an accepted warm start lowers the first solve's CG
    iterations.
@@ -37,12 +40,15 @@ def ws(shk, cuda):
 
 
 @pytest.mark.parametrize("ci,co,N,H,W", [(16, 32, 1, 40, 37), (32, 64, 2, 16, 24), (64, 128, 1, 33, 17),
-                                         (128, 256, 1, 20, 20), (32, 8, 1, 13, 11)])
+                                         (128, 256, 1, 20, 20), (32, 8, 1, 13, 11), (256, 128, 2, 35, 70),
+                                         (64, 16, 3, 5, 3)])
 def test_tensor_core_convolution(ws, cuda, monkeypatch, ci, co, N, H, W):
-    """The tcgen05 convolution (128-pixel x Cout tiles, TMEM accumulator): forward with bias and ReLU
-    and the flipped input-gradient form, against the oracle and the mma.sync form; ragged pixel
-    counts, 16-channel chunks (Cin = 16), Cout padded to the 16-wide tile (Cout = 8), the 256-wide
-    tile.  Both tensor-core forms accumulate BF16 products in Float32 (1e-5)."""
+    """The three convolution forms -- tcgen05 on TMA-loaded halo tiles (the default), tcgen05 with
+    per-tap gathered A tiles (SHK_NN_TC_GATHER=1), mma.sync (SHK_NN_MMA_SYNC=1) -- forward with bias
+    and ReLU and the flipped input-gradient form, against the oracle and each other: images whose
+    sides are not multiples of the 16 x 8 M tile, several images, 16-channel input (Cin = 16), Cout
+    padded to the 16-wide N tile (Cout = 8), the 256-wide tile.  All accumulate BF16 products in
+    Float32 (1e-5)."""
     torch = cuda
     net = ws.WarmStartNet(seed=3)
     L, s = net.L, net._s()
@@ -53,9 +59,11 @@ def test_tensor_core_convolution(ws, cuda, monkeypatch, ci, co, N, H, W):
     wb = torch.from_numpy(Wf).cuda().to(torch.bfloat16)
     Xn, Wn = X.float().cpu().numpy(), wb.float().cpu().numpy()
     out = {}
-    for form in ("tc", "mma_sync"):
+    for form in ("tc", "gather", "mma_sync"):
         if form == "mma_sync":
             monkeypatch.setenv("SHK_NN_MMA_SYNC", "1")
+        if form == "gather":
+            monkeypatch.setenv("SHK_NN_TC_GATHER", "1")
         Yf = torch.empty((N, H, W, co), dtype=torch.float32, device="cuda")
         Yb = torch.empty((N, H, W, co), dtype=torch.bfloat16, device="cuda")
         assert L.shk_nn_conv3x3(ws._p(X), ws._p(wb), ws._fp(bias), ws._p(Yb), ws._fp(Yf), N, H, W, ci, co, 1, 0,
@@ -68,16 +76,20 @@ def test_tensor_core_convolution(ws, cuda, monkeypatch, ci, co, N, H, W):
         torch.cuda.synchronize()
         out[form] = (Yf.cpu().numpy(), Yb.float().cpu().numpy(), None if dX is None else dX.cpu().numpy())
         monkeypatch.delenv("SHK_NN_MMA_SYNC", raising=False)
+        monkeypatch.delenv("SHK_NN_TC_GATHER", raising=False)
     fault = C.c_int(-1)
     assert L.shk_nn_conv_fault(C.byref(fault)) == 0 and fault.value == 0
     ref = no.conv3x3(Xn, Wn, bias.cpu().numpy(), relu=True)
     assert rel(out["tc"][0], ref) < 1e-5
     assert rel(out["tc"][0], out["mma_sync"][0]) < 1e-5
+    assert rel(out["gather"][0], ref) < 1e-5 and rel(out["mma_sync"][0], ref) < 1e-5
     assert np.array_equal(out["tc"][1], no.bf16(out["tc"][0]))  # the BF16 output is the rounded Float32 one
     if out["tc"][2] is not None:
-        ref_dx = no.conv3x3(out["tc"][1], Wn.transpose(0, 2, 1), None, flip=True)
-        assert rel(out["tc"][2], ref_dx) < 1e-5
-        assert rel(out["tc"][2], out["mma_sync"][2]) < 1e-5
+        # each form's input gradient from its own BF16 forward output (the forms' outputs may differ
+        # by one BF16 step where their Float32 sums straddle a rounding boundary)
+        for form, (_, yb, dx) in out.items():
+            ref_dx = no.conv3x3(yb, Wn.transpose(0, 2, 1), None, flip=True)
+            assert rel(dx, ref_dx) < 1e-5, form
 
 
 def test_kernels_match_oracle(ws, cuda):
@@ -142,12 +154,22 @@ def test_network_gradients_match_oracle(ws, cuda):
     Y, A = no.forward(params, None, X.float().cpu().numpy())
     lref, G = no.backward(params, A, Y, Tn, None)
     assert abs(loss - lref) <= 1e-3 * abs(lref)
+    # the oracle's backward pass fed the GPU's own stored activations and head output
+    Ag = {k: v.float().cpu().numpy() for k, v in net._acts.items()}
+    _, Gg = no.backward(params, Ag, net._bufs["y"].cpu().numpy(), Tn, None)
+    report = {}
     for name, *_ in ws.LAYERS:
         gw = net.P[name]["gw"].cpu().numpy().ravel()
+        gb = net.P[name]["gb"].cpu().numpy()
         rw = G[name][0].ravel()
         cos = float(gw @ rw / (np.linalg.norm(gw) * np.linalg.norm(rw)))
+        report[name] = (round(rel(gw, rw), 5), round(rel(gw, Gg[name][0].ravel()), 6))
         assert cos >= 0.99 and rel(gw, rw) <= 0.15, (name, cos, rel(gw, rw))
-        assert rel(net.P[name]["gb"].cpu().numpy(), G[name][1]) <= 0.15, name
+        assert rel(gb, G[name][1]) <= 0.15, name
+        assert rel(gw, Gg[name][0].ravel()) <= 0.01 and rel(gb, Gg[name][1]) <= 0.02, (name, report[name])
+    print("weight-gradient rel. error per layer (end to end, given the GPU's activations):", report)
+    print("stored activations, rel. error vs the oracle's forward pass:",
+          {k: round(rel(Ag[k], A[k]), 6) for k in A})
 
 
 def test_training_lowers_the_loss(ws, cuda):
@@ -230,6 +252,9 @@ def test_trained_network_gain_is_measured(shk, ws, cuda):
     print("warm-start gain:", {k: (unseeded[k], seeded[k]) for k in ("cg_per_step", "picard_per_step")},
           "accepted", seeded["seed"]["seeded"], "r_seed/r_prev",
           [round(b / a, 2) for a, b in zip(seeded["seed"]["r_prev"], seeded["seed"]["r_seed"])])
+    # the evaluation is only meaningful where Picard converges (this instance: 9-15 iterations a step)
+    for r in unseeded["per_step"] + seeded["per_step"]:
+        assert r["converged"] and r["picard"] < 500, r
     for u, s_, used in zip(unseeded["per_step"], seeded["per_step"], seeded["seed"]["seeded"]):
         if not used:
             assert s_["cg"] == u["cg"] and s_["picard"] == u["picard"]
