@@ -212,6 +212,9 @@ SHK_API int shk_create(int nx, int ny, double lx, double ly, void *stream, void 
     if (const char *v = getenv("SHK_MG_OMEGA_C")) c->mg_omega_c = (float)atof(v);
     if (const char *v = getenv("SHK_MG_FUSED")) c->mg_fused = std::min(2, std::max(0, atoi(v)));
     if (const char *v = getenv("SHK_MG_TMA")) c->mg_tma = atoi(v) != 0;
+    // SHK_MG_CLUSTER=1: the coarse levels from the finest one whose row slabs fit eight CTAs' shared
+    // memory run on one thread-block cluster (default: tile kernels down to the one-block bottom)
+    if (const char *v = getenv("SHK_MG_CLUSTER")) c->mg_cluster = atoi(v) != 0;
     // SHK_CG_GRAPHS: 0 issues each CG iteration's kernels directly, 1 replays one CUDA graph per
     // iteration in host-sized batches, 2 (default) runs the whole iteration loop as one graph with a
     // device-side WHILE node

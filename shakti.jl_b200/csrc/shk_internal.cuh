@@ -150,6 +150,7 @@ struct Ctx {
     float mg_omega_c = 1.6f;
     int mg_fused = 1;        // nu = 2 level kernels: 1 tile (default), 2 warp-marching, 0 per-sweep
     int mg_tma = 1;          // tile kernels stage through TMA copies where the level's pitch allows
+    bool mg_cluster = false;  // the coarse levels on one thread-block cluster (measured slower; opt-in)
     struct MgTma *mg_maps = nullptr;  // the levels' tensor maps (built on first use)
     int max_blocks = 0;
     int grid_stencil = 0;    // blocks for tile-stride kernels

@@ -1369,6 +1369,297 @@ __global__ void __launch_bounds__(1024) k_mg_bottom(BottomPlan P, const float *b
 }
 
 // ---------------------------------------------------------------------------------------------
+// The coarse levels on one thread-block cluster (kClusterCtas CTAs of 1024 threads).  The levels
+// from lc (the finest level whose slabs fit the CTAs' shared memory) down to the last one with more
+// than kCta0Cells cells are "distributed": CTA k holds rows [rows0[k], rows0[k+1]) << (ndist - l) of
+// level l in its shared memory (the partition of the first CTA-0 level doubled level by level, so a
+// coarse row and the two fine rows it aggregates live in the same CTA) and reads the one row above
+// and below its slab from the neighbouring CTAs' shared memory (ld.shared::cluster).  The levels
+// from there on are small and live in CTA 0 alone, which runs the one-block bottom solve on them
+// while the other CTAs wait.  The V-cycle and its arithmetic are mg_bottom_body's: first sweep from
+// zero, nu - 1 more, residual restricted by 2 x 2 sums, exact coarsest solve, prolongation scaled by
+// wc, nu sweeps -- so the cluster kernel and the one-block kernel produce the same V-cycle.
+// Synchronisation between phases: the hardware cluster barrier (cl_sync), the same sequence of
+// barriers in every CTA.  Measured at 4096^2 (one multigrid CG iteration): 584 us against 580 us
+// for the tile kernels down to the one-block bottom kernel, so this form is opt-in
+// (SHK_MG_CLUSTER=1); with barriers built on mbarriers (bounded polling) it took 597-609 us.
+// ---------------------------------------------------------------------------------------------
+constexpr int kClusterCtas = 8, kClusterThreads = 1024;
+constexpr long long kCta0Cells = 1024;           // levels at most this size are solved by CTA 0
+constexpr size_t kClusterBytes = 200 * 1024;     // dynamic shared memory per CTA
+constexpr size_t kClusterBytesPerCell = 7 * sizeof(float) + 1;
+
+struct ClusterPlan {
+    int nlev, ndist, total;          // levels lc .. lc + nlev - 1 (kernel-local 0 .. nlev - 1)
+    int rows0[kClusterCtas + 1];     // rows of level ndist per CTA (the distributed levels: doubled)
+    int slot_rows[kMgMaxLevels];     // distributed level: rows of every CTA's slot (+ 1 south halo row)
+    BottomLevel lv[kMgMaxLevels];    // nx, ny, off (the level's offset in every CTA's arrays)
+    const float *aE[kMgMaxLevels], *aN[kMgMaxLevels], *dP[kMgMaxLevels], *wD[kMgMaxLevels];
+    const uint8_t *act[kMgMaxLevels];
+    const int *done;
+};
+
+__device__ __forceinline__ uint32_t cl_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cl_map(const void *p, uint32_t rank) {
+    uint32_t a;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(su32(p)), "r"(rank));
+    return a;
+}
+__device__ __forceinline__ float cl_ld(const float *p, uint32_t rank) {
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(cl_map(p, rank)) : "memory");
+    return v;
+}
+__device__ __forceinline__ void cl_st(float *p, uint32_t rank, float v) {
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(cl_map(p, rank)), "f"(v) : "memory");
+}
+
+// Cluster barrier: the hardware barrier.cluster (release/acquire at cluster scope for every thread's
+// shared-memory stores and remote loads).  Like __syncthreads it waits for threads, not for a value
+// in memory: the cluster's CTAs are resident together and all take the same barriers.
+__device__ __forceinline__ void cl_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterPlan P, const float *b_top, float *x_top,
+                                                                   int nu, float wc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t rank = cl_rank();
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5, nty = kClusterThreads >> 5;
+    if (cg_finished(P.done)) return;  // the same flag in every CTA: all return, no remote access made
+    const int T = P.total, L = P.nlev, ND = P.ndist;
+    float *sE = (float *)smem_raw, *sN = sE + T, *sD = sN + T, *sP = sD + T, *sX = sP + T, *sY = sX + T, *sB = sY + T;
+    uint8_t *sA = (uint8_t *)(sB + T);
+    float *Xb[2] = {sX, sY};
+    // rows of CTA k on distributed level l
+    auto rows = [&](int l, int k, int &s, int &e) {
+        const int sh = ND - l, ny = P.lv[l].ny;
+        s = min(P.rows0[k] << sh, ny);
+        e = min(P.rows0[k + 1] << sh, ny);
+    };
+    // the nearest CTAs below and above with rows (the same on every distributed level)
+    int south = -1, north = -1;
+    for (int k = (int)rank - 1; k >= 0 && south < 0; k--)
+        if (P.rows0[k] < P.rows0[k + 1]) south = k;
+    for (int k = (int)rank + 1; k < kClusterCtas && north < 0; k++)
+        if (P.rows0[k] < P.rows0[k + 1]) north = k;
+    // slot index of (ix, iy) on distributed level l in the arrays of a CTA whose rows start at s
+    auto at = [&](int l, int s, int ix, int iy) { return P.lv[l].off + (iy - s + 1) * P.lv[l].nx + ix; };
+    int s0, e0;
+    rows(0, rank, s0, e0);
+    // operators of this CTA's slabs (and the south halo row's north coupling), the top rhs
+    for (int l = 0; l < ND; l++) {
+        int s, e;
+        rows(l, rank, s, e);
+        const int nx = P.lv[l].nx, lo = s > 0 ? s - 1 : s;
+        for (int iy = lo + ty; iy < e; iy += nty)
+            for (int ix = tx; ix < nx; ix += 32) {
+                const int g = ix + iy * nx, i = at(l, s, ix, iy);
+                sN[i] = P.aN[l][g];
+                if (iy < s) continue;
+                sE[i] = P.aE[l][g];
+                sD[i] = P.dP[l][g];
+                sP[i] = P.wD[l][g];
+                sA[i] = P.act[l][g];
+                if (l == 0) sB[i] = b_top[g];
+            }
+    }
+    if (rank == 0)
+        for (int l = ND; l < L; l++) {
+            const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
+            for (int i = tid; i < n; i += kClusterThreads) {
+                sE[o + i] = P.aE[l][i];
+                sN[o + i] = P.aN[l][i];
+                sD[o + i] = P.dP[l][i];
+                sP[o + i] = P.wD[l][i];
+                sA[o + i] = P.act[l][i];
+            }
+        }
+    __syncthreads();
+    // (A X)_i on distributed level l at (ix, iy), slot index i, rows [s, e) of this CTA
+    auto Axd = [&](int l, const float *X, int ix, int iy, int i, int s, int e) -> float {
+        const int nx = P.lv[l].nx, ny = P.lv[l].ny;
+        const float xc = X[i];
+        float y = sD[i] * xc;
+        if (ix < nx - 1) y += sE[i] * (xc - X[i + 1]);
+        if (ix > 0) y += sE[i - 1] * (xc - X[i - 1]);
+        if (iy < ny - 1) {
+            float xn;
+            if (iy + 1 < e) xn = X[i + nx];
+            else {
+                int sn, en;
+                rows(l, north, sn, en);
+                xn = cl_ld(X + at(l, sn, ix, iy + 1), north);
+            }
+            y += sN[i] * (xc - xn);
+        }
+        if (iy > 0) {
+            float xs;
+            if (iy - 1 >= s) xs = X[i - nx];
+            else {
+                int ss, es;
+                rows(l, south, ss, es);
+                xs = cl_ld(X + at(l, ss, ix, iy - 1), south);
+            }
+            y += sN[i - nx] * (xc - xs);
+        }
+        return y;
+    };
+    auto sweep_d = [&](int l, int cur) {
+        int s, e;
+        rows(l, rank, s, e);
+        const int nx = P.lv[l].nx;
+        const float *XI = Xb[cur];
+        float *XO = Xb[cur ^ 1];
+        for (int iy = s + ty; iy < e; iy += nty)
+            for (int ix = tx; ix < nx; ix += 32) {
+                const int i = at(l, s, ix, iy);
+                XO[i] = XI[i] + sP[i] * (sB[i] - Axd(l, XI, ix, iy, i, s, e));
+            }
+        cl_sync();
+        return cur ^ 1;
+    };
+    const int cur_down = (nu - 1) & 1, cur_up = 1;
+    for (int l = 0; l < ND; l++) {  // descend on the distributed levels
+        int s, e;
+        rows(l, rank, s, e);
+        const int nx = P.lv[l].nx, ny = P.lv[l].ny;
+        for (int iy = s + ty; iy < e; iy += nty)
+            for (int ix = tx; ix < nx; ix += 32) {
+                const int i = at(l, s, ix, iy);
+                sX[i] = sP[i] * sB[i];
+            }
+        cl_sync();
+        int cur = 0;
+        for (int k = 1; k < nu; k++) cur = sweep_d(l, cur);
+        const float *XC = Xb[cur];
+        const int nxc = P.lv[l + 1].nx, nyc = P.lv[l + 1].ny;
+        int cs, ce;
+        if (l + 1 < ND) rows(l + 1, rank, cs, ce);
+        else {
+            cs = P.rows0[rank];
+            ce = P.rows0[rank + 1];
+        }
+        for (int J = cs + ty; J < ce; J += nty)
+            for (int I = tx; I < nxc; I += 32) {
+                float sres = 0.0f;
+                for (int dj = 0; dj < 2; dj++)
+                    for (int di = 0; di < 2; di++) {
+                        const int i = 2 * I + di, j = 2 * J + dj;
+                        if (i >= nx || j >= ny) continue;
+                        const int f = at(l, s, i, j);
+                        if (!sA[f]) continue;
+                        sres += sB[f] - Axd(l, XC, i, j, f, s, e);
+                    }
+                if (l + 1 < ND) sB[at(l + 1, cs, I, J)] = sres;
+                else if (rank == 0) sB[P.lv[l + 1].off + I + J * nxc] = sres;
+                else cl_st(sB + P.lv[l + 1].off + I + J * nxc, 0, sres);
+            }
+        (void)nyc;
+        if (l + 1 < ND) __syncthreads();
+        else cl_sync();
+    }
+    if (rank == 0) {  // the small levels: the one-block bottom solve in CTA 0
+        auto Ax = [&](int l, const float *X, int ix, int iy, int i) -> float {
+            const int nx = P.lv[l].nx, ny = P.lv[l].ny, o = P.lv[l].off;
+            const float xc = X[o + i];
+            float y = sD[o + i] * xc;
+            if (ix < nx - 1) y += sE[o + i] * (xc - X[o + i + 1]);
+            if (ix > 0) y += sE[o + i - 1] * (xc - X[o + i - 1]);
+            if (iy < ny - 1) y += sN[o + i] * (xc - X[o + i + nx]);
+            if (iy > 0) y += sN[o + i - nx] * (xc - X[o + i - nx]);
+            return y;
+        };
+        auto sweep = [&](int l, int cur) {
+            const int nx = P.lv[l].nx, ny = P.lv[l].ny, o = P.lv[l].off;
+            const float *XI = Xb[cur];
+            float *XO = Xb[cur ^ 1];
+            for (int iy = ty; iy < ny; iy += nty)
+                for (int ix = tx; ix < nx; ix += 32) {
+                    const int i = ix + iy * nx;
+                    XO[o + i] = XI[o + i] + sP[o + i] * (sB[o + i] - Ax(l, XI, ix, iy, i));
+                }
+            __syncthreads();
+            return cur ^ 1;
+        };
+        for (int l = ND; l < L - 1; l++) {
+            const int n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
+            for (int i = tid; i < n; i += kClusterThreads) sX[o + i] = sP[o + i] * sB[o + i];
+            __syncthreads();
+            int cur = 0;
+            for (int k = 1; k < nu; k++) cur = sweep(l, cur);
+            const float *XC = Xb[cur];
+            const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, nxc = P.lv[l + 1].nx, nyc = P.lv[l + 1].ny,
+                      oc = P.lv[l + 1].off;
+            for (int J = ty; J < nyc; J += nty)
+                for (int I = tx; I < nxc; I += 32) {
+                    float sres = 0.0f;
+                    for (int dj = 0; dj < 2; dj++)
+                        for (int di = 0; di < 2; di++) {
+                            const int i = 2 * I + di, j = 2 * J + dj;
+                            if (i >= nxf || j >= nyf) continue;
+                            const int f = i + j * nxf;
+                            if (!sA[o + f]) continue;
+                            sres += sB[o + f] - Ax(l, XC, i, j, f);
+                        }
+                    sB[oc + I + J * nxc] = sres;
+                }
+            __syncthreads();
+        }
+        {  // coarsest level: exact solve
+            const int l = L - 1, n = P.lv[l].nx * P.lv[l].ny, o = P.lv[l].off;
+            for (int i = tid; i < n; i += kClusterThreads) sX[o + i] = sA[o + i] ? sB[o + i] / sD[o + i] : sB[o + i];
+            __syncthreads();
+        }
+        for (int l = L - 2; l >= ND; l--) {
+            const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, o = P.lv[l].off, nxc = P.lv[l + 1].nx,
+                      oc = P.lv[l + 1].off;
+            float *XF = Xb[cur_down];
+            const float *XC = Xb[l + 1 == L - 1 ? 0 : cur_up];
+            for (int j = ty; j < nyf; j += nty)
+                for (int i = tx; i < nxf; i += 32) {
+                    const int f = i + j * nxf;
+                    if (sA[o + f]) XF[o + f] += wc * XC[oc + (i >> 1) + (j >> 1) * nxc];
+                }
+            __syncthreads();
+            int cur = cur_down;
+            for (int k = 0; k < nu; k++) cur = sweep(l, cur);
+        }
+    }
+    cl_sync();
+    for (int l = ND - 1; l >= 0; l--) {  // ascend on the distributed levels
+        int s, e;
+        rows(l, rank, s, e);
+        const int nx = P.lv[l].nx, nxc = P.lv[l + 1].nx;
+        float *XF = Xb[cur_down];
+        const float *XC = Xb[l + 1 == L - 1 ? 0 : cur_up];
+        int cs, ce;
+        if (l + 1 < ND) rows(l + 1, rank, cs, ce);
+        for (int iy = s + ty; iy < e; iy += nty)
+            for (int ix = tx; ix < nx; ix += 32) {
+                const int f = at(l, s, ix, iy);
+                if (!sA[f]) continue;
+                float xc;
+                if (l + 1 < ND) xc = XC[at(l + 1, cs, ix >> 1, iy >> 1)];
+                else {
+                    const float *q = XC + P.lv[l + 1].off + (ix >> 1) + (iy >> 1) * nxc;
+                    xc = rank == 0 ? *q : cl_ld(q, 0);
+                }
+                XF[f] += wc * xc;
+            }
+        cl_sync();
+        int cur = cur_down;
+        for (int k = 0; k < nu; k++) cur = sweep_d(l, cur);
+    }
+    for (int iy = s0 + ty; iy < e0; iy += nty)
+        for (int ix = tx; ix < P.lv[0].nx; ix += 32) x_top[ix + iy * P.lv[0].nx] = Xb[cur_up][at(0, s0, ix, iy)];
+}
+
+// ---------------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------------
 static int mg_grid(Ctx *c, long long n) {
@@ -1425,6 +1716,87 @@ static size_t bottom_plan(const Ctx *c, int lb, BottomPlan *P) {
     return (size_t)off * kBottomBytesPerCell;
 }
 
+// The cluster kernel's levels: lc = the finest level >= 1 whose slabs fit kClusterBytes, the CTA-0
+// levels from the first one with at most kCta0Cells cells.  False when the hierarchy has no level
+// to distribute (small grids: the one-block bottom kernel serves them).
+static bool cluster_plan(const Ctx *c, int *lc_out, ClusterPlan *P, size_t *bytes) {
+    const int nl = c->mg_levels;
+    int ld = -1;
+    for (int l = 2; l < nl && ld < 0; l++)
+        if ((long long)c->mg[l].nx * c->mg[l].ny <= kCta0Cells) ld = l;
+    if (ld < 2) return false;
+    int rows0[kClusterCtas + 1];
+    for (int k = 0; k <= kClusterCtas; k++) rows0[k] = (int)((long long)k * c->mg[ld].ny / kClusterCtas);
+    auto slab_rows = [&](int l) {  // the most rows any CTA holds on distributed level l
+        const int sh = ld - l, ny = c->mg[l].ny;
+        int r = 0;
+        for (int k = 0; k < kClusterCtas; k++)
+            r = std::max(r, std::min(rows0[k + 1] << sh, ny) - std::min(rows0[k] << sh, ny));
+        return r;
+    };
+    long long small = 0;
+    for (int l = ld; l < nl; l++) small += (long long)c->mg[l].nx * c->mg[l].ny;
+    for (int lc = 1; lc < ld; lc++) {
+        long long cells = small;
+        for (int l = lc; l < ld; l++) cells += (long long)(slab_rows(l) + 1) * c->mg[l].nx;
+        if ((size_t)cells * kClusterBytesPerCell > kClusterBytes) continue;
+        memset(P, 0, sizeof(*P));
+        P->nlev = nl - lc;
+        P->ndist = ld - lc;
+        P->total = (int)cells;
+        for (int k = 0; k <= kClusterCtas; k++) P->rows0[k] = rows0[k];
+        int off = 0;
+        for (int k = 0; k < P->nlev; k++) {
+            const MgLevel &m = c->mg[lc + k];
+            P->lv[k] = BottomLevel{m.nx, m.ny, off};
+            P->aE[k] = m.aE; P->aN[k] = m.aN; P->dP[k] = m.dP; P->wD[k] = m.wD; P->act[k] = m.act;
+            P->slot_rows[k] = k < P->ndist ? slab_rows(lc + k) + 1 : m.ny;
+            off += P->slot_rows[k] * m.nx;
+        }
+        *lc_out = lc;
+        *bytes = (size_t)cells * kClusterBytesPerCell;
+        return true;
+    }
+    return false;
+}
+
+// Per device: 0 not yet checked, 1 the cluster kernel can run, -1 it cannot (no cluster of
+// kClusterCtas CTAs with its shared memory fits).  Checked in mg_setup, outside any stream capture.
+static int g_cluster_ok[128] = {};
+
+static int cluster_check(Ctx *c) {
+    if (c->device < 0 || c->device >= 128) return fail(c, SHK_BAD_ARG, "device ordinal out of range");
+    if (g_cluster_ok[c->device]) return SHK_OK;
+    cudaError_t e = cudaFuncSetAttribute(k_mg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterBytes);
+    int n = 0;
+    if (e == cudaSuccess) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(kClusterCtas);
+        cfg.blockDim = dim3(kClusterThreads);
+        cfg.dynamicSmemBytes = kClusterBytes;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = kClusterCtas;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        e = cudaOccupancyMaxActiveClusters(&n, k_mg_cluster, &cfg);
+    }
+    if (e != cudaSuccess) cudaGetLastError();
+    g_cluster_ok[c->device] = (e == cudaSuccess && n > 0) ? 1 : -1;
+    return SHK_OK;
+}
+
+// The first level of the cluster kernel, or -1 when the one-block bottom kernel serves (also where
+// the bottom kernel alone already starts at or above that level: small grids).
+static int cluster_start(const Ctx *c, ClusterPlan *P, size_t *bytes) {
+    if (!c->mg_cluster || c->device < 0 || c->device >= 128 || g_cluster_ok[c->device] != 1) return -1;
+    int lc = -1;
+    if (!cluster_plan(c, &lc, P, bytes) || lc >= bottom_level(c)) return -1;
+    return lc;
+}
+
 struct MgTma;
 static MgTma *tma_maps(Ctx *c, int *rc);
 
@@ -1466,6 +1838,10 @@ int mg_setup(Ctx *c) {
                                                  (int)kBottomBytes);
             if (e != cudaSuccess) return check_cuda(c, e, "multigrid bottom shared memory");
             attr_set[c->device] = true;
+        }
+        if (c->mg_cluster) {
+            const int rc = cluster_check(c);
+            if (rc) return rc;
         }
         if (fused(c) && !marching(c)) {  // tensor maps and kernel attributes, outside any capture
             int rc = SHK_OK;
@@ -1628,6 +2004,30 @@ static int vcycle(Ctx *c, int l, CgDev *cg, int *res) {
     const int *done = &cg->done;
     const Lv L = level_view(m, done);
     const float wc = c->mg_omega_c;
+    {
+        ClusterPlan CP;
+        size_t bytes = 0;
+        if (l == cluster_start(c, &CP, &bytes)) {
+            CP.done = done;
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(kClusterCtas);
+            cfg.blockDim = dim3(kClusterThreads);
+            cfg.dynamicSmemBytes = bytes;
+            cfg.stream = c->stream;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = kClusterCtas;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            const cudaError_t e = cudaLaunchKernelEx(&cfg, k_mg_cluster, CP, (const float *)m.b, m.x[0], c->mg_nu, wc);
+            if (e != cudaSuccess) return check_cuda(c, e, "multigrid cluster kernel launch");
+            c->launches++;
+            *res = 0;
+            return SHK_OK;
+        }
+    }
     if (l == bottom_level(c)) {
         BottomPlan P;
         const size_t smem = bottom_plan(c, l, &P);

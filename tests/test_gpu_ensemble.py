@@ -110,9 +110,10 @@ def test_ensemble_multigrid_form_matches_single_instance_runs(shk, cuda, monkeyp
     """The mixed-precision form (Float64 CG, Float32 multigrid V-cycle) batched over instances: every
     level kernel is one launch over the instances that have that level, each instance's bottom
     solve one block of one launch.  Against each instance's own run through the same (LDG-staged)
-    level kernels, with the context's own CG tile height (no autotune): equal Picard counts, fields
-    within 1e-10."""
+    level kernels and one-block bottom solve, with the context's own CG tile height (no autotune):
+    equal Picard counts, fields within 1e-10."""
     monkeypatch.setenv("SHK_MG_TMA", "0")  # read at context creation: the single runs' staging
+    monkeypatch.setenv("SHK_MG_CLUSTER", "0")  # and their coarse levels: the one-block bottom kernel
     steps = 3
     ens_sims = [make_sim(shk, *sp, steps, rtol=1e-10, multigrid=True) for sp in MG_SPECS]
     ref_sims = [make_sim(shk, *sp, steps, rtol=1e-10, multigrid=True) for sp in MG_SPECS]

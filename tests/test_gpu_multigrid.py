@@ -108,6 +108,26 @@ def test_cg_launch_modes_are_bit_identical_tma(shk, cuda, monkeypatch):
     assert np.array_equal(h0, h1) and np.array_equal(h0, h2)
 
 
+@pytest.mark.parametrize("which", ["ragged301", "tma512x360"])
+def test_cluster_coarse_levels_match_tile_levels_and_bottom(shk, cuda, monkeypatch, which):
+    """The coarse levels on one thread-block cluster (slabs of the levels below the tile kernels in
+    eight CTAs' shared memory, halo rows read from the neighbouring CTAs, the smallest levels in CTA
+    0) against the same V-cycle run by the tile kernels down to the one-block bottom kernel
+    (SHK_MG_CLUSTER=0).  The two form the coarse levels' Float32 multiply-adds in a different order,
+    so after one CG iteration the heads agree to Float32 rounding of the V-cycle (1e-6), and full
+    solves take the same number of iterations (+-1) and agree within the rel-res 1e-8 error ball."""
+    w = ragged_workload(shk) if which == "ragged301" else tma_workload(shk, 512, 360)
+    h_c, st_c = solve(shk, w, {"SHK_MG_CLUSTER": "1"}, monkeypatch, itmax=1, rtol=0.0)
+    h_b, st_b = solve(shk, w, {"SHK_MG_CLUSTER": "0"}, monkeypatch, itmax=1, rtol=0.0)
+    assert st_c.niter == st_b.niter == 1
+    assert relerr(h_c, h_b) <= 1e-6, relerr(h_c, h_b)
+    h_c, st_c = solve(shk, w, {"SHK_MG_CLUSTER": "1"}, monkeypatch)
+    h_b, st_b = solve(shk, w, {"SHK_MG_CLUSTER": "0"}, monkeypatch)
+    assert st_c.status == st_b.status == 0
+    assert abs(st_c.niter - st_b.niter) <= 1, (st_c.niter, st_b.niter)
+    assert relerr(h_c, h_b) <= 1e-7, relerr(h_c, h_b)
+
+
 def test_tma_multigrid_run_matches_oracle(shk, orc, cuda, monkeypatch):
     """The TMA-staged multigrid form against the oracle (not only against the LDG staging) at
     512 x 360, where levels 0-2 stage through TMA: one linear solve at rel-res 1e-12 on the GROUNDED
