@@ -73,6 +73,9 @@ def parse():
                          "prints its own JSON line instead of the 4096^2 one")
     ap.add_argument("--ens-form", default="multigrid", choices=["multigrid", "plain"],
                     help="ensemble mode: Float64 CG with the Float32 multigrid V-cycle (mixed precision) or Jacobi")
+    ap.add_argument("--ens-c-range", type=float, nargs=2, default=(5e3, 5e4), metavar=("C_MIN", "C_MAX"),
+                    help="ensemble mode: range of the instances' sliding coefficient C (default: the described "
+                         "5e3-5e4, with which many instances' Picard loops do not converge)")
     ap.add_argument("--ens-sequential", type=int, default=32,
                     help="ensemble mode: instances also run one after another through the single-instance path")
     ap.add_argument("--warmstart", action="store_true",
@@ -670,7 +673,7 @@ def ensemble_bench(args):
     are outside the timed region)."""
     import torch
     shk = entry.load_package()
-    specs = shk.configs.ensemble_specs(args.ensemble)
+    specs = shk.configs.ensemble_specs(args.ensemble, c_range=tuple(args.ens_c_range))
     params = dict(shk.configs.SEASONAL_PARAMS)
 
     def make(sp):
@@ -719,7 +722,8 @@ def ensemble_bench(args):
                                 if args.ens_form == "multigrid" else "batched Float64 Jacobi CG, ")
                                + "one launch per kernel over all instances, one CUDA graph per timestep (device-side "
                                  "Picard and CG loops)",
-                       "params": params, "picard": "500 iters, tol 1e-6", "dt_s": args.dt,
+                       "params": params, "sliding_C_range": list(args.ens_c_range),
+                       "picard": "500 iters, tol 1e-6", "dt_s": args.dt,
                        "timing": "the same K steps from the initial states in both arms"},
             "march_th_by_size": by_size, "setup_s": round(setup_s, 2),
             "instance_steps": len(sims) * args.steps, "converged_instance_steps": conv,
