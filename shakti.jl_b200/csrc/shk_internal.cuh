@@ -152,6 +152,7 @@ struct Ctx {
     int mg_tma = 1;          // tile kernels stage through TMA copies where the level's pitch allows
     bool mg_cluster = false;  // the coarse levels on one thread-block cluster (measured slower; opt-in)
     struct MgTma *mg_maps = nullptr;  // the levels' tensor maps (built on first use)
+    struct CgTma *cg_maps = nullptr;  // the plain Jacobi CG's tensor maps (built before its first capture)
     int max_blocks = 0;
     int grid_stencil = 0;    // blocks for tile-stride kernels
     int march_th = 8;        // row-marching tile height
@@ -286,6 +287,9 @@ int mg_setup(Ctx *c);
 void mg_release(Ctx *c);
 int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init);
 bool mg_fuses_cg_update(const Ctx *c);
+int cg_tma_prepare(Ctx *c);
+int cg_jac_matvec(Ctx *c, int par, const double *r, const double *p_old, double *p_new, double *Ap, CgDev *cg,
+                  double eps_curv, bool *launched);
 int mg_cg_matvec(Ctx *c, int par, const double *aP, const double *aE, const double *aN, const double *z,
                  const double *p_old, double *p_new, double *Ap, CgDev *cg, double eps_curv, bool *launched);
 int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, const double *p, const double *Ap,

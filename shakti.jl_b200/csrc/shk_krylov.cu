@@ -872,6 +872,10 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
         return SHK_OK;
     };
     const double eps_curv = sizeof(T) == 8 ? DBL_EPSILON : (double)FLT_EPSILON;
+    if constexpr (std::is_same<T, double>::value) {
+        if (jac && !lapl)  // tensor maps of the tile form, before any capture below
+            if (int rc0 = cg_tma_prepare(c)) return rc0;
+    }
     cgh->trips = 0;
     if (int rc0 = move_scalars(c, cgd, cgh, sizeof(CgDev), false)) return rc0;
     cudaError_t e = cudaSuccess;
@@ -914,9 +918,17 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
                 nx, ny, c->march_th, aP, aE, aN, r, nullptr, p_old, p_new, Ap, cgd, c->partials, c->counter, eps_curv,
                 lapl);
         } else if (jac) {
-            k_cg_A<T, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(nx, ny, c->march_th, aP, aE, aN, r, nullptr,
-                                                                       p_old, p_new, Ap, cgd, c->partials, c->counter,
-                                                                       eps_curv);
+            bool launched = false;  // the TMA-staged tile form where the context's maps cover the buffers
+            if constexpr (std::is_same<T, double>::value) {
+                if (aP == c->aP && aE == c->aE && aN == c->aN) {
+                    const int rc = cg_jac_matvec(c, par, r, p_old, p_new, Ap, cgd, eps_curv, &launched);
+                    if (rc) return rc;
+                }
+            }
+            if (!launched)
+                k_cg_A<T, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(nx, ny, c->march_th, aP, aE, aN, r,
+                                                                           nullptr, p_old, p_new, Ap, cgd,
+                                                                           c->partials, c->counter, eps_curv);
         } else if (lapl) {
             k_cg_A<T, false, true><<<c->march_blocks, kMarchX, 0, c->stream>>>(
                 nx, ny, c->march_th, aP, aE, aN, r, z, p_old, p_new, Ap, cgd, c->partials, c->counter, eps_curv, lapl);
@@ -1129,7 +1141,7 @@ int run_cg(Ctx *c, const shk_cg_opts *o, shk_cg_stats *st) {
         if ((rc = check_launch(c, "cg finish"))) return rc;
         if ((rc = read_scalars(c))) return rc;
         const CgDev &g = c->host_dev->cg;
-        if (g.fault) return fail(c, SHK_CUDA_ERROR, "multigrid: a tile copy did not complete (bounded wait ran out)");
+        if (g.fault) return fail(c, SHK_CUDA_ERROR, "a TMA tile copy did not complete (bounded wait ran out)");
         s.niter = (long)g.iter;
         s.status = g.status;
         s.rnorm0 = g.rnorm0;

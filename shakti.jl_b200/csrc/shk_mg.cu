@@ -953,20 +953,25 @@ struct MvArgs {
 
 constexpr unsigned rnd128(unsigned v) { return (v + 127u) & ~127u; }
 
-struct MvLayout {
-    static constexpr unsigned pB = kMvW * kMvH * 8, apB = kFW * kFH * 8, aeB = (kFW + 2) * kFH * 8,
+// JAC: the plain Jacobi-preconditioned CG's form -- z = r / aP is formed in the kernel, so aP is
+// staged over the same 36 x 18 region as r and p_old.
+template <bool JAC = false>
+struct MvLayoutT {
+    static constexpr unsigned pB = kMvW * kMvH * 8, apB = JAC ? pB : kFW * kFH * 8, aeB = (kFW + 2) * kFH * 8,
                               anB = kFW * (kFH + 1) * 8;
     static constexpr unsigned o_z = 0, o_po = rnd128(pB), o_aP = rnd128(o_po + pB), o_aE = rnd128(o_aP + apB),
                               o_aN = rnd128(o_aE + aeB), stage = rnd128(o_aN + anB);
     static constexpr unsigned o_p = 2 * stage, o_bar = rnd128(o_p + pB), bytes = o_bar + 16;
 };
+using MvLayout = MvLayoutT<false>;
 
+template <bool JAC>
 __global__ void __launch_bounds__(256, 4) k_cg_matvec_t(const __grid_constant__ MvArgs M, int nx, int ny,
                                                         double *p_new, double *Ap, CgDev *cg, double *partials,
                                                         unsigned int *counter, double eps_curv) {
     const CgView cv = block_cg_view(cg);
     if (cv.done) return;
-    using Y = MvLayout;
+    using Y = MvLayoutT<JAC>;
     extern __shared__ __align__(128) unsigned char sm[];
     double *P = reinterpret_cast<double *>(sm + Y::o_p);
     const bool first = cv.first != 0;
@@ -985,7 +990,8 @@ __global__ void __launch_bounds__(256, 4) k_cg_matvec_t(const __grid_constant__ 
             tma_expect(b, tx);
             tma_load(st + Y::o_z, &M.z, b, x0 - 2, y0 - 1);
             if (!first) tma_load(st + Y::o_po, &M.po, b, x0 - 2, y0 - 1);
-            tma_load(st + Y::o_aP, &M.aP, b, x0, y0);
+            if (JAC) tma_load(st + Y::o_aP, &M.aP, b, x0 - 2, y0 - 1);
+            else tma_load(st + Y::o_aP, &M.aP, b, x0, y0);
             tma_load(st + Y::o_aE, &M.aE, b, x0 - 2, y0);
             tma_load(st + Y::o_aN, &M.aN, b, x0, y0 - 1);
         },
@@ -993,8 +999,13 @@ __global__ void __launch_bounds__(256, 4) k_cg_matvec_t(const __grid_constant__ 
         [&](unsigned char *st, int x0, int y0) {
             const double *Z = reinterpret_cast<const double *>(st + Y::o_z);
             const double *PO = reinterpret_cast<const double *>(st + Y::o_po);
+            const double *APh = reinterpret_cast<const double *>(st + Y::o_aP);
             auto form = [&](int k) {
-                const double2 z = *reinterpret_cast<const double2 *>(Z + k);
+                double2 z = *reinterpret_cast<const double2 *>(Z + k);  // JAC: r
+                if (JAC) {  // outside the grid r = aP = 0 gives NaN there, a value no output reads
+                    const double2 d = *reinterpret_cast<const double2 *>(APh + k);
+                    z = make_double2(__ddiv_rn(z.x, d.x), __ddiv_rn(z.y, d.y));
+                }
                 double2 v = z;
                 if (!first) {
                     const double2 po = *reinterpret_cast<const double2 *>(PO + k);
@@ -1016,7 +1027,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_matvec_t(const __grid_constant__ 
                 for (int e = 0; e < 2; e++) {
                     const int k = kp + e, ix = gx + e;
                     const double pk = P[k];
-                    double v = __dmul_rn(AP[r * kFW + pc + e], pk);
+                    double v = __dmul_rn(JAC ? AP[k] : AP[r * kFW + pc + e], pk);
                     if (ix < nx - 1) v = __dsub_rn(v, __dmul_rn(AE[r * (kFW + 2) + pc + e + 2], P[k + 1]));
                     if (ix > 0) v = __dsub_rn(v, __dmul_rn(AE[r * (kFW + 2) + pc + e + 1], P[k - 1]));
                     if (gy + 1 < ny) v = __dsub_rn(v, __dmul_rn(AN[(r + 1) * kFW + pc + e], P[k + kMvW]));
@@ -1894,6 +1905,8 @@ static int tma_kernel_bps(Ctx *c, K kernel, unsigned smem, int *blocks_per_sm) {
 void mg_release(Ctx *c) {
     delete c->mg_maps;
     c->mg_maps = nullptr;
+    delete c->cg_maps;
+    c->cg_maps = nullptr;
 }
 
 // The maps, or nullptr when the TMA kernels are off or no level qualifies.
@@ -1955,7 +1968,7 @@ static MgTma *tma_maps(Ctx *c, int *rc) {
     if (!e) e = tma_kernel_bps(c, k_mg_down_t<float, false>, TLayout<float, false, false>::bytes, &bps[TK_DOWN]);
     if (!e) e = tma_kernel_bps(c, k_mg_up_t<double, true>, TLayout<double, true, false>::bytes, &bps[TK_UP0]);
     if (!e) e = tma_kernel_bps(c, k_mg_up_t<float, false>, TLayout<float, true, false>::bytes, &bps[TK_UP]);
-    if (!e) e = tma_kernel_bps(c, k_cg_matvec_t, MvLayout::bytes, &bps[TK_MV]);
+    if (!e) e = tma_kernel_bps(c, k_cg_matvec_t<false>, MvLayout::bytes, &bps[TK_MV]);
     if (e) {
         delete T;
         *rc = e;
@@ -2194,10 +2207,62 @@ int mg_cg_matvec(Ctx *c, int par, const double *aP, const double *aE, const doub
         return SHK_OK;
     const MgLevel &m = c->mg[0];
     const MvArgs a{T->mv_z, T->mv_p[par], T->mv_aP, T->mv_aE, T->mv_aN};
-    k_cg_matvec_t<<<tma_grid(c, T, TK_MV, m), 256, MvLayout::bytes, c->stream>>>(
+    k_cg_matvec_t<false><<<tma_grid(c, T, TK_MV, m), 256, MvLayout::bytes, c->stream>>>(
         a, m.nx, m.ny, p_new, Ap, cg, c->partials, c->counter, eps_curv);
     *launched = true;
     return check_launch(c, "cg matvec");
+}
+
+// The plain Jacobi-preconditioned Float64 CG's p update and matvec on the same TMA-staged tiles
+// (k_cg_matvec_t<true>: z = r / aP formed in the kernel; the roundings of k_cg_A<double, true>).
+// Maps of the context's r, p[0], p[1], aP, aE, aN, built once per context before any capture.
+struct CgTma {
+    bool ok = false;
+    CUtensorMap r, p[2], aP, aE, aN;
+    int grid = 0;  // blocks of one resident wave
+};
+
+int cg_tma_prepare(Ctx *c) {
+    if (c->cg_maps || !c->mg_tma) return SHK_OK;
+    CgTma *T = new CgTma();
+    c->cg_maps = T;
+    void *fp = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fp, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fp) {
+        cudaGetLastError();
+        return SHK_OK;  // k_cg_A serves
+    }
+    const EncodeTiledFn fn = (EncodeTiledFn)fp;
+    const CUtensorMapDataType F64 = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const int nx = c->nx, ny = c->ny;
+    const bool maps = encode(fn, &T->r, F64, 8, c->r, nx, ny, kMvW, kMvH) &&
+                      encode(fn, &T->p[0], F64, 8, c->p[0], nx, ny, kMvW, kMvH) &&
+                      encode(fn, &T->p[1], F64, 8, c->p[1], nx, ny, kMvW, kMvH) &&
+                      encode(fn, &T->aP, F64, 8, c->aP, nx, ny, kMvW, kMvH) &&
+                      encode(fn, &T->aE, F64, 8, c->aE, nx, ny, kFW + 2, kFH) &&
+                      encode(fn, &T->aN, F64, 8, c->aN, nx, ny, kFW, kFH + 1);
+    if (!maps) return SHK_OK;
+    int bps = 0;
+    if (int e = tma_kernel_bps(c, k_cg_matvec_t<true>, MvLayoutT<true>::bytes, &bps)) return e;
+    if (bps < 1) return SHK_OK;
+    T->grid = c->num_sms * bps;
+    T->ok = true;
+    return SHK_OK;
+}
+
+int cg_jac_matvec(Ctx *c, int par, const double *r, const double *p_old, double *p_new, double *Ap, CgDev *cg,
+                  double eps_curv, bool *launched) {
+    *launched = false;
+    const CgTma *T = c->cg_maps;
+    if (!T || !T->ok || r != c->r || p_old != c->p[par] || p_new != c->p[par ^ 1] || Ap != c->Ap) return SHK_OK;
+    const long long tiles = (long long)((c->nx + kFW - 1) / kFW) * ((c->ny + kFH - 1) / kFH);
+    const int grid = (int)std::max(1LL, std::min({tiles, (long long)c->max_blocks, (long long)T->grid}));
+    const MvArgs a{T->r, T->p[par], T->aP, T->aE, T->aN};
+    k_cg_matvec_t<true><<<grid, 256, MvLayoutT<true>::bytes, c->stream>>>(a, c->nx, c->ny, p_new, Ap, cg,
+                                                                           c->partials, c->counter, eps_curv);
+    *launched = true;
+    return check_launch(c, "cg matvec (Jacobi)");
 }
 
 // One iteration's x/r update fused into the V-cycle's first level-0 kernel (tile form, nu = 2):
