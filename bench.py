@@ -341,7 +341,8 @@ def roofline_for(shk, sim, form, w, peaks):
     nbytes = iteration_bytes(form, w.nx, w.ny)
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = nbytes / (it_ms / 1e3) / 1e9
-    kernel = {"plain": "k_cg_A + k_cg_B (one Jacobi-PCG iteration, Float64)",
+    kernel = {"plain": "k_cg_matvec_t<true> + k_cg_B (one Jacobi-PCG iteration, Float64: the p update with "
+                       "z = r/aP and the matvec on TMA-staged tiles, then the x/r update)",
               "fp32cg": "k_cg_A + k_cg_B (one Jacobi-PCG iteration, Float32 Laplacian form)",
               "multigrid": "one multigrid-preconditioned CG iteration: the TMA-staged Float64 p update and "
                            "matvec (k_cg_matvec_t), the Float32 V-cycle on TMA-staged tiles (k_mg_down_t, its "
