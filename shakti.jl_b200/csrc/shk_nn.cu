@@ -25,6 +25,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 
+#include <type_traits>
+
 #include "../../include/shakti_b200.h"
 
 namespace shk {
@@ -340,6 +342,7 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(const bf16 *__restrict__ X, 
 // flight are waited for, TMEM is freed.
 // ---------------------------------------------------------------------------------------------
 constexpr int kHxRows = 16, kHxThreads = 160;
+constexpr uint32_t kHxMaxSmem = 227u * 1024;  // dynamic shared memory a CTA may have on sm_100
 
 template <int NT>
 struct HxCfg {
@@ -351,11 +354,20 @@ struct HxCfg {
     static constexpr uint32_t WG = 9 * NT * 16;                  // one 8-channel group of the weights
     static constexpr uint32_t stage = 2 * HG + 2 * WG;
     static constexpr int S = 4 * stage <= 200u * 1024 ? 4 : (3 * stage <= 200u * 1024 ? 3 : 2);
-    static constexpr uint32_t bars = S * stage;                  // full[S], empty[S], accf[ACC], acce[ACC]
-    static constexpr uint32_t misc = bars + 8 * (2 * S + 2 * ACC);  // TMEM address, abort flag
+    static constexpr uint32_t bars = S * stage;  // full[S], empty[S], accf[ACC], acce[ACC], the weights' barrier
+    static constexpr uint32_t misc = bars + 8 * (2 * S + 2 * ACC + 1);  // TMEM address, abort flag
     static constexpr uint32_t used = misc + 16;
     // more than half of an SM's shared memory: one CTA per SM, which then owns all 512 TMEM columns
     static constexpr uint32_t bytes = used > 120u * 1024 ? used : 120u * 1024;
+    // weights-resident form: all of a layer's weights loaded once per CTA after the halo stages,
+    // the stages carry halo chunks only
+    static constexpr uint32_t rstage = 2 * HG;
+    static constexpr int RS = 4;
+    static uint32_t __host__ __device__ res_bars(int Cin) { return (RS * rstage + (uint32_t)(Cin / 8) * WG + 127) / 128 * 128; }
+    static uint32_t __host__ __device__ res_bytes(int Cin) {
+        const uint32_t u = res_bars(Cin) + 8 * (2 * RS + 2 * ACC + 1) + 16;
+        return u > 120u * 1024 ? u : 120u * 1024;
+    }
 };
 
 __device__ __forceinline__ void hx_expect(uint64_t *bar, uint32_t bytes) {
@@ -405,19 +417,21 @@ __device__ __forceinline__ void hx_commit(uint64_t *bar) {
                  : "memory");
 }
 
-template <int NT>
+template <int NT, bool RES>
 __global__ void __launch_bounds__(kHxThreads, 1) k_conv3x3_hx(const __grid_constant__ CUtensorMap mx,
                                                               const __grid_constant__ CUtensorMap mw,
                                                               const float *__restrict__ bias, bf16 *__restrict__ Y,
                                                               float *__restrict__ Yf, int N, int H, int W, int Cin,
                                                               int Cout, int relu, int flip, int *err) {
     using Cf = HxCfg<NT>;
-    constexpr int MT = Cf::MT, ACC = Cf::ACC, S = Cf::S;
+    constexpr int MT = Cf::MT, ACC = Cf::ACC, S = RES ? Cf::RS : Cf::S;
+    constexpr uint32_t STG = RES ? Cf::rstage : Cf::stage;  // bytes of one stage
     extern __shared__ __align__(1024) unsigned char sm[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(sm + Cf::bars), *empty = full + S, *accf = empty + S,
-             *acce = accf + ACC;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + Cf::misc);
-    volatile int *abort = reinterpret_cast<volatile int *>(sm + Cf::misc + 4);
+    const uint32_t bars_off = RES ? Cf::res_bars(Cin) : Cf::bars, misc_off = bars_off + 8 * (2 * S + 2 * ACC + 1);
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm + bars_off), *empty = full + S, *accf = empty + S,
+             *acce = accf + ACC, *wbar = acce + ACC;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + misc_off);
+    volatile int *abort = reinterpret_cast<volatile int *>(sm + misc_off + 4);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_x = (W + 8 * MT - 1) / (8 * MT), tiles_y = (H + kHxRows - 1) / kHxRows;
     const long long T = (long long)N * tiles_x * tiles_y;
@@ -440,6 +454,7 @@ __global__ void __launch_bounds__(kHxThreads, 1) k_conv3x3_hx(const __grid_const
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&accf[i])) : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(su32(&acce[i])) : "memory");
         }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(wbar)) : "memory");
         *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -465,17 +480,24 @@ __global__ void __launch_bounds__(kHxThreads, 1) k_conv3x3_hx(const __grid_const
                 const int slot = (int)(q % S), kc = (int)(q % nc);
                 int n, y0, x0;
                 tile_at(q / nc, n, y0, x0);
-                unsigned char *st = sm + slot * Cf::stage;
-                hx_expect(&full[slot], 2 * (Cf::HB + Cf::WG));
+                unsigned char *st = sm + slot * STG;
+                hx_expect(&full[slot], RES ? 2 * Cf::HB : 2 * (Cf::HB + Cf::WG));
                 for (int g = 0; g < 2; g++) {
                     hx_load4(st + g * Cf::HG, &mx, &full[slot], kc * 16 + g * 8, x0 - 1, y0 - 1, n);
-                    hx_load3(st + 2 * Cf::HG + g * Cf::WG, &mw, &full[slot], kc * 16 + g * 8, 0, 0);
+                    if (!RES) hx_load3(st + 2 * Cf::HG + g * Cf::WG, &mw, &full[slot], kc * 16 + g * 8, 0, 0);
                 }
             };
+            unsigned char *wres = sm + S * STG;  // RES: the layer's weights, [group][tap][co][8 channels]
+            if (RES) {
+                hx_expect(wbar, (uint32_t)(Cin / 8) * Cf::WG);
+                for (int g = 0; g < Cin / 8; g++) hx_load3(wres + g * Cf::WG, &mw, wbar, g * 8, 0, 0);
+            }
             constexpr uint32_t idesc = umma_idesc_bf16(kTcM, NT);
             long long issued = 0, consumed = 0;
             bool ok = true;
             for (; issued < total && issued < S - 1; issued++) load(issued);
+            bool wdone = !RES;
+            if (RES) wdone = ok = hx_wait(wbar, 0, abort);
             for (long long q = 0; q < total && ok; q++) {
                 const int slot = (int)(q % S), kc = (int)(q % nc);
                 const long long ti = q / nc;
@@ -484,19 +506,28 @@ __global__ void __launch_bounds__(kHxThreads, 1) k_conv3x3_hx(const __grid_const
                 if (ok && kc == 0 && ti >= ACC) ok = hx_wait(&acce[buf], (uint32_t)((ti / ACC - 1) & 1), abort);
                 if (!ok) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t st = su32(sm + slot * Cf::stage), wt = st + 2 * Cf::HG;
-#pragma unroll 1
-                for (int t = 0; t < 9; t++) {
-                    int dy = t / 3 - 1, dx = t % 3 - 1;
-                    if (flip) { dy = -dy; dx = -dx; }
-                    const uint64_t db = umma_desc(wt + (uint32_t)(t * NT * 16), Cf::WG, 128);
+                const uint32_t st = su32(sm + slot * STG),
+                               wt = RES ? su32(wres) + (uint32_t)(2 * kc) * Cf::WG : st + 2 * Cf::HG;
+                // two base descriptors per chunk; a tap's and an M tile's operands are constant offsets
+                // (in 16-byte units) added to the start-address field, which never carries out of it
+                // (shared-memory addresses stay below 2^14 x 16 B)
+                const uint64_t da0 = umma_desc(st, Cf::HG, Cf::HW * 16), db0 = umma_desc(wt, Cf::WG, 128);
+                const uint32_t d0 = tmem + (uint32_t)(buf * MT * NT);
+                auto issue = [&](auto flipc) {
+                    constexpr bool F = decltype(flipc)::value;
 #pragma unroll
-                    for (int j = 0; j < MT; j++) {
-                        const uint32_t a = st + (uint32_t)(((1 + dy) * Cf::HW + 8 * j + 1 + dx) * 16);
-                        const uint64_t da = umma_desc(a, Cf::HG, Cf::HW * 16);
-                        hx_mma(tmem + (uint32_t)((buf * MT + j) * NT), da, db, idesc, (kc > 0 || t > 0) ? 1u : 0u);
+                    for (int t = 0; t < 9; t++) {
+                        const int dy = F ? 1 - t / 3 : t / 3 - 1, dx = F ? 1 - t % 3 : t % 3 - 1;
+                        const uint64_t db = db0 + (uint64_t)(t * NT);  // t * NT * 16 bytes
+                        const uint32_t acc = (kc > 0 || t > 0) ? 1u : 0u;
+#pragma unroll
+                        for (int j = 0; j < MT; j++)
+                            hx_mma(d0 + (uint32_t)(j * NT), da0 + (uint64_t)((1 + dy) * Cf::HW + 8 * j + 1 + dx), db,
+                                   idesc, acc);
                     }
-                }
+                };
+                if (flip) issue(std::true_type{});
+                else issue(std::false_type{});
                 hx_commit(&empty[slot]);
                 if (kc == nc - 1) hx_commit(&accf[buf]);
                 consumed = q + 1;
@@ -513,6 +544,7 @@ __global__ void __launch_bounds__(kHxThreads, 1) k_conv3x3_hx(const __grid_const
             }
             // wind down: every copy issued has landed and every MMA committed has finished
             for (long long q = consumed; q < issued; q++) hx_wait(&full[q % S], (uint32_t)((q / S) & 1), nullptr);
+            if (!wdone) hx_wait(wbar, 0, nullptr);
             if (consumed > 0) {
                 const long long q = consumed - 1;
                 if (!hx_wait(&empty[q % S], (uint32_t)((q / S) & 1), nullptr)) atomicExch(err, 1);
@@ -910,12 +942,18 @@ static int launch_conv_hx(const bf16 *x, const bf16 *w, const float *bias, bf16 
     int *fault = nullptr;
     if (int rc = tc_fault_word(dev, &fault)) return rc;
     if (!attr_done[dev]) {
-        if (cudaFuncSetAttribute(k_conv3x3_hx<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cf::bytes) !=
-                cudaSuccess ||
+        if (cudaFuncSetAttribute(k_conv3x3_hx<NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Cf::bytes) != cudaSuccess ||
+            cudaFuncSetAttribute(k_conv3x3_hx<NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kHxMaxSmem) != cudaSuccess ||
             cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
             return SHK_CUDA_ERROR;
         attr_done[dev] = 1;
     }
+    // the weights stay resident in each CTA where they fit beside the halo stages (SHK_NN_HX_STREAM=1:
+    // always restage them with every chunk)
+    const char *ev = getenv("SHK_NN_HX_STREAM");
+    const bool res = !(ev && atoi(ev) != 0) && Cf::res_bytes(Cin) <= kHxMaxSmem;
     CUtensorMap mx, mw;
     const cuuint64_t xd[4] = {(cuuint64_t)Cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
     const cuuint64_t xs[3] = {(cuuint64_t)Cin * 2, (cuuint64_t)W * Cin * 2, (cuuint64_t)H * W * Cin * 2};
@@ -932,7 +970,12 @@ static int launch_conv_hx(const bf16 *x, const bf16 *w, const float *bias, bf16 
         return SHK_OK;
     const long long tiles = (long long)N * ((W + 8 * Cf::MT - 1) / (8 * Cf::MT)) * ((H + kHxRows - 1) / kHxRows);
     const int grid = (int)(tiles < sms[dev] ? tiles : sms[dev]);
-    k_conv3x3_hx<NT><<<grid, kHxThreads, Cf::bytes, s>>>(mx, mw, bias, y, Yf, N, H, W, Cin, Cout, relu, flip, fault);
+    if (res)
+        k_conv3x3_hx<NT, true><<<grid, kHxThreads, Cf::res_bytes(Cin), s>>>(mx, mw, bias, y, Yf, N, H, W, Cin, Cout,
+                                                                           relu, flip, fault);
+    else
+        k_conv3x3_hx<NT, false><<<grid, kHxThreads, Cf::bytes, s>>>(mx, mw, bias, y, Yf, N, H, W, Cin, Cout, relu,
+                                                                    flip, fault);
     *launched = true;
     return cudaGetLastError() == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
 }

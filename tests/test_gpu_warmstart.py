@@ -43,8 +43,9 @@ def ws(shk, cuda):
                                          (128, 256, 1, 20, 20), (32, 8, 1, 13, 11), (256, 128, 2, 35, 70),
                                          (64, 16, 3, 5, 3)])
 def test_tensor_core_convolution(ws, cuda, monkeypatch, ci, co, N, H, W):
-    """The three convolution forms -- tcgen05 on TMA-loaded halo tiles (the default), tcgen05 with
-    per-tap gathered A tiles (SHK_NN_TC_GATHER=1), mma.sync (SHK_NN_MMA_SYNC=1) -- forward with bias
+    """The convolution forms -- tcgen05 on TMA-loaded halo tiles with the layer's weights resident in
+    each CTA where they fit (the default) or restaged with every chunk (SHK_NN_HX_STREAM=1), tcgen05
+    with per-tap gathered A tiles (SHK_NN_TC_GATHER=1), mma.sync (SHK_NN_MMA_SYNC=1) -- forward with bias
     and ReLU and the flipped input-gradient form, against the oracle and each other: images whose
     sides are not multiples of the 16 x 8 M tile, several images, 16-channel input (Cin = 16), Cout
     padded to the 16-wide N tile (Cout = 8), the 256-wide tile.  All accumulate BF16 products in
@@ -59,11 +60,13 @@ def test_tensor_core_convolution(ws, cuda, monkeypatch, ci, co, N, H, W):
     wb = torch.from_numpy(Wf).cuda().to(torch.bfloat16)
     Xn, Wn = X.float().cpu().numpy(), wb.float().cpu().numpy()
     out = {}
-    for form in ("tc", "gather", "mma_sync"):
+    for form in ("tc", "stream", "gather", "mma_sync"):
         if form == "mma_sync":
             monkeypatch.setenv("SHK_NN_MMA_SYNC", "1")
         if form == "gather":
             monkeypatch.setenv("SHK_NN_TC_GATHER", "1")
+        if form == "stream":
+            monkeypatch.setenv("SHK_NN_HX_STREAM", "1")
         Yf = torch.empty((N, H, W, co), dtype=torch.float32, device="cuda")
         Yb = torch.empty((N, H, W, co), dtype=torch.bfloat16, device="cuda")
         assert L.shk_nn_conv3x3(ws._p(X), ws._p(wb), ws._fp(bias), ws._p(Yb), ws._fp(Yf), N, H, W, ci, co, 1, 0,
@@ -77,12 +80,14 @@ def test_tensor_core_convolution(ws, cuda, monkeypatch, ci, co, N, H, W):
         out[form] = (Yf.cpu().numpy(), Yb.float().cpu().numpy(), None if dX is None else dX.cpu().numpy())
         monkeypatch.delenv("SHK_NN_MMA_SYNC", raising=False)
         monkeypatch.delenv("SHK_NN_TC_GATHER", raising=False)
+        monkeypatch.delenv("SHK_NN_HX_STREAM", raising=False)
     fault = C.c_int(-1)
     assert L.shk_nn_conv_fault(C.byref(fault)) == 0 and fault.value == 0
     ref = no.conv3x3(Xn, Wn, bias.cpu().numpy(), relu=True)
     assert rel(out["tc"][0], ref) < 1e-5
     assert rel(out["tc"][0], out["mma_sync"][0]) < 1e-5
     assert rel(out["gather"][0], ref) < 1e-5 and rel(out["mma_sync"][0], ref) < 1e-5
+    assert np.array_equal(out["stream"][0], out["tc"][0])  # the same MMAs, weights staged differently
     assert np.array_equal(out["tc"][1], no.bf16(out["tc"][0]))  # the BF16 output is the rounded Float32 one
     if out["tc"][2] is not None:
         # each form's input gradient from its own BF16 forward output (the forms' outputs may differ
