@@ -1264,6 +1264,10 @@ __global__ void __launch_bounds__(128) k_mg_up_m(Lv L, const TB *b, const float 
 // ---------------------------------------------------------------------------------------------
 constexpr size_t kBottomBytesPerCell = 7 * sizeof(float) + 1;
 constexpr size_t kBottomBytes = 200 * 1024;
+// The one-block bottom kernel takes the levels of at most this many cells in all: with 1400 (the
+// levels up to 32 x 32) one multigrid iteration at 4096^2 measured 590 us against 595 us with every
+// level that fits its shared memory (up to 64 x 64), which the tile kernels then spread over all SMs.
+constexpr long long kBottomMaxCells = 1400;
 
 struct BottomLevel {
     int nx, ny, off;  // offset of this level's cells in the shared arrays
@@ -1702,13 +1706,14 @@ static int fused_grid(const Ctx *c, const MgLevel &m) {
     return (int)std::max(1LL, std::min({tiles, (long long)c->max_blocks, (long long)c->num_sms * 6}));
 }
 
-// First level >= 1 from which the rest of the hierarchy fits the bottom kernel's shared memory.
+// First level >= 1 from which the rest of the hierarchy fits the bottom kernel's shared memory and
+// holds at most kBottomMaxCells cells.
 static int bottom_level(const Ctx *c) {
     long long rest = 0;
     int lb = c->mg_levels - 1;
     for (int l = c->mg_levels - 1; l >= 1; l--) {
         rest += (long long)c->mg[l].nx * c->mg[l].ny;
-        if ((size_t)rest * kBottomBytesPerCell > kBottomBytes) break;
+        if ((size_t)rest * kBottomBytesPerCell > kBottomBytes || rest > kBottomMaxCells) break;
         lb = l;
     }
     return lb;
