@@ -166,7 +166,7 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, u
 // ---------------------------------------------------------------------------------------------
 struct CgView {
     int done, first;
-    double alpha, beta;
+    double alpha, beta, alpha_prev;
 };
 
 __device__ __forceinline__ CgView block_cg_view(const CgDev *cg) {
@@ -176,6 +176,7 @@ __device__ __forceinline__ CgView block_cg_view(const CgDev *cg) {
         v.first = cg->first;
         v.alpha = cg->alpha;
         v.beta = cg->beta;
+        v.alpha_prev = cg->alpha_prev;
     }
     __syncthreads();
     return v;

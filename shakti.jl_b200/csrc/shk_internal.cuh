@@ -59,6 +59,10 @@ struct CgDev {
     int cont;        // init continues the previous search direction instead of restarting
     unsigned int trips;  // trips of the device-side iteration loop (bounded)
     int fault;           // set by a kernel whose bounded wait for a tile copy ran out
+    // paired x updates of the multigrid form: alpha of the previous iteration, and which search
+    // direction's x update is still to be applied (0 none, 1 + the p buffer's index)
+    double alpha_prev;
+    int x_pending;
 };
 
 struct ChebDev {
@@ -293,6 +297,7 @@ int cg_jac_matvec(Ctx *c, int par, const double *r, const double *p_old, double 
 int mg_cg_matvec(Ctx *c, int par, const double *aP, const double *aE, const double *aN, const double *z,
                  const double *p_old, double *p_new, double *Ap, CgDev *cg, double eps_curv, bool *launched);
 int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, const double *p, const double *Ap,
-                          double *z, CgDev *cg);
+                          double *z, CgDev *cg, const double *p_prev = nullptr, int mode = 0, int pbuf = 0);
+int mg_catch_up(Ctx *c, double *x, CgDev *cg);
 
 } // namespace shk

@@ -909,7 +909,10 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
                 if (launched) {
                     T *rb[2] = {r, c->r2};
                     c->launches += 1;
-                    return mg_apply_fused_update(c, rb[par], rb[par ^ 1], x, p_new, Ap, z, cgd);
+                    // x updated once per two iterations: the first of a pair (par == p_parity)
+                    // leaves it pending, the second applies both directions' updates
+                    return mg_apply_fused_update(c, rb[par], rb[par ^ 1], x, p_new, Ap, z, cgd, p_old,
+                                                 par == p_parity ? 1 : 2, par ^ 1);
                 }
             }
         }
@@ -955,6 +958,13 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
         return SHK_OK;
     };
 
+    // a pending x update of the paired form, applied after the last iteration
+    auto catch_up = [&]() -> int {
+        if constexpr (std::is_same<T, double>::value) {
+            if (fuse_update && !jac && !lapl) return mg_catch_up(c, x, cgd);
+        }
+        return SHK_OK;
+    };
     // Graphs are keyed by everything that their kernel arguments depend on within one context.
     const long long key_base = ((long long)(lapl != nullptr) << 41) | ((long long)(sizeof(T) == 4) << 40) |
                                ((long long)o->precond << 32) | ((long long)deg << 8);
@@ -1043,6 +1053,7 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
                 c->launches += slot->launches * (long long)cgh->trips;
                 if (!cgh->done) return fail(c, SHK_CUDA_ERROR, "cg device loop reached its trip bound before stopping");
             }
+            if ((rc = catch_up())) return rc;
             if (iters_out) *iters_out = (long)cgh->iter;
             return SHK_OK;
         }
@@ -1094,6 +1105,7 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
         if (cgh->iter > cgh->itmax + 4 || enq > cgh->itmax + 2LL * batch_max + 8)
             return fail(c, SHK_CUDA_ERROR, "cg iteration accounting overran itmax");
     }
+    if ((rc = catch_up())) return rc;
     if (iters_out) *iters_out = (long)cgh->iter;
     return SHK_OK;
 }

@@ -376,10 +376,17 @@ __device__ __forceinline__ float ax_sm(const FusedSm &S, const float (&X)[kFSH][
 // FB (level 0 of an iteration): the outer CG's x/r update (k_cg_B's arithmetic, unfused) is done
 // here: the staged rhs is r_new = r + (-alpha) Ap, and the tile's own cells write r_new to the
 // other r buffer (never the one neighbouring blocks read) and x += alpha p.
+// The outer CG's x/r update folded into the level-0 descending kernel.  mode 0: x += alpha p;
+// mode 1 (first iteration of a pair): x untouched, the update recorded as pending; mode 2 (second):
+// x = (x + alpha_prev p_prev) + alpha p -- the same two roundings as two single updates, so the
+// pair gives x bit for bit, and one read and write of x per two iterations.
 struct FusedB {
     const double *Ap, *p;
     double *x, *r_out;
     double alpha;
+    const double *p_prev;
+    int mode, pbuf;  // pbuf: index of the context's p buffer that p is (mode 1)
+    double alpha_prev;
 };
 
 template <typename TB, bool UP, bool FB = false>
@@ -790,6 +797,8 @@ __global__ void __launch_bounds__(256, 3) k_mg_down_t(const __grid_constant__ Tm
         const CgView cv = block_cg_view(cg);
         if (cv.done) return;
         fbv.alpha = cv.alpha;
+        fbv.alpha_prev = cv.alpha_prev;
+        if (fbv.mode && blockIdx.x == 0 && threadIdx.x == 0) cg->x_pending = fbv.mode == 1 ? 1 + fbv.pbuf : 0;
     } else {
         if (cg_finished(L.done)) return;
     }
@@ -814,9 +823,14 @@ __global__ void __launch_bounds__(256, 3) k_mg_down_t(const __grid_constant__ Tm
             inside = gx < L.nx && gy < L.ny;  // nx is even: both cells of the pair, or neither
             q = (size_t)gx + (size_t)gy * L.nx;
             if constexpr (FB) {
-                if (inside) {
+                if (inside && fbv.mode != 1) {
                     xq = *reinterpret_cast<const double2 *>(fbv.x + q);
                     pq = *reinterpret_cast<const double2 *>(fbv.p + q);
+                    if (fbv.mode == 2) {
+                        const double2 pp = *reinterpret_cast<const double2 *>(fbv.p_prev + q);
+                        xq = make_double2(__dadd_rn(xq.x, __dmul_rn(fbv.alpha_prev, pp.x)),
+                                          __dadd_rn(xq.y, __dmul_rn(fbv.alpha_prev, pp.y)));
+                    }
                 }
             }
         },
@@ -832,9 +846,10 @@ __global__ void __launch_bounds__(256, 3) k_mg_down_t(const __grid_constant__ Tm
                     bq.y = __dadd_rn(bq.y, __dmul_rn(-fbv.alpha, ap.y));
                     if (tile && inside) {
                         *reinterpret_cast<double2 *>(fbv.r_out + q) = bq;
-                        *reinterpret_cast<double2 *>(fbv.x + q) =
-                            make_double2(__dadd_rn(xq.x, __dmul_rn(fbv.alpha, pq.x)),
-                                         __dadd_rn(xq.y, __dmul_rn(fbv.alpha, pq.y)));
+                        if (fbv.mode != 1)
+                            *reinterpret_cast<double2 *>(fbv.x + q) =
+                                make_double2(__dadd_rn(xq.x, __dmul_rn(fbv.alpha, pq.x)),
+                                             __dadd_rn(xq.y, __dmul_rn(fbv.alpha, pq.y)));
                     }
                 }
                 pair_load(P, O);
@@ -1051,6 +1066,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_matvec_t(const __grid_constant__ 
             cg->done = 1;
             cg->status = SHK_BREAKDOWN;
         } else {
+            cg->alpha_prev = cg->alpha;
             cg->alpha = __ddiv_rn(cg->gamma, pAp);
         }
     }
@@ -2274,8 +2290,27 @@ int cg_jac_matvec(Ctx *c, int par, const double *r, const double *p_old, double 
 // r_new = r_in - alpha Ap into r_out, x += alpha p, then z = M^-1 r_new and the CG's r'z, r'r.
 bool mg_fuses_cg_update(const Ctx *c) { return marching(c) ? false : fused(c) && c->mg_levels > 1; }
 
+// After a solve whose last iteration was the first of a pair: x += alpha p for the pending p (the
+// rounding of the single update).  Returns at once when nothing is pending.
+__global__ void k_cg_catchup(long long n, double *x, const double *p0, const double *p1, const CgDev *cg) {
+    const int pend = cg->x_pending;
+    if (!pend) return;
+    const double *p = pend == 1 ? p0 : p1;
+    const double a = cg->alpha;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] = __dadd_rn(x[i], __dmul_rn(a, p[i]));
+}
+
+int mg_catch_up(Ctx *c, double *x, CgDev *cg) {
+    k_cg_catchup<<<c->num_sms * 8, 256, 0, c->stream>>>((long long)c->nx * c->ny, x, c->p[0], c->p[1], cg);
+    c->launches++;
+    return check_launch(c, "cg pending x update");
+}
+
+// mode / p_prev / pbuf: the paired x update of FusedB (mode 0: x updated every iteration); the
+// pairing needs the TMA-staged kernel, whose matvec records alpha_prev.
 int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, const double *p, const double *Ap,
-                          double *z, CgDev *cg) {
+                          double *z, CgDev *cg, const double *p_prev, int mode, int pbuf) {
     MgLevel &m = c->mg[0];
     const Lv L = level_view(m, &cg->done);
     MgLevel &g = c->mg[1];
@@ -2287,7 +2322,7 @@ int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, 
         const int gd = tma_grid(c, T, TK_DOWN0_FB, m), gu = tma_grid(c, T, TK_UP0, m);
         k_mg_down_t<double, true><<<gd, 256, TLayout<double, false, true>::bytes, c->stream>>>(
             tma_args(T, 0, *r_map(c, T, r_in), &T->Ap, nullptr), L, m.x[0], g.nx, g.ny, g.b,
-            FusedB{Ap, p, x, r_out, 0.0}, cg);
+            FusedB{Ap, p, x, r_out, 0.0, p_prev, mode, pbuf, 0.0}, cg);
         c->launches++;
         int gres = 0;
         int rc = vcycle(c, 1, cg, &gres);
@@ -2298,6 +2333,7 @@ int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, 
         c->launches++;
         return check_launch(c, "multigrid apply");
     }
+    if (mode) return fail(c, SHK_CUDA_ERROR, "paired x updates need the TMA-staged level-0 kernel");
     const int gt = fused_grid(c, m);
     k_mg_down<double, true><<<gt, 256, 0, c->stream>>>(L, r_in, m.x[0], g.nx, g.ny, g.b,
                                                         FusedB{Ap, p, x, r_out, 0.0}, cg);
