@@ -236,13 +236,14 @@ def run_steps(shk, sim, n, record=None):
 def mg_vcycle_bytes(nx, ny, fused=True):
     """Algorithmic bytes of one V-cycle (all levels, nu = 2 sweeps per side).
     Fused level kernels (the default): level 0 (Float64 residual in, Float64 z out), per fine cell,
-    descending half 70 B with the CG's x/r update folded in (r, Ap, p, x 32 B, activity flag 1,
-    operator wD dP aE aN 16 in; new r 8, x 8, the level's iterate 4, coarse rhs 1 out) and
-    ascending half 38 B (iterate 4, coarse iterate 1, flag 1, operator 16, r 8 in; z 8 out); each
-    coarse level above the bottom, per cell, 26 + 30 B (Float32 rhs).  Per-sweep kernels: level 0
-    17 + 33 + 26 + 34 + 37 B, coarse levels 13 + 29 + 22 + 30 + 29 B.  The levels that fit in one
-    block's shared memory (29 B per cell, 200 KiB) are read once (operator 17 B + rhs 4 B per
-    cell) and level lb's result written once (4 B per cell)."""
+    descending half with the CG's r update folded in and its x update once per two iterations --
+    62 B on average: r, Ap 16 B, activity flag 1, operator wD dP aE aN 16 in, new r 8, the level's
+    iterate 4, coarse rhs 1 out, and every second iteration p, p_prev, x 24 B in and x 8 B out --
+    and ascending half 38 B (iterate 4, coarse iterate 1, flag 1, operator 16, r 8 in; z 8 out);
+    each coarse level above the bottom, per cell, 26 + 30 B (Float32 rhs).  Per-sweep kernels:
+    level 0 17 + 33 + 26 + 34 + 37 B, coarse levels 13 + 29 + 22 + 30 + 29 B.  The levels the
+    one-block bottom kernel takes (at most 1400 cells in all, 29 B per cell within 200 KiB) are
+    read once (operator 17 B + rhs 4 B per cell) and level lb's result written once (4 B)."""
     dims = [(nx, ny)]
     while dims[-1] != (1, 1):
         a, b = dims[-1]
@@ -252,10 +253,10 @@ def mg_vcycle_bytes(nx, ny, fused=True):
     rest = 0
     for l in range(len(dims) - 1, 0, -1):
         rest += cells[l]
-        if rest * 29 > 200 * 1024:
+        if rest * 29 > 200 * 1024 or rest > 1400:
             break
         lb = l
-    top, coarse = (108, 56) if fused else (147 + 48, 123)  # per-sweep: plus k_cg_B's 48 B
+    top, coarse = (100, 56) if fused else (147 + 48, 123)  # per-sweep: plus k_cg_B's 48 B
     total = top * cells[0] if len(dims) > 1 else 37 * cells[0]
     for l in range(1, lb):
         total += coarse * cells[l]
