@@ -215,6 +215,8 @@ SHK_API int shk_create(int nx, int ny, double lx, double ly, void *stream, void 
     // SHK_MG_CLUSTER=1: the coarse levels from the finest one whose row slabs fit eight CTAs' shared
     // memory run on one thread-block cluster (default: tile kernels down to the one-block bottom)
     if (const char *v = getenv("SHK_MG_CLUSTER")) c->mg_cluster = atoi(v) != 0;
+    // SHK_MG_PAIR_X=0: the multigrid form's x updated in every iteration (the same x bit for bit)
+    if (const char *v = getenv("SHK_MG_PAIR_X")) c->mg_pair_x = atoi(v) != 0;
     // SHK_CG_GRAPHS: 0 issues each CG iteration's kernels directly, 1 replays one CUDA graph per
     // iteration in host-sized batches, 2 (default) runs the whole iteration loop as one graph with a
     // device-side WHILE node

@@ -155,6 +155,7 @@ struct Ctx {
     int mg_fused = 1;        // nu = 2 level kernels: 1 tile (default), 2 warp-marching, 0 per-sweep
     int mg_tma = 1;          // tile kernels stage through TMA copies where the level's pitch allows
     bool mg_cluster = false;  // the coarse levels on one thread-block cluster (measured slower; opt-in)
+    bool mg_pair_x = true;    // the outer CG's x updated once per two iterations (bit-identical x)
     struct MgTma *mg_maps = nullptr;  // the levels' tensor maps (built on first use)
     struct CgTma *cg_maps = nullptr;  // the plain Jacobi CG's tensor maps (built before its first capture)
     int max_blocks = 0;

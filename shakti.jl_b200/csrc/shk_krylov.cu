@@ -912,7 +912,7 @@ static int cg_core(Ctx *c, const shk_cg_opts *o, CgDev *cgd, CgDev *cgh, const T
                     // x updated once per two iterations: the first of a pair (par == p_parity)
                     // leaves it pending, the second applies both directions' updates
                     return mg_apply_fused_update(c, rb[par], rb[par ^ 1], x, p_new, Ap, z, cgd, p_old,
-                                                 par == p_parity ? 1 : 2, par ^ 1);
+                                                 !c->mg_pair_x ? 0 : (par == p_parity ? 1 : 2), par ^ 1);
                 }
             }
         }

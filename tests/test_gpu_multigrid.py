@@ -128,6 +128,24 @@ def test_cluster_coarse_levels_match_tile_levels_and_bottom(shk, cuda, monkeypat
     assert relerr(h_c, h_b) <= 1e-7, relerr(h_c, h_b)
 
 
+@pytest.mark.parametrize("itmax", [0, 3, 4])
+def test_paired_x_updates_are_bit_identical(shk, cuda, monkeypatch, itmax):
+    """The outer CG's x updated once per two iterations (the second of a pair adds both directions'
+    terms in the single updates' order; a pending term is added after the last iteration) against x
+    updated in every iteration (SHK_MG_PAIR_X=0): the same heads bit for bit and the same iteration
+    count -- for a full solve, an odd iteration count (the pending term applied at the end) and an
+    even one, and in each CG launch mode."""
+    w = tma_workload(shk, 512, 360)
+    rtol = 1e-8 if itmax == 0 else 0.0
+    for graphs in ("0", "1", "2"):
+        h_p, s_p = solve(shk, w, {"SHK_MG_PAIR_X": "1", "SHK_CG_GRAPHS": graphs}, monkeypatch, itmax=itmax, rtol=rtol)
+        h_i, s_i = solve(shk, w, {"SHK_MG_PAIR_X": "0", "SHK_CG_GRAPHS": graphs}, monkeypatch, itmax=itmax, rtol=rtol)
+        assert s_p.status == s_i.status and s_p.niter == s_i.niter
+        if itmax:
+            assert s_p.niter == itmax
+        assert np.array_equal(h_p, h_i)
+
+
 def test_tma_multigrid_run_matches_oracle(shk, orc, cuda, monkeypatch):
     """The TMA-staged multigrid form against the oracle (not only against the LDG staging) at
     512 x 360, where levels 0-2 stage through TMA: one linear solve at rel-res 1e-12 on the GROUNDED
