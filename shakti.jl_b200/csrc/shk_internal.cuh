@@ -147,10 +147,8 @@ struct Ctx {
     MgLevel mg[kMgMaxLevels];
     int mg_levels = 0;
     int mg_nu = 2;           // damped-Jacobi sweeps before and after each coarse correction
-    float mg_omega = 0.8f;   // Jacobi damping
-    // Coarse-correction scaling.  Piecewise-constant (unsmoothed) aggregation under-corrects the
-    // smooth error; over-correcting by 1.6 (inside (0, 2), where the symmetric two-grid cycle stays
-    // a positive definite preconditioner) halves the outer CG's iterations at 4096^2.
+    // Jacobi damping and coarse-correction scaling, set per grid size by mg_default_weights.
+    float mg_omega = 0.8f;
     float mg_omega_c = 1.6f;
     int mg_fused = 1;        // nu = 2 level kernels: 1 tile (default), 2 warp-marching, 0 per-sweep
     int mg_tma = 1;          // tile kernels stage through TMA copies where the level's pitch allows
