@@ -170,18 +170,36 @@ SHK_API const char *shk_status_string(int s) {
     }
 }
 
-// The multigrid cycle's Jacobi damping omega and coarse-correction scaling omega_c by grid size.
+// The multigrid cycle's smoothing weights and coarse-correction scaling omega_c by grid size.
 // Piecewise-constant (unsmoothed) aggregation under-corrects the smooth error, so every coarse
 // correction is scaled by omega_c inside (0, 2), where the symmetric cycle stays a positive definite
-// preconditioner; the deeper the hierarchy, the smaller the best scaling.  Measured outer CG
-// iterations over 10 timesteps of the seasonal workloads (Picard re-solves), (0.8, 1.6) / (0.9, 1.3)
-// / (0.9, 1.45): 4096^2 3182 / 2163 / 2309 (at 1.4); 2048^2 2089 / 1729 / 1788; 1024^2 1600 / 1520 /
-// 1448; the ragged 128^2-1024^2 ensemble (20 steps) 266059 / 320142 / 279021.  Undamped Jacobi
-// (omega = 1) leaves the highest frequencies: 9626 at 4096^2.
+// preconditioner; the deeper the hierarchy, the smaller the best scaling.  The two sweeps on each
+// side take either one damping omega (damped Jacobi) or the degree-2 Chebyshev pair of weights.
+// Measured outer CG iterations over 10 timesteps of the seasonal workloads (Picard re-solves):
+//   damped Jacobi (0.8, 1.6) / (0.9, 1.3) / (0.9, 1.45), Chebyshev pair with the size's omega_c:
+//   4096^2: 3182 / 2163 / 2309 (at 1.4) / 2003;   2048^2: 2089 / 1729 / 1788 / 1623;
+//   1024^2: 1600 / 1520 / 1448 / 1310;   the ragged 128^2-1024^2 ensemble (20 steps, Jacobi only):
+//   266059 / 320142 / 279021.  Undamped Jacobi (omega = 1) leaves the highest frequencies: 9626 at
+//   4096^2.  Grids of at most 512 cells a side keep damped Jacobi (0.8, 1.6).
+static void mg_chebyshev_weights(Ctx *c) {
+    // the reciprocals of the two roots of the degree-2 Chebyshev polynomial for the interval
+    // [0.45, 1.8] of the spectrum of D^-1 A; the smaller weight first before the coarse correction
+    // and last after it
+    const double lo = 0.45, hi = 1.8, mid = 0.5 * (hi + lo), half = 0.5 * (hi - lo) * std::sqrt(0.5);
+    const double tau1 = 1.0 / (mid + half), tau2 = 1.0 / (mid - half);
+    c->mg_omega = (float)tau1;
+    c->mg_s2 = (float)(tau2 / tau1);
+}
+
 static void mg_default_weights(Ctx *c) {
     const int n = std::max(c->nx, c->ny);
-    c->mg_omega = n > 512 ? 0.9f : 0.8f;
     c->mg_omega_c = n > 1024 ? 1.3f : (n > 512 ? 1.45f : 1.6f);
+    if (n > 512) {
+        mg_chebyshev_weights(c);
+    } else {
+        c->mg_omega = 0.8f;
+        c->mg_s2 = 1.0f;
+    }
 }
 
 SHK_API int shk_create(int nx, int ny, double lx, double ly, void *stream, void **ctx_out) {
@@ -223,7 +241,21 @@ SHK_API int shk_create(int nx, int ny, double lx, double ly, void *stream, void 
     }
     mg_default_weights(c);
     if (const char *v = getenv("SHK_MG_NU")) c->mg_nu = std::max(1, atoi(v));
-    if (const char *v = getenv("SHK_MG_OMEGA")) c->mg_omega = (float)atof(v);
+    // SHK_MG_CHEB=1: the Chebyshev pair on every grid size; 0: damped Jacobi (omega 0.9 above 512
+    // cells a side, 0.8 below)
+    if (const char *v = getenv("SHK_MG_CHEB")) {
+        if (atoi(v) != 0) {
+            mg_chebyshev_weights(c);
+        } else {
+            c->mg_omega = std::max(c->nx, c->ny) > 512 ? 0.9f : 0.8f;
+            c->mg_s2 = 1.0f;
+        }
+    }
+    // SHK_MG_OMEGA: damped Jacobi with this damping
+    if (const char *v = getenv("SHK_MG_OMEGA")) {
+        c->mg_omega = (float)atof(v);
+        c->mg_s2 = 1.0f;
+    }
     if (const char *v = getenv("SHK_MG_OMEGA_C")) c->mg_omega_c = (float)atof(v);
     if (const char *v = getenv("SHK_MG_FUSED")) c->mg_fused = std::min(2, std::max(0, atoi(v)));
     if (const char *v = getenv("SHK_MG_TMA")) c->mg_tma = atoi(v) != 0;

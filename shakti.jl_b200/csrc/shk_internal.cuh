@@ -150,6 +150,9 @@ struct Ctx {
     // Jacobi damping and coarse-correction scaling, set per grid size by mg_default_weights.
     float mg_omega = 0.8f;
     float mg_omega_c = 1.6f;
+    // The weight of the two sweeps next to each coarse correction relative to mg_omega: 1 for
+    // damped Jacobi; tau2/tau1 for the degree-2 Chebyshev pair (mg_omega = tau1).
+    float mg_s2 = 1.0f;
     int mg_fused = 1;        // nu = 2 level kernels: 1 tile (default), 2 warp-marching, 0 per-sweep
     int mg_tma = 1;          // tile kernels stage through TMA copies where the level's pitch allows
     bool mg_cluster = false;  // the coarse levels on one thread-block cluster (measured slower; opt-in)

@@ -213,6 +213,11 @@ struct Lv {
     const float *aE, *aN, *dP, *wD;
     const uint8_t *act;
     const int *done;  // the outer CG's stop flag: V-cycles issued after the stop do no work
+    // The weight of the two sweeps next to the coarse correction (the last one before it, the
+    // first one after it) relative to wD: 1 for plain damped Jacobi; tau2/tau1 for the degree-2
+    // Chebyshev pair (wD = tau1/aP).  The pre- and post-smoothers apply the same two factors, so the
+    // cycle stays symmetric.
+    float s2 = 1.0f;
 };
 
 // The outer CG's stop flag, read once per block (all threads must call it first).
@@ -244,14 +249,14 @@ __global__ void k_mg_pre0(Lv L, const TB *b, float *x) {
     if (inside) x[k] = L.wD[k] * (float)b[k];
 }
 
-// One damped-Jacobi sweep: xo = xi + wD (b - A xi).
+// One damped-Jacobi sweep: xo = xi + (s wD) (b - A xi).
 template <typename TB>
-__global__ void k_mg_sweep(Lv L, const TB *b, const float *xi, float *xo) {
+__global__ void k_mg_sweep(Lv L, const TB *b, const float *xi, float *xo, float s) {
     CELL2D();
     if (!inside) return;
     const float xc = xi[k];
     const float ax = lapl_apply(L, ix, iy, k, xc, [&](size_t q) { return xi[q]; });
-    xo[k] = xc + L.wD[k] * ((float)b[k] - ax);
+    xo[k] = xc + __fmul_rn(L.wD[k], s) * ((float)b[k] - ax);
 }
 
 // Restriction of the residual: bc(C) = sum over the active fine cells of aggregate C of (b - A x).
@@ -285,10 +290,10 @@ __device__ __forceinline__ float prolonged(const Lv &L, const float *xi, const f
 }
 
 // Prolongation fused with the first post-smoothing sweep:
-//   xt = xi + omega_c P xc,  xo = xt + wD (b - A xt).
+//   xt = xi + omega_c P xc,  xo = xt + (s wD) (b - A xt).
 template <typename TB>
 __global__ void k_mg_prolong_sweep(Lv L, const TB *b, const float *xi, const float *xc, int nxc, float wc,
-                                   float *xo) {
+                                   float *xo, float s) {
     CELL2D();
     if (!inside) return;
     const float xk = prolonged(L, xi, xc, nxc, wc, ix, iy, k);
@@ -297,7 +302,7 @@ __global__ void k_mg_prolong_sweep(Lv L, const TB *b, const float *xi, const flo
     if (ix > 0) y += L.aE[k - 1] * (xk - prolonged(L, xi, xc, nxc, wc, ix - 1, iy, k - 1));
     if (iy < L.ny - 1) y += L.aN[k] * (xk - prolonged(L, xi, xc, nxc, wc, ix, iy + 1, k + L.nx));
     if (iy > 0) y += L.aN[k - L.nx] * (xk - prolonged(L, xi, xc, nxc, wc, ix, iy - 1, k - L.nx));
-    xo[k] = xk + L.wD[k] * ((float)b[k] - y);
+    xo[k] = xk + __fmul_rn(L.wD[k], s) * ((float)b[k] - y);
 }
 
 // Last post-smoothing sweep on level 0, writing z in Float64 and finishing the outer CG's r'z:
@@ -434,13 +439,15 @@ __device__ __forceinline__ void stage_level(FusedSm &S, const Lv &L, const TB *b
     }
 }
 
-// One damped-Jacobi sweep XO = XI + wD (b - A XI) over the staged positions within distance 1 of
-// the tile.
-__device__ __forceinline__ void sweep_sm(FusedSm &S, const float (&XI)[kFSH][kFSW], float (&XO)[kFSH][kFSW]) {
+// One damped-Jacobi sweep XO = XI + (s wD) (b - A XI) over the staged positions within distance 1
+// of the tile.
+__device__ __forceinline__ void sweep_sm(FusedSm &S, const float (&XI)[kFSH][kFSW], float (&XO)[kFSH][kFSW],
+                                         float s) {
     constexpr int wdt = kFW + 2, hgt = kFH + 2;
     for (int k = threadIdx.x; k < wdt * hgt; k += blockDim.x) {
         const int hx = kFR - 1 + k % wdt, hy = kFR - 1 + k / wdt;
-        XO[hy][hx] = __fmaf_rn(S.wD[hy][hx], __fsub_rn(S.b[hy][hx], ax_sm(S, XI, hx, hy)), XI[hy][hx]);
+        XO[hy][hx] =
+            __fmaf_rn(__fmul_rn(S.wD[hy][hx], s), __fsub_rn(S.b[hy][hx], ax_sm(S, XI, hx, hy)), XI[hy][hx]);
     }
 }
 
@@ -463,7 +470,7 @@ __device__ __forceinline__ void mg_down_body(Blk B, const Lv &L, const TB *b, fl
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
         stage_level<TB, false, FB>(S, L, b, x0, y0, nullptr, nullptr, nullptr, 0, 0.0f, &fbv);
         __syncthreads();
-        sweep_sm(S, S.x0, S.x1);
+        sweep_sm(S, S.x0, S.x1, L.s2);
         __syncthreads();
         // x1 out, and each tile cell's residual (0 on inactive cells) into the x0 array, which
         // the restriction then sums per aggregate
@@ -515,7 +522,7 @@ __device__ __forceinline__ void mg_up_body(Blk B, const Lv &L, const TB *b, cons
         const int x0 = (t % tiles_x) * kFW, y0 = (t / tiles_x) * kFH;
         stage_level<TB, true>(S, L, b, x0, y0, LAST ? r64 : nullptr, xi, xc, nxc, wc);
         __syncthreads();
-        sweep_sm(S, S.x0, S.x1);
+        sweep_sm(S, S.x0, S.x1, L.s2);
         __syncthreads();
         for (int r = ty; r < kFH; r += 8) {
             const int gx = x0 + tx, gy = y0 + r;
@@ -721,8 +728,9 @@ __device__ __forceinline__ float2 pair_ax(const Pair &P, const float *X) {
     return y;
 }
 
-__device__ __forceinline__ void pair_sweep(const Pair &P, const float *XI, float *XO) {
-    st2(XO + P.k, __ffma2_rn(P.W, sub2(P.B, pair_ax(P, XI)), ld2(XI + P.k)));
+__device__ __forceinline__ void pair_sweep(const Pair &P, const float *XI, float *XO, float s) {
+    const float2 w = __fmul2_rn(P.W, make_float2(s, s));
+    st2(XO + P.k, __ffma2_rn(w, sub2(P.B, pair_ax(P, XI)), ld2(XI + P.k)));
 }
 
 // Records a failed wait (the solve stops and reports it).  Before the block returns, thread 0
@@ -859,8 +867,8 @@ __global__ void __launch_bounds__(256, 3) k_mg_down_t(const __grid_constant__ Tm
             prep(P0, true);
             if (has1) prep(P1, false);
             __syncthreads();
-            pair_sweep(P0, X0, X1);
-            if (has1 && P1.sweep) pair_sweep(P1, X0, X1);
+            pair_sweep(P0, X0, X1, L.s2);
+            if (has1 && P1.sweep) pair_sweep(P1, X0, X1, L.s2);
             __syncthreads();
             // residual of the tile pair (0 on inactive cells), x1 out, restriction by shuffle
             const float2 ax = pair_ax(P0, X1);
@@ -923,8 +931,8 @@ __global__ void __launch_bounds__(256, 4) k_mg_up_t(const __grid_constant__ TmaA
             prep(P0);
             if (has1) prep(P1);
             __syncthreads();
-            pair_sweep(P0, X0, X1);
-            if (has1 && P1.sweep) pair_sweep(P1, X0, X1);
+            pair_sweep(P0, X0, X1, L.s2);
+            if (has1 && P1.sweep) pair_sweep(P1, X0, X1, L.s2);
             __syncthreads();
             const int gx = x0 + gx0, gy = y0 + gy0;
             if (gx < L.nx && gy < L.ny) {
@@ -1148,7 +1156,7 @@ __global__ void __launch_bounds__(128) k_mg_down_m(Lv L, const TB *b, float *xo,
             const float x0j = cj.wD * cj.b;
             // x1 at row j-1 (c1, x0a) from x0 at rows j-2 (x0b), j-1, j
             const float ax0 = ax_row(c1, c2.aN, x0a, x0b, x0j);
-            const float x1n = x0a + c1.wD * (c1.b - ax0);
+            const float x1n = x0a + __fmul_rn(c1.wD, L.s2) * (c1.b - ax0);
             // residual at row j-2 (c2, x1a) from x1 at rows j-3 (x1b), j-2, j-1
             if (j - 2 >= y0) {
                 const float ax1 = ax_row(c2, c3.aN, x1a, x1b, x1n);
@@ -1231,7 +1239,7 @@ __global__ void __launch_bounds__(128) k_mg_up_m(Lv L, const TB *b, const float 
             const float xtj = xt_of(cj, fi, co);
             // x2 at row j-1 from xt at rows j-2, j-1, j
             const float axt = ax_row(c1, c2.aN, xta, xtb, xtj);
-            const float x2n = xta + c1.wD * (c1.b - axt);
+            const float x2n = xta + __fmul_rn(c1.wD, L.s2) * (c1.b - axt);
             // final sweep at row j-2 from x2 at rows j-3, j-2, j-1
             if (j - 2 >= y0) {
                 const float ax2 = ax_row(c2, c3.aN, x2a, x2b, x2n);
@@ -1294,6 +1302,7 @@ struct BottomPlan {
     const float *aE[kMgMaxLevels], *aN[kMgMaxLevels], *dP[kMgMaxLevels], *wD[kMgMaxLevels];
     const uint8_t *act[kMgMaxLevels];
     const int *done;
+    float s2;  // Lv::s2
 };
 
 // Every loop over a level runs on a 2D thread map (32 columns x blockDim/32 rows), so no cell's
@@ -1335,18 +1344,21 @@ __device__ __forceinline__ void mg_bottom_body(const BottomPlan &P, const float 
     // Xb[(nu - 1) & 1]; the ascending half (nu sweeps from there) in Xb[(2 nu - 1) & 1] = sY;
     // the coarsest level's exact solve in sX.
     float *Xb[2] = {sX, sY};
-    auto sweep = [&](int l, int cur) {
+    auto sweep = [&](int l, int cur, float w) {
         const int nx = P.lv[l].nx, ny = P.lv[l].ny, o = P.lv[l].off;
         const float *XI = Xb[cur];
         float *XO = Xb[cur ^ 1];
         for (int iy = ty; iy < ny; iy += nty)
             for (int ix = tx; ix < nx; ix += 32) {
                 const int i = ix + iy * nx;
-                XO[o + i] = XI[o + i] + sP[o + i] * (sB[o + i] - Ax(l, XI, ix, iy, i));
+                XO[o + i] = XI[o + i] + __fmul_rn(sP[o + i], w) * (sB[o + i] - Ax(l, XI, ix, iy, i));
             }
         __syncthreads();
         return cur ^ 1;
     };
+    // the last sweep before and the first after the coarse correction take the factor s2
+    auto wpre = [&](int k) { return k == nu - 1 ? P.s2 : 1.0f; };
+    auto wpost = [&](int k) { return k == 0 && nu > 1 ? P.s2 : 1.0f; };
     const int L = P.nlev;
     const int cur_down = (nu - 1) & 1, cur_up = 1;
     for (int l = 0; l < L - 1; l++) {  // descend
@@ -1354,7 +1366,7 @@ __device__ __forceinline__ void mg_bottom_body(const BottomPlan &P, const float 
         for (int i = tid; i < n; i += nt) sX[o + i] = sP[o + i] * sB[o + i];
         __syncthreads();
         int cur = 0;
-        for (int s = 1; s < nu; s++) cur = sweep(l, cur);
+        for (int s = 1; s < nu; s++) cur = sweep(l, cur, wpre(s));
         const float *XC = Xb[cur];
         const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, nxc = P.lv[l + 1].nx, nyc = P.lv[l + 1].ny, oc = P.lv[l + 1].off;
         for (int J = ty; J < nyc; J += nty)
@@ -1388,7 +1400,7 @@ __device__ __forceinline__ void mg_bottom_body(const BottomPlan &P, const float 
             }
         __syncthreads();
         int cur = cur_down;
-        for (int s = 0; s < nu; s++) cur = sweep(l, cur);
+        for (int s = 0; s < nu; s++) cur = sweep(l, cur, wpost(s));
     }
     const float *X0 = Xb[L == 1 ? 0 : cur_up];
     for (int i = tid; i < P.lv[0].nx * P.lv[0].ny; i += nt) x_top[i] = X0[i];
@@ -1428,6 +1440,7 @@ struct ClusterPlan {
     const float *aE[kMgMaxLevels], *aN[kMgMaxLevels], *dP[kMgMaxLevels], *wD[kMgMaxLevels];
     const uint8_t *act[kMgMaxLevels];
     const int *done;
+    float s2;  // Lv::s2
 };
 
 __device__ __forceinline__ uint32_t cl_rank() {
@@ -1540,7 +1553,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterPlan P
         }
         return y;
     };
-    auto sweep_d = [&](int l, int cur) {
+    auto sweep_d = [&](int l, int cur, float w) {
         int s, e;
         rows(l, rank, s, e);
         const int nx = P.lv[l].nx;
@@ -1549,11 +1562,14 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterPlan P
         for (int iy = s + ty; iy < e; iy += nty)
             for (int ix = tx; ix < nx; ix += 32) {
                 const int i = at(l, s, ix, iy);
-                XO[i] = XI[i] + sP[i] * (sB[i] - Axd(l, XI, ix, iy, i, s, e));
+                XO[i] = XI[i] + __fmul_rn(sP[i], w) * (sB[i] - Axd(l, XI, ix, iy, i, s, e));
             }
         cl_sync();
         return cur ^ 1;
     };
+    // the last sweep before and the first after the coarse correction take the factor s2
+    auto wpre = [&](int k) { return k == nu - 1 ? P.s2 : 1.0f; };
+    auto wpost = [&](int k) { return k == 0 && nu > 1 ? P.s2 : 1.0f; };
     const int cur_down = (nu - 1) & 1, cur_up = 1;
     for (int l = 0; l < ND; l++) {  // descend on the distributed levels
         int s, e;
@@ -1566,7 +1582,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterPlan P
             }
         cl_sync();
         int cur = 0;
-        for (int k = 1; k < nu; k++) cur = sweep_d(l, cur);
+        for (int k = 1; k < nu; k++) cur = sweep_d(l, cur, wpre(k));
         const float *XC = Xb[cur];
         const int nxc = P.lv[l + 1].nx, nyc = P.lv[l + 1].ny;
         int cs, ce;
@@ -1605,14 +1621,14 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterPlan P
             if (iy > 0) y += sN[o + i - nx] * (xc - X[o + i - nx]);
             return y;
         };
-        auto sweep = [&](int l, int cur) {
+        auto sweep = [&](int l, int cur, float w) {
             const int nx = P.lv[l].nx, ny = P.lv[l].ny, o = P.lv[l].off;
             const float *XI = Xb[cur];
             float *XO = Xb[cur ^ 1];
             for (int iy = ty; iy < ny; iy += nty)
                 for (int ix = tx; ix < nx; ix += 32) {
                     const int i = ix + iy * nx;
-                    XO[o + i] = XI[o + i] + sP[o + i] * (sB[o + i] - Ax(l, XI, ix, iy, i));
+                    XO[o + i] = XI[o + i] + __fmul_rn(sP[o + i], w) * (sB[o + i] - Ax(l, XI, ix, iy, i));
                 }
             __syncthreads();
             return cur ^ 1;
@@ -1622,7 +1638,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterPlan P
             for (int i = tid; i < n; i += kClusterThreads) sX[o + i] = sP[o + i] * sB[o + i];
             __syncthreads();
             int cur = 0;
-            for (int k = 1; k < nu; k++) cur = sweep(l, cur);
+            for (int k = 1; k < nu; k++) cur = sweep(l, cur, wpre(k));
             const float *XC = Xb[cur];
             const int nxf = P.lv[l].nx, nyf = P.lv[l].ny, nxc = P.lv[l + 1].nx, nyc = P.lv[l + 1].ny,
                       oc = P.lv[l + 1].off;
@@ -1658,7 +1674,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterPlan P
                 }
             __syncthreads();
             int cur = cur_down;
-            for (int k = 0; k < nu; k++) cur = sweep(l, cur);
+            for (int k = 0; k < nu; k++) cur = sweep(l, cur, wpost(k));
         }
     }
     cl_sync();
@@ -1684,7 +1700,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterPlan P
             }
         cl_sync();
         int cur = cur_down;
-        for (int k = 0; k < nu; k++) cur = sweep_d(l, cur);
+        for (int k = 0; k < nu; k++) cur = sweep_d(l, cur, wpost(k));
     }
     for (int iy = s0 + ty; iy < e0; iy += nty)
         for (int ix = tx; ix < P.lv[0].nx; ix += 32) x_top[ix + iy * P.lv[0].nx] = Xb[cur_up][at(0, s0, ix, iy)];
@@ -1702,9 +1718,13 @@ static int mg_grid(Ctx *c, long long n) {
 static const dim3 kBlock2d(32, 8);
 static dim3 grid2d(int nx, int ny) { return dim3((unsigned)((nx + 31) / 32), (unsigned)((ny + 7) / 8)); }
 
-static Lv level_view(const MgLevel &m, const int *done) {
-    return Lv{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, done};
+static Lv level_view(const Ctx *c, const MgLevel &m, const int *done) {
+    return Lv{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, done, c->mg_s2};
 }
+// Per-sweep kernels: the weight factor of pre-sweep s (1 .. nu - 1; sweep 0 is k_mg_pre0) and of
+// post-sweep s (0 .. nu - 1), as the fused kernels apply it.
+static float sweep_pre(const Ctx *c, int s) { return s == c->mg_nu - 1 ? c->mg_s2 : 1.0f; }
+static float sweep_post(const Ctx *c, int s) { return s == 0 && c->mg_nu > 1 ? c->mg_s2 : 1.0f; }
 
 // The fused two-sweep level kernels serve nu = 2 (the default); other nu use the per-sweep kernels.
 // Among the fused kernels, the tile ones are the default (SHK_MG_FUSED=1); the warp-marching ones
@@ -1745,6 +1765,7 @@ static size_t bottom_plan(const Ctx *c, int lb, BottomPlan *P) {
         off += m.nx * m.ny;
     }
     P->total = off;
+    P->s2 = c->mg_s2;
     return (size_t)off * kBottomBytesPerCell;
 }
 
@@ -1785,6 +1806,7 @@ static bool cluster_plan(const Ctx *c, int *lc_out, ClusterPlan *P, size_t *byte
             P->slot_rows[k] = k < P->ndist ? slab_rows(lc + k) + 1 : m.ny;
             off += P->slot_rows[k] * m.nx;
         }
+        P->s2 = c->mg_s2;
         *lc_out = lc;
         *bytes = (size_t)cells * kClusterBytesPerCell;
         return true;
@@ -2036,7 +2058,7 @@ static const CUtensorMap *r_map(const Ctx *c, const MgTma *T, const double *r) {
 static int vcycle(Ctx *c, int l, CgDev *cg, int *res) {
     MgLevel &m = c->mg[l];
     const int *done = &cg->done;
-    const Lv L = level_view(m, done);
+    const Lv L = level_view(c, m, done);
     const float wc = c->mg_omega_c;
     {
         ClusterPlan CP;
@@ -2119,17 +2141,17 @@ static int vcycle(Ctx *c, int l, CgDev *cg, int *res) {
     k_mg_pre0<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[0]);
     int cur = 0;
     for (int s = 1; s < c->mg_nu; s++, cur ^= 1)
-        k_mg_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1]);
+        k_mg_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1], sweep_pre(c, s));
     k_mg_restrict<float><<<gc, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], g.nx, g.ny, g.b);
     c->launches += 1 + c->mg_nu;
     int gres = 0;
     int rc = vcycle(c, l + 1, cg, &gres);
     if (rc) return rc;
     k_mg_prolong_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], g.x[gres], g.nx, wc,
-                                                              m.x[cur ^ 1]);
+                                                              m.x[cur ^ 1], sweep_post(c, 0));
     cur ^= 1;
     for (int s = 1; s < c->mg_nu; s++, cur ^= 1)
-        k_mg_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1]);
+        k_mg_sweep<float><<<gf, kBlock2d, 0, c->stream>>>(L, m.b, m.x[cur], m.x[cur ^ 1], sweep_post(c, s));
     c->launches += c->mg_nu;
     *res = cur;
     return SHK_OK;
@@ -2138,7 +2160,7 @@ static int vcycle(Ctx *c, int l, CgDev *cg, int *res) {
 // z = M^-1 r on level 0 (r Float64), then the outer CG's r'z (init or iteration finish).
 int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
     MgLevel &m = c->mg[0];
-    const Lv L = level_view(m, &cg->done);
+    const Lv L = level_view(c, m, &cg->done);
     const int n = m.nx * m.ny;
     const float wc = c->mg_omega_c;
     const int gl = std::min(c->max_blocks, std::max(1, std::min(c->num_sms * 8, (n + kThreads - 1) / kThreads)));
@@ -2194,7 +2216,7 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
     k_mg_pre0<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[0]);
     int cur = 0;
     for (int s = 1; s < c->mg_nu; s++, cur ^= 1)
-        k_mg_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1]);
+        k_mg_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1], sweep_pre(c, s));
     k_mg_restrict<double><<<gc, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], g.nx, g.ny, g.b);
     c->launches += 1 + c->mg_nu;
     int gres = 0;
@@ -2206,10 +2228,10 @@ int mg_apply(Ctx *c, const double *r, double *z, CgDev *cg, bool init) {
         c->launches++;
     } else {
         k_mg_prolong_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], g.x[gres], g.nx, wc,
-                                                                   m.x[cur ^ 1]);
+                                                                   m.x[cur ^ 1], sweep_post(c, 0));
         cur ^= 1;
         for (int s = 2; s < c->mg_nu; s++, cur ^= 1)
-            k_mg_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1]);
+            k_mg_sweep<double><<<gf, kBlock2d, 0, c->stream>>>(L, r, m.x[cur], m.x[cur ^ 1], 1.0f);
         k_mg_last<false><<<gl, kThreads, 0, c->stream>>>(L, r, m.x[cur], nullptr, 1, wc, z, cg, init, c->partials,
                                                          c->counter);
         c->launches += c->mg_nu;
@@ -2312,7 +2334,7 @@ int mg_catch_up(Ctx *c, double *x, CgDev *cg) {
 int mg_apply_fused_update(Ctx *c, const double *r_in, double *r_out, double *x, const double *p, const double *Ap,
                           double *z, CgDev *cg, const double *p_prev, int mode, int pbuf) {
     MgLevel &m = c->mg[0];
-    const Lv L = level_view(m, &cg->done);
+    const Lv L = level_view(c, m, &cg->done);
     MgLevel &g = c->mg[1];
     const float wc = c->mg_omega_c;
     int trc = SHK_OK;
@@ -2386,6 +2408,7 @@ struct EnsMg {
     float wc;
     int nu;
     double omega;
+    float s2;  // Lv::s2
 };
 
 // block -> (instance, position in its range) for table `tab` of depth d
@@ -2435,7 +2458,7 @@ __global__ void __launch_bounds__(256, 6) k_ens_mg_down0(EnsInst *E, const EnsMg
     if (!I.pic_active) return;
     const EnsMg &G = M[q.i];
     const MgLevel &m = G.lv[0], &g = G.lv[1];
-    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done};
+    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done, G.s2};
     if constexpr (FB) {
         const double *r_in = parity ? I.r2 : I.r;
         double *r_out = parity ? I.r : I.r2;
@@ -2452,7 +2475,7 @@ __global__ void __launch_bounds__(256, 6) k_ens_mg_down(EnsInst *E, const EnsMg 
     if (!I.pic_active) return;
     const EnsMg &G = M[q.i];
     const MgLevel &m = G.lv[d], &g = G.lv[d + 1];
-    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done};
+    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done, G.s2};
     mg_down_body<float, false>(q.B, L, m.b, m.x[0], g.nx, g.ny, g.b, FusedB{}, nullptr);
 }
 
@@ -2471,7 +2494,7 @@ __global__ void __launch_bounds__(256, 6) k_ens_mg_up(EnsInst *E, const EnsMg *M
     if (!I.pic_active) return;
     const EnsMg &G = M[q.i];
     const MgLevel &m = G.lv[d], &g = G.lv[d + 1];
-    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done};
+    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done, G.s2};
     const float *xc = g.x[d + 1 == G.lb ? 0 : 1];
     mg_up_body<float, false>(q.B, L, m.b, m.x[0], xc, g.nx, G.wc, m.x[1], nullptr, nullptr, 0, nullptr, nullptr);
 }
@@ -2485,7 +2508,7 @@ __global__ void __launch_bounds__(256, 6) k_ens_mg_up0(EnsInst *E, const EnsMg *
     if (!I.pic_active) return;
     const EnsMg &G = M[q.i];
     const MgLevel &m = G.lv[0], &g = G.lv[1];
-    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done};
+    const Lv L{m.nx, m.ny, m.aE, m.aN, m.dP, m.wD, m.act, &I.cg->done, G.s2};
     const double *r = init ? I.r : (parity ? I.r : I.r2);  // the iteration's new residual buffer
     const float *xc = g.x[1 == G.lb ? 0 : 1];
     mg_up_body<double, true>(q.B, L, r, m.x[0], xc, g.nx, G.wc, nullptr, I.z, I.cg, init, I.partials, I.counter);
@@ -2538,6 +2561,7 @@ int ens_mg_upload(EnsMg *dM, int i, Ctx *c, const int *blk0_vc, const int *blk0_
     G.wc = c->mg_omega_c;
     G.nu = c->mg_nu;
     G.omega = (double)c->mg_omega;
+    G.s2 = c->mg_s2;
     return cudaMemcpy(dM + i, &G, sizeof(G), cudaMemcpyHostToDevice) == cudaSuccess ? SHK_OK : SHK_CUDA_ERROR;
 }
 
