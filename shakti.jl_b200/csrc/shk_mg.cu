@@ -10,10 +10,12 @@
 // in Float32, the outer CG (residual, updates, stopping test) in Float64.
 //
 // Identity rows (OCEAN/LAND/OTHER_BASIN cells: aP = 1, no couplings) are not aggregated (their row
-// of P is zero); the smoother solves them exactly.  The V-cycle is symmetric (the same damped-Jacobi
-// sweeps before and after the coarse correction; exact solve on the 1x1 coarsest level), so it is
-// a valid CG preconditioner.  Per level: nu damped-Jacobi sweeps (omega) before and after, coarse
-// correction scaled by omega_c; the levels that fit in one block's shared memory run as one kernel.
+// of P is zero); the smoother solves them exactly.  The V-cycle is symmetric (the same sweep weights
+// before and after the coarse correction; exact solve on the 1x1 coarsest level), so it is a valid
+// CG preconditioner.  Per level: nu Jacobi sweeps before and after, with the stored damped inverse
+// diagonal wD = omega/aP, the two sweeps next to the coarse correction scaled by Lv::s2 (1 for
+// damped Jacobi, tau2/tau1 for the degree-2 Chebyshev pair), coarse correction scaled by omega_c;
+// the levels that fit in one block's shared memory run as one kernel.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <float.h>
